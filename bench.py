@@ -1,0 +1,343 @@
+#!/usr/bin/env python3
+"""Throughput of the tracer advection step on B200.
+
+Workload (the plain method at scale): doubly periodic analytic mesh
+nx = ny = 1000 (998,001 nodes, 2,994,003 edges, 1,996,002 triangles), 64
+levels, per-node bottom level uniform in [3, 64] (seed 0), a seeded layered
+flow with |u| <= 1 m/s at CFL 0.5 (dt = 0.5 dx / 1 m/s), two tracers
+(temperature-like U[0,20] + Gaussian blobs, salinity-like 35 + N(0, 0.5)),
+MUSCL + PPM + FCT in FP64, valuesAB := values each step.  One "step" advances
+both tracers once.  Metric: tracer cell-updates/s = wet cells x tracers /
+step time.
+
+Arms:
+  default            this library, through its C ABI (device-resident inputs
+                     for "value"; host buffers copied in and out every step for
+                     "e2e")
+  --impl reference   the reference algorithm on the host cores: the CPU
+                     oracle (a C restatement of the reference's Fortran, which
+                     cannot be compiled here: no Fortran compiler), OpenMP over
+                     all host threads, on a bounded sample of the same workload.
+
+Multi-GPU (torchrun): every rank advects its own replica of the workload on
+its own GPU with no data-path collective (weak scaling); a barrier brackets
+the timed region and the device time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+BYTES_PER_CELL = {"fp64": 112}  # 14 words per wet cell at storage precision
+L2_BYTES = 126 * 2**20
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--nx", type=int, default=1000)
+    p.add_argument("--nl", type=int, default=64)
+    p.add_argument("--e2e-steps", type=int, default=3)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def workload_name(nx, nl):
+    return f"periodic {nx}x{nx}x{nl}, bathymetry U[3,{nl}] seed 0, MUSCL+PPM+FCT, 2 tracers"
+
+
+def make_inputs(api, nx, nl):
+    from fesom2_tracer_dwarf_b200 import synth_bathymetry
+    N = api.lib.tracer_analytic_nodes(nx, nx, 1)
+    K = synth_bathymetry(N, nl, 0)
+    api.init_analytic(nx, nx, nl, periodic=True, full_rings=True, node_K=K)
+    uv, w = api.synth_velocity(seed=1, umax=1.0, mode2=0.5)
+    T = api.synth_tracer(seed=2, kind=0)
+    S = api.synth_tracer(seed=3, kind=1)
+    dt = 0.5 * (1.0e5 / (nx - 1)) / 1.0
+    cells = int((api.mesh_array("nlevels_nod2D") - 1).sum())
+    return K, uv, w, T, S, dt, cells
+
+
+# ---------------------------------------------------------------------------
+# clocks
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits", "-i", str(self.gpu),
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        for line in Path(self.path).read_text().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                rows.append((float(f[1]), float(f[2]), float(f[3]), f[5], f[6], f[7], f[8]))
+            except ValueError:
+                continue
+        os.unlink(self.path)
+        if not rows:
+            return None
+        loaded = [r for r in rows if r[2] > 200.0] or rows
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in loaded:
+            for nm, v in zip(names, r[3:]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(r[0] for r in loaded), "sm_max_mhz": max(r[1] for r in rows),
+                "reasons": sorted(reasons), "samples": len(loaded)}
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def committed_traffic():
+    """DRAM bytes per step of the plain FP64 step from the committed ncu
+    summary (profiles/step_c2_fp64.md, line 'dram_bytes_per_step_scaled: X')."""
+    p = ROOT / "profiles" / "step_c2_fp64.md"
+    if not p.exists():
+        return None
+    for line in p.read_text().splitlines():
+        if line.strip().startswith("dram_bytes_per_step_scaled:"):
+            try:
+                return float(line.split(":", 1)[1].split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+# ---------------------------------------------------------------------------
+# CPU arm: the oracle on a bounded sample
+# ---------------------------------------------------------------------------
+def cpu_rate(nx_sample, nl, steps, warmup=1):
+    """Cell-updates/s of the OpenMP oracle on a periodic nx_sample^2 x nl
+    mesh drawn like the GPU workload.  Returns (rate, threads, sample text,
+    per-step seconds)."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import pyoracle
+    from fesom2_tracer_dwarf_b200 import FESOMTracerAdvection
+    api = FESOMTracerAdvection()
+    api.cleanup()
+    K, uv, w, T, S, dt, cells = make_inputs(api, nx_sample, nl)
+    api.cleanup()
+    o = pyoracle.Oracle(openmp=True)
+    o.set_threads(os.cpu_count() or 1)
+    m = pyoracle.OracleMesh(o, nx_sample, nx_sample, nl, periodic=True, full_rings=True, node_K=K)
+    N = m.nod2D
+    vals = np.ascontiguousarray(np.stack([T.T, S.T]))  # (2, nod2D, nl-1): each tracer a Fortran (nl-1, nod2D) block
+    ab = vals.copy()
+    m.run(vals, ab, uv, w, dt, warmup, "MUSCL", "PPM", "FCT", refresh_ab=True)
+    per = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        m.run(vals, ab, uv, w, dt, 1, "MUSCL", "PPM", "FCT", refresh_ab=True)
+        per.append(time.perf_counter() - t0)
+    sec = statistics.median(per)
+    rate = 2 * cells / sec
+    sample = (f"periodic {nx_sample}x{nx_sample}x{nl} ({N} nodes, {cells} wet cells), same bathymetry/flow/tracer "
+              f"distributions, 2 tracers, median of {steps} steps after {warmup} warm-up")
+    return rate, o.threads(), sample, per
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    nx_sample = min(args.nx, 300)
+    steps = max(1, args.steps)
+    rate, threads, sample, per = cpu_rate(nx_sample, args.nl, steps, warmup=max(1, min(args.warmup, 2)))
+    sec = statistics.median(per)
+    line = {
+        "metric": "tracer cell-updates/s", "value": rate, "unit": "cell-updates/s", "impl": "reference",
+        "n_gpus": args.gpus, "steps": steps, "warmup": args.warmup, "ms_per_step": sec * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": workload_name(args.nx, args.nl), "sample": sample},
+        "cpu_baseline": {"value": rate, "unit": "cell-updates/s", "cores": threads, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": rate, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------
+def run_ours(args):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as tdist
+        torch.cuda.set_device(local)
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                 device_id=torch.device("cuda", local))
+        dist = tdist
+
+    from fesom2_tracer_dwarf_b200 import FESOMTracerAdvection
+    api = FESOMTracerAdvection()
+    api.cleanup()
+    if api.lib.tracer_set_device(local) != 0:
+        raise RuntimeError(api.lib.tracer_last_error().decode())
+    K, uv, w, T, S, dt, cells = make_inputs(api, args.nx, args.nl)
+    api.allocate_tracers(2)
+    api.set_values(1, T)
+    api.set_values(2, S)
+    for t in (1, 2):
+        api.set_scheme(t, "MUSCL", "PPM", "FCT")
+    api.set_velocity(uv, w)
+    api.set_ab_refresh(True)
+    api.advect_steps(args.warmup, dt)
+    launches_per_step = api.lib.tracer_launches_per_step()
+    dev_bytes = api.lib.tracer_device_bytes()
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    # device-resident throughput, CUDA events on the engine's stream
+    clock = ClockSampler(local)
+    clock.start()
+    barrier()
+    ms = api.time_steps(args.steps, dt)
+    barrier()
+    clocks = clock.stop()
+    if dist is not None:
+        import torch
+        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    ms_per_step = ms / args.steps
+    value = world * 2 * cells / (ms_per_step / 1e3)
+
+    # per-kernel breakdown (events around each launch), untimed otherwise
+    nk = 6
+    kms = np.zeros(nk)
+    names = (ctypes.c_char_p * nk)()
+    launches = np.zeros(1, dtype=np.int32)
+    prof_steps = max(2, min(args.steps, 5))
+    rc = api.lib.tracer_profile_steps(prof_steps, dt, kms.ctypes.data_as(ctypes.c_void_p),
+                                      ctypes.cast(names, ctypes.c_void_p), nk,
+                                      launches.ctypes.data_as(ctypes.POINTER(ctypes.c_int)))
+    if rc != 0:
+        raise RuntimeError(api.lib.tracer_last_error().decode())
+    kernel_ms = {names[i].decode(): kms[i] / prof_steps for i in range(nk)}
+
+    # end to end through the C ABI with host buffers: set both tracers from
+    # host memory, one step, read both back, every step
+    L, N = args.nl - 1, T.shape[1]
+    Th, Sh = np.asfortranarray(api.get_tracer_values(1)), np.asfortranarray(api.get_tracer_values(2))
+    outT = np.zeros_like(Th, order="F")
+    outS = np.zeros_like(Sh, order="F")
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.e2e_steps):
+        api.set_values(1, Th)
+        api.set_values(2, Sh)
+        if api.advect_step(dt) != 0:
+            raise RuntimeError(api.lib.tracer_last_error().decode())
+        api.lib.tracer_get_values_id(1, outT.ctypes.data_as(ctypes.c_void_p), L, N)
+        api.lib.tracer_get_values_id(2, outS.ctypes.data_as(ctypes.c_void_p), L, N)
+    e2e_sec = (time.perf_counter() - t0) / args.e2e_steps
+    if dist is not None:
+        import torch
+        t = torch.tensor([e2e_sec], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_sec = float(t.item())
+    h2d = 2 * L * N * 8
+    d2h = 2 * L * N * 8
+
+    result = None
+    if rank == 0:
+        peak, peak_kind = measured_peaks()
+        alg_bytes_step = BYTES_PER_CELL["fp64"] * cells * 2
+        achieved = alg_bytes_step / (ms_per_step / 1e3) / 1e9
+        traffic = committed_traffic()
+        result = {
+            "metric": "tracer cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": workload_name(args.nx, args.nl), "wet_cells": cells, "tracers": 2,
+                       "dt_s": dt, "parallelism": f"replicas x{world}",
+                       "l2": f"inputs larger than L2 ({dev_bytes / 1e9:.1f} GB resident vs 0.13 GB L2)"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "kernel": "full step (all kernels of one step, 112 B/cell algorithmic)",
+                         "peak_source": f"{peak_kind} hbm_gbs"},
+            "kernel_ms_per_step": kernel_ms,
+            "e2e": {"value": world * 2 * cells / e2e_sec, "unit": "cell-updates/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "gpu_launches": launches_per_step * args.steps,
+            "clocks": clocks,
+        }
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    api.cleanup()
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        rate, threads, sample, _ = cpu_rate(min(args.nx, 300), args.nl, 3)
+        result["cpu_baseline"] = {"value": rate, "unit": "cell-updates/s", "cores": threads, "kind": "port",
+                                  "sample": sample}
+    if rank == 0:
+        print(json.dumps(result))
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

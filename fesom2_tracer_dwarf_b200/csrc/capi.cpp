@@ -1,0 +1,615 @@
+// C ABI of libfesom_tracer.so (declarations and reference citations in
+// include/fesom_tracer.h).  One global instance, like the module state of the
+// reference's lib/tracer_c_interface.F90.
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/fesom_tracer.h"
+#include "engine.hpp"
+
+using namespace fesom;
+
+namespace {
+
+struct State {
+  bool initialized = false;     // tracer_initialized of the reference
+  bool ab_refresh = false;
+  int nl = 0, nod2D = 0, edge2D = 0, elem2D = 0;  // tracer_set_mesh_dims
+  int myDim = 0, eDim = 0;
+  std::vector<int> nlevels_nod2D;
+  std::vector<double> hnode_new;
+  std::unique_ptr<MeshHost> mesh;  // connectivity (analytic or from arrays)
+  std::unique_ptr<Engine> eng;
+  int ntr = 0;
+  std::vector<TracerScheme> schemes;
+  // host copies kept until the engine exists
+  std::vector<std::vector<double>> pend_values, pend_ab;
+  std::vector<double> pend_uv, pend_w;  // uv in (2, nl-1, elem2D)
+  bool pend_vel = false;
+};
+State g;
+
+int fail(const std::string &msg) {
+  set_last_error(msg);
+  std::fprintf(stderr, "### error: %s\n", msg.c_str());
+  return -1;
+}
+
+template <class F>
+int guarded(F &&f) {
+  try {
+    set_last_error("");
+    return f();
+  } catch (const std::exception &e) {
+    return fail(e.what());
+  }
+}
+
+// Create the engine once a mesh with connectivity exists, then push any
+// values that were set before.
+void ensure_engine() {
+  if (g.eng) return;
+  if (!g.mesh) throw std::runtime_error("no mesh connectivity: use tracer_init_analytic or tracer_set_mesh_arrays");
+  g.eng.reset(new Engine(*g.mesh));
+  if (g.ntr > 0) {
+    g.eng->allocate_tracers(g.ntr);
+    for (int i = 0; i < g.ntr; i++) {
+      g.eng->set_scheme(i, g.schemes[i]);
+      if (!g.pend_values[i].empty()) g.eng->set_values(i, g.pend_values[i].data(), true);
+      if (!g.pend_ab[i].empty()) g.eng->set_values_ab(i, g.pend_ab[i].data());
+    }
+  }
+  if (g.pend_vel) g.eng->set_velocity(g.pend_uv.data(), g.pend_w.data());
+}
+
+void install_mesh(MeshHost &&m) {
+  g.eng.reset();
+  g.mesh.reset(new MeshHost(std::move(m)));
+  g.nl = g.mesh->nl;
+  g.nod2D = g.mesh->nod2D;
+  g.edge2D = g.mesh->edge2D;
+  g.elem2D = g.mesh->elem2D;
+  g.myDim = g.nod2D;
+  g.eDim = 0;
+  g.nlevels_nod2D = g.mesh->nlev_node;
+  g.hnode_new = g.mesh->hnode_new;
+  g.pend_vel = false;
+}
+
+TracerScheme parse_scheme(const char *hor, const char *ver, const char *lim, double ph, double pv) {
+  TracerScheme s;
+  std::string h = hor ? hor : "", v = ver ? ver : "", l = lim ? lim : "";
+  auto trim = [](std::string &x) { while (!x.empty() && (x.back() == ' ' || x.back() == '\0')) x.pop_back(); };
+  trim(h); trim(v); trim(l);
+  if (h == "UPW1") s.hor = 0; else if (h == "MUSCL") s.hor = 1; else if (h == "MFCT") s.hor = 2;
+  else throw std::invalid_argument("Unknown horizontal advection type " + h);
+  if (v == "UPW1") s.ver = 0; else if (v == "PPM") s.ver = 1; else if (v == "QR4C") s.ver = 2; else if (v == "CDIFF") s.ver = 3;
+  else throw std::invalid_argument("Unknown vertical advection type " + v);
+  if (l == "NONE") s.lim = 0; else if (l == "FCT") s.lim = 1;
+  else throw std::invalid_argument("Unknown limiter type " + l);
+  s.ph = ph;
+  s.pv = pv;
+  return s;
+}
+
+int check_ready() {
+  if (!g.initialized) return fail("tracer not initialized. Call tracer_init first.");
+  return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int tracer_init_mpi(int) { return 0; }
+int tracer_finalize_mpi(void) { return 0; }
+
+int tracer_init(const char *restart_dir) {
+  return fail(std::string("binary restart input is not supported by this build (") + (restart_dir ? restart_dir : "") + ")");
+}
+int tracer_finalize(const char *output_dir) {
+  return fail(std::string("binary restart output is not supported by this build (") + (output_dir ? output_dir : "") + ")");
+}
+int tracer_run_workflow(const char *restart_dir, int, double) { return tracer_init(restart_dir); }
+int tracer_load_mesh_partition(const char *restart_dir) {
+  return fail(std::string("binary restart input is not supported by this build (") + (restart_dir ? restart_dir : "") + ")");
+}
+int tracer_load_mesh_from_files(const char *mesh_path) {
+  return fail(std::string("the ASCII mesh reader is not part of this build (") + (mesh_path ? mesh_path : "") + ")");
+}
+
+int tracer_cleanup(void) {
+  return guarded([&] {
+    g.eng.reset();
+    g = State();
+    return 0;
+  });
+}
+
+int tracer_set_mesh_dims(int nl, int nod2D, int edge2D, int elem2D) {
+  if (nl < 3 || nod2D < 1 || edge2D < 0 || elem2D < 0) return fail("invalid mesh dimensions");
+  if (g.mesh && (g.mesh->nl != nl || g.mesh->nod2D != nod2D || g.mesh->edge2D != edge2D || g.mesh->elem2D != elem2D))
+    return fail("mesh dimensions differ from the loaded mesh");
+  g.nl = nl; g.nod2D = nod2D; g.edge2D = edge2D; g.elem2D = elem2D;
+  return 0;
+}
+
+int tracer_set_levels(const int *nlevels, const int *ulevels, int nod2D) {
+  if (!nlevels || !ulevels) return fail("null level array");
+  if (nod2D != g.nod2D) return fail("tracer_set_levels: nod2D does not match the mesh dimensions");
+  for (int i = 0; i < nod2D; i++) {
+    if (ulevels[i] != 1) return fail("ulevels /= 1 (cavities) is not supported");
+    if (nlevels[i] < 2 || nlevels[i] > g.nl) return fail("nlevels outside [2, nl]");
+  }
+  if (g.mesh)
+    for (int i = 0; i < nod2D; i++)
+      if (nlevels[i] != g.mesh->nlev_node[i]) return fail("nlevels differ from the loaded mesh");
+  g.nlevels_nod2D.assign(nlevels, nlevels + nod2D);
+  return 0;
+}
+
+int tracer_set_thickness(const double *hnode, int nl, int nod2D) {
+  if (!hnode) return fail("null thickness array");
+  if (nl != g.nl || nod2D != g.nod2D) return fail("tracer_set_thickness: dimensions do not match");
+  g.hnode_new.assign(hnode, hnode + (size_t)(nl - 1) * nod2D);
+  if (g.mesh) {
+    g.mesh->hnode_new = g.hnode_new;
+    g.eng.reset();  // geometry changed: rebuild the device copy lazily
+  }
+  return 0;
+}
+
+int tracer_set_partition(int myDim_nod2D, int eDim_nod2D) {
+  if (eDim_nod2D != 0) return fail("halo nodes (eDim_nod2D > 0) are not supported on one GPU");
+  if (myDim_nod2D != g.nod2D) return fail("myDim_nod2D does not match nod2D");
+  g.myDim = myDim_nod2D;
+  g.eDim = 0;
+  return 0;
+}
+
+int tracer_allocate_tracers(int num_tracers, int nl, int nod2D, int AB_order) {
+  return guarded([&] {
+    if (num_tracers < 1) return fail("num_tracers < 1");
+    if (nl != g.nl || nod2D != g.nod2D) return fail("tracer_allocate_tracers: dimensions do not match");
+    if (AB_order < 1) return fail("AB_order < 1");
+    g.ntr = num_tracers;
+    g.schemes.assign(num_tracers, TracerScheme());
+    g.pend_values.assign(num_tracers, std::vector<double>((size_t)(nl - 1) * nod2D, 0.0));
+    g.pend_ab.assign(num_tracers, std::vector<double>());
+    if (g.eng) {
+      g.eng->allocate_tracers(num_tracers);
+      for (int i = 0; i < num_tracers; i++) g.eng->set_values(i, g.pend_values[i].data(), true);
+    }
+    return 0;
+  });
+}
+
+int tracer_set_values(int tracer_id, const double *values, int nl, int nod2D) {
+  return guarded([&] {
+    if (tracer_id < 1 || tracer_id > g.ntr)
+      return fail("invalid tracer_id " + std::to_string(tracer_id) + ", num_tracers=" + std::to_string(g.ntr));
+    if (!values) return fail("null values");
+    if (nl != g.nl || nod2D != g.nod2D) return fail("tracer_set_values: dimensions do not match");
+    g.pend_values[tracer_id - 1].assign(values, values + (size_t)(nl - 1) * nod2D);
+    g.pend_ab[tracer_id - 1].clear();
+    if (g.eng) g.eng->set_values(tracer_id - 1, values, true);
+    return 0;
+  });
+}
+
+int tracer_set_values_ab(int tracer_id, const double *values, int nl, int nod2D) {
+  return guarded([&] {
+    if (tracer_id < 1 || tracer_id > g.ntr) return fail("invalid tracer_id " + std::to_string(tracer_id));
+    if (!values) return fail("null values");
+    if (nl != g.nl || nod2D != g.nod2D) return fail("tracer_set_values_ab: dimensions do not match");
+    g.pend_ab[tracer_id - 1].assign(values, values + (size_t)(nl - 1) * nod2D);
+    if (g.eng) g.eng->set_values_ab(tracer_id - 1, values);
+    return 0;
+  });
+}
+
+int tracer_set_velocity_zero(int nl, int nod2D, int) {
+  return guarded([&] {
+    if (nl != g.nl || nod2D != g.nod2D) return fail("tracer_set_velocity_zero: dimensions do not match");
+    g.pend_uv.assign((size_t)2 * (nl - 1) * g.elem2D, 0.0);
+    g.pend_w.assign((size_t)nl * nod2D, 0.0);
+    g.pend_vel = true;
+    if (g.eng) g.eng->set_velocity_zero();
+    return 0;
+  });
+}
+
+int tracer_set_velocity_elem(const double *uv, const double *w, int nl, int nod2D, int elem2D) {
+  return guarded([&] {
+    if (!uv || !w) return fail("null velocity");
+    if (nl != g.nl || nod2D != g.nod2D || elem2D != g.elem2D) return fail("tracer_set_velocity_elem: dimensions do not match");
+    g.pend_uv.assign(uv, uv + (size_t)2 * (nl - 1) * elem2D);
+    g.pend_w.assign(w, w + (size_t)nl * nod2D);
+    g.pend_vel = true;
+    if (g.eng) g.eng->set_velocity(uv, w);
+    return 0;
+  });
+}
+
+int tracer_set_velocity(const double *uv, const double *w, int nl, int nod2D, int nelem) {
+  return guarded([&] {
+    if (!uv || !w) return fail("null velocity");
+    if (nelem != g.elem2D)
+      return fail("tracer_set_velocity: uv must be (nl-1, elem2D, 2); got " + std::to_string(nelem) +
+                  " columns for " + std::to_string(g.elem2D) + " elements");
+    const int L = nl - 1;
+    std::vector<double> t((size_t)2 * L * nelem);
+    for (int c = 0; c < 2; c++)
+      for (int e = 0; e < nelem; e++)
+        for (int k = 0; k < L; k++) t[2 * ((size_t)e * L + k) + c] = uv[((size_t)c * nelem + e) * L + k];
+    return tracer_set_velocity_elem(t.data(), w, nl, nod2D, nelem);
+  });
+}
+
+int tracer_init_complete(void) {
+  g.initialized = true;
+  return 0;
+}
+
+int tracer_init_ale_arrays(void) {
+  if (!g.initialized) return fail("tracer_init_ale_arrays called before initialization");
+  if (!g.mesh) return fail("tracer_init_ale_arrays: no vertical grid (zbar) loaded");
+  g.mesh->hnode_new = g.mesh->hnode;
+  g.hnode_new = g.mesh->hnode_new;
+  g.eng.reset();
+  return 0;
+}
+
+int tracer_init_for_advection(void) {
+  return guarded([&] {
+    if (!g.initialized) return fail("tracer_init_for_advection called before mesh loaded");
+    ensure_engine();
+    return 0;
+  });
+}
+
+int tracer_init_analytic(int nx, int ny, int nl, double Lx, double Ly, double max_depth, int periodic,
+                         int full_rings, const int *node_K) {
+  return guarded([&] {
+    if (node_K) {
+      int nn = analytic_nodes(nx, ny, periodic != 0);
+      for (int i = 0; i < nn; i++)
+        if (node_K[i] < 3 || node_K[i] > nl) return fail("node_K outside [3, nl]");
+    }
+    install_mesh(build_analytic_mesh(nx, ny, nl, Lx, Ly, max_depth, periodic != 0, full_rings != 0, node_K));
+    g.initialized = true;
+    return 0;
+  });
+}
+
+int tracer_analytic_nodes(int nx, int ny, int periodic) { return analytic_nodes(nx, ny, periodic != 0); }
+
+int tracer_set_mesh_arrays(int nl, int nod2D, int elem2D, int edge2D, int max_ring, const int *elem2D_nodes,
+                           const int *edges, const int *edge_tri, const int *nlevels, const int *nlevels_nod2D,
+                           const int *ring_num, const int *ring, const double *elem_area, const double *area,
+                           const double *areasvol, const double *edge_dxdy, const double *edge_cross_dxdy,
+                           const double *gradient_sca, const double *elem_cos, const double *zbar,
+                           const double *hnode, const double *hnode_new, const double *helem,
+                           const double *coord_nod2D, double Lx, double Ly) {
+  return guarded([&] {
+    if (nl < 3 || nod2D < 1 || elem2D < 1 || edge2D < 1 || max_ring < 1) return fail("invalid mesh dimensions");
+    const void *ptrs[] = {elem2D_nodes, edges, edge_tri, nlevels, nlevels_nod2D, ring_num, ring, elem_area, area,
+                          areasvol, edge_dxdy, edge_cross_dxdy, gradient_sca, elem_cos, zbar, hnode, hnode_new,
+                          helem, coord_nod2D};
+    for (const void *p : ptrs)
+      if (!p) return fail("null mesh array");
+    MeshHost m;
+    m.nl = nl; m.nod2D = nod2D; m.elem2D = elem2D; m.edge2D = edge2D;
+    m.periodic = Lx > 0.0 && Ly > 0.0;
+    m.Lx = Lx; m.Ly = Ly;
+    m.coord.assign(coord_nod2D, coord_nod2D + 2 * (size_t)nod2D);
+    m.elem_nodes.resize(3 * (size_t)elem2D);
+    for (size_t i = 0; i < m.elem_nodes.size(); i++) m.elem_nodes[i] = elem2D_nodes[i] - 1;
+    m.edge_nodes.resize(2 * (size_t)edge2D);
+    m.edge_tri.resize(2 * (size_t)edge2D);
+    for (size_t i = 0; i < m.edge_nodes.size(); i++) {
+      m.edge_nodes[i] = edges[i] - 1;
+      m.edge_tri[i] = edge_tri[i] > 0 ? edge_tri[i] - 1 : -1;
+    }
+    for (int e = 0; e < edge2D; e++)
+      if (m.edge_tri[2 * e] < 0) return fail("edge_tri(1, e) must be a valid element");
+    m.nlev_elem.assign(nlevels, nlevels + elem2D);
+    m.nlev_node.assign(nlevels_nod2D, nlevels_nod2D + nod2D);
+    m.ring_ptr.assign(nod2D + 1, 0);
+    for (int n = 0; n < nod2D; n++) {
+      if (ring_num[n] < 1 || ring_num[n] > max_ring) return fail("ring_num outside [1, max_ring]");
+      m.ring_ptr[n + 1] = m.ring_ptr[n] + ring_num[n];
+    }
+    m.ring_elem.resize(m.ring_ptr[nod2D]);
+    for (int n = 0; n < nod2D; n++)
+      for (int j = 0; j < ring_num[n]; j++) m.ring_elem[m.ring_ptr[n] + j] = ring[(size_t)n * max_ring + j] - 1;
+    m.elem_area.assign(elem_area, elem_area + elem2D);
+    m.area.assign(area, area + (size_t)nl * nod2D);
+    m.areasvol.assign(areasvol, areasvol + (size_t)nl * nod2D);
+    m.edge_dxdy.assign(edge_dxdy, edge_dxdy + 2 * (size_t)edge2D);
+    m.edge_cross.assign(edge_cross_dxdy, edge_cross_dxdy + 4 * (size_t)edge2D);
+    m.grad_sca.assign(gradient_sca, gradient_sca + 6 * (size_t)elem2D);
+    m.elem_cos.assign(elem_cos, elem_cos + elem2D);
+    m.zbar.assign(zbar, zbar + nl);
+    m.Z.resize(nl - 1);
+    for (int k = 0; k < nl - 1; k++) m.Z[k] = 0.5 * (m.zbar[k] + m.zbar[k + 1]);
+    m.hnode.assign(hnode, hnode + (size_t)(nl - 1) * nod2D);
+    m.hnode_new.assign(hnode_new, hnode_new + (size_t)(nl - 1) * nod2D);
+    m.helem.assign(helem, helem + (size_t)(nl - 1) * elem2D);
+    for (int i = 0; i < 3 * elem2D; i++)
+      if (m.elem_nodes[i] < 0 || m.elem_nodes[i] >= nod2D) return fail("elem2D_nodes out of range");
+    for (int i = 0; i < 2 * edge2D; i++)
+      if (m.edge_nodes[i] < 0 || m.edge_nodes[i] >= nod2D || m.edge_tri[i] >= elem2D) return fail("edges / edge_tri out of range");
+    for (int r : m.ring_elem)
+      if (r < 0 || r >= elem2D) return fail("nod_in_elem2D out of range");
+    m.finalize_tables();
+    std::string bad = m.validate();
+    if (!bad.empty()) return fail("mesh: " + bad);
+    install_mesh(std::move(m));
+    g.initialized = true;
+    return 0;
+  });
+}
+
+int tracer_set_scheme(int tracer_id, const char *hor, const char *ver, const char *lim, double ph, double pv) {
+  return guarded([&] {
+    if (tracer_id < 1 || tracer_id > g.ntr) return fail("invalid tracer_id " + std::to_string(tracer_id));
+    g.schemes[tracer_id - 1] = parse_scheme(hor, ver, lim, ph, pv);
+    if (g.eng) g.eng->set_scheme(tracer_id - 1, g.schemes[tracer_id - 1]);
+    return 0;
+  });
+}
+
+int tracer_set_ab_refresh(int on) {
+  g.ab_refresh = on != 0;
+  return 0;
+}
+
+int tracer_advect_steps(int nsteps, double dt) {
+  return guarded([&] {
+    if (check_ready()) return -1;
+    if (g.ntr < 1) return fail("no tracers allocated");
+    if (!(dt > 0.0)) return fail("dt must be positive");
+    ensure_engine();
+    for (int s = 0; s < nsteps; s++) g.eng->step(dt, g.ab_refresh);
+    g.eng->synchronize();
+    return 0;
+  });
+}
+
+int tracer_advect_step(double dt) { return tracer_advect_steps(1, dt); }
+
+int tracer_get_values_id(int tracer_id, double *values, int nz, int nn) {
+  return guarded([&] {
+    if (check_ready()) return -1;
+    if (tracer_id < 1 || tracer_id > g.ntr) return fail("invalid tracer_id " + std::to_string(tracer_id));
+    if (!values) return fail("null values");
+    if (nz != g.nl - 1 || nn != g.nod2D) return fail("tracer_get_values: expected (" + std::to_string(g.nl - 1) + ", " + std::to_string(g.nod2D) + ")");
+    if (g.eng) g.eng->get_values(tracer_id - 1, values);
+    else std::memcpy(values, g.pend_values[tracer_id - 1].data(), sizeof(double) * (size_t)nz * nn);
+    return 0;
+  });
+}
+
+int tracer_get_values(double *values, int nz, int nn) { return tracer_get_values_id(1, values, nz, nn); }
+
+int tracer_get_stats_id(int tracer_id, double *s4) {
+  return guarded([&] {
+    if (check_ready()) return -1;
+    if (tracer_id < 1 || tracer_id > g.ntr) return fail("invalid tracer_id " + std::to_string(tracer_id));
+    if (g.eng) {
+      g.eng->stats(tracer_id - 1, s4);
+    } else {
+      const std::vector<double> &v = g.pend_values[tracer_id - 1];
+      double mn = v[0], mx = v[0], sm = 0.0, nan = 0.0;
+      for (double x : v) { mn = x < mn ? x : mn; mx = x > mx ? x : mx; sm += x; nan += (x != x); }
+      s4[0] = mn; s4[1] = mx; s4[2] = sm; s4[3] = nan;
+    }
+    return 0;
+  });
+}
+
+int tracer_get_stats(double *tmin, double *tmax, double *tsum) {
+  if (!g.initialized) {
+    if (tmin) *tmin = 0.0;
+    if (tmax) *tmax = 0.0;
+    if (tsum) *tsum = 0.0;
+    return fail("tracer not initialized.");
+  }
+  double s4[4];
+  int rc = tracer_get_stats_id(1, s4);
+  if (rc) return rc;
+  *tmin = s4[0]; *tmax = s4[1]; *tsum = s4[2];
+  return 0;
+}
+
+int tracer_get_size(int *nz, int *nn) {
+  if (!g.initialized) {
+    if (nz) *nz = 0;
+    if (nn) *nn = 0;
+    return fail("tracer not initialized.");
+  }
+  *nz = g.nl - 1;
+  *nn = g.nod2D;
+  return 0;
+}
+
+int tracer_analytic_fields(double *T, double *S, double *uv, double *w) {
+  return guarded([&] {
+    if (!g.mesh) return fail("no analytic mesh");
+    std::vector<double> t, s, u, ww;
+    analytic_driver_fields(*g.mesh, t, s, u, ww);
+    if (T) std::memcpy(T, t.data(), t.size() * 8);
+    if (S) std::memcpy(S, s.data(), s.size() * 8);
+    if (uv) std::memcpy(uv, u.data(), u.size() * 8);
+    if (w) std::memcpy(w, ww.data(), ww.size() * 8);
+    return 0;
+  });
+}
+
+int tracer_synth_bathymetry(int nnodes, int nl, uint64_t seed, int *K) {
+  return guarded([&] {
+    if (!K || nnodes < 0 || nl < 3) return fail("invalid bathymetry request");
+    std::vector<int> k = synth_bathymetry(nnodes, nl, seed);
+    std::memcpy(K, k.data(), sizeof(int) * (size_t)nnodes);
+    return 0;
+  });
+}
+
+int tracer_synth_velocity(uint64_t seed, double umax, double frac, double *uv, double *w) {
+  return guarded([&] {
+    if (!g.mesh) return fail("no mesh");
+    std::vector<double> u, ww;
+    synth_velocity(*g.mesh, seed, umax, frac, u, ww);
+    if (uv) std::memcpy(uv, u.data(), u.size() * 8);
+    if (w) std::memcpy(w, ww.data(), ww.size() * 8);
+    return 0;
+  });
+}
+
+int tracer_synth_tracer(uint64_t seed, int kind, double *values) {
+  return guarded([&] {
+    if (!g.mesh) return fail("no mesh");
+    std::vector<double> t;
+    synth_tracer(*g.mesh, seed, kind, t);
+    std::memcpy(values, t.data(), t.size() * 8);
+    return 0;
+  });
+}
+
+int tracer_mesh_dims(int *d) {
+  if (!g.mesh) return fail("no mesh");
+  d[0] = g.mesh->nl; d[1] = g.mesh->nod2D; d[2] = g.mesh->elem2D; d[3] = g.mesh->edge2D;
+  long long wc = g.mesh->wet_cells();
+  d[4] = (int)(wc & 0x7fffffff);
+  d[5] = (g.mesh->nl + 3) / 4 * 4;
+  return 0;
+}
+
+static bool mesh_field(const char *name, const std::vector<int> **vi, const std::vector<double> **vd) {
+  const MeshHost &m = *g.mesh;
+  *vi = nullptr;
+  *vd = nullptr;
+  std::string s = name ? name : "";
+  if (s == "coord") *vd = &m.coord;
+  else if (s == "elem_area") *vd = &m.elem_area;
+  else if (s == "area") *vd = &m.area;
+  else if (s == "areasvol") *vd = &m.areasvol;
+  else if (s == "edge_dxdy") *vd = &m.edge_dxdy;
+  else if (s == "edge_cross_dxdy") *vd = &m.edge_cross;
+  else if (s == "gradient_sca") *vd = &m.grad_sca;
+  else if (s == "hnode") *vd = &m.hnode;
+  else if (s == "hnode_new") *vd = &m.hnode_new;
+  else if (s == "helem") *vd = &m.helem;
+  else if (s == "zbar") *vd = &m.zbar;
+  else if (s == "elem2D_nodes") *vi = &m.elem_nodes;
+  else if (s == "edges") *vi = &m.edge_nodes;
+  else if (s == "edge_tri") *vi = &m.edge_tri;
+  else if (s == "nlevels") *vi = &m.nlev_elem;
+  else if (s == "nlevels_nod2D") *vi = &m.nlev_node;
+  else if (s == "nlevels_nod2D_min") *vi = &m.nlev_node_min;
+  else if (s == "edge_up_dn_tri") *vi = &m.up_dn_tri;
+  else if (s == "nboundary_lay") *vi = &m.nboundary_lay;
+  else if (s == "ring_num") *vi = &m.ring_ptr;
+  else return false;
+  return true;
+}
+
+long tracer_mesh_len(const char *name) {
+  if (!g.mesh) return -1;
+  const std::vector<int> *vi;
+  const std::vector<double> *vd;
+  if (!mesh_field(name, &vi, &vd)) return -1;
+  if (std::string(name) == "ring_num") return g.mesh->nod2D;
+  return vi ? (long)vi->size() : (long)vd->size();
+}
+
+int tracer_mesh_get_int(const char *name, int *out) {
+  if (!g.mesh) return fail("no mesh");
+  const std::vector<int> *vi;
+  const std::vector<double> *vd;
+  if (!mesh_field(name, &vi, &vd) || !vi) return fail(std::string("unknown integer mesh array ") + (name ? name : ""));
+  const std::string s(name);
+  if (s == "ring_num") {
+    for (int n = 0; n < g.mesh->nod2D; n++) out[n] = g.mesh->ring_ptr[n + 1] - g.mesh->ring_ptr[n];
+    return 0;
+  }
+  const bool index = (s == "elem2D_nodes" || s == "edges" || s == "edge_tri" || s == "edge_up_dn_tri");
+  for (size_t i = 0; i < vi->size(); i++) out[i] = index ? ((*vi)[i] >= 0 ? (*vi)[i] + 1 : 0) : (*vi)[i];
+  return 0;
+}
+
+int tracer_mesh_get_dbl(const char *name, double *out) {
+  if (!g.mesh) return fail("no mesh");
+  const std::vector<int> *vi;
+  const std::vector<double> *vd;
+  if (!mesh_field(name, &vi, &vd) || !vd) return fail(std::string("unknown real mesh array ") + (name ? name : ""));
+  std::memcpy(out, vd->data(), vd->size() * sizeof(double));
+  return 0;
+}
+
+int tracer_time_steps(int nsteps, double dt, float *ms) {
+  return guarded([&] {
+    if (check_ready()) return -1;
+    if (g.ntr < 1) return fail("no tracers allocated");
+    ensure_engine();
+    cudaStream_t s = (cudaStream_t)g.eng->stream();
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    g.eng->synchronize();
+    cudaEventRecord(a, s);
+    for (int i = 0; i < nsteps; i++) g.eng->step(dt, g.ab_refresh);
+    cudaEventRecord(b, s);
+    cudaEventSynchronize(b);
+    cudaEventElapsedTime(ms, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(cudaGetErrorString(e));
+    return 0;
+  });
+}
+
+int tracer_profile_steps(int nsteps, double dt, double *ms, const char **names, int nkinds, int *launches) {
+  return guarded([&] {
+    if (check_ready()) return -1;
+    if (g.ntr < 1) return fail("no tracers allocated");
+    ensure_engine();
+    int nk = 0;
+    const char *const *nm = Engine::kernel_kind_names(&nk);
+    if (names)
+      for (int k = 0; k < nkinds && k < nk; k++) names[k] = nm[k];
+    int l = g.eng->profile_steps(nsteps, dt, g.ab_refresh, ms, nkinds);
+    if (launches) *launches = l;
+    return 0;
+  });
+}
+
+int tracer_set_device(int device) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || device < 0 || device >= n)
+    return fail("invalid CUDA device " + std::to_string(device));
+  if (g.eng) return fail("tracer_set_device must come before the engine is created");
+  if (cudaSetDevice(device) != cudaSuccess) return fail("cudaSetDevice failed");
+  return 0;
+}
+
+int tracer_launches_per_step(void) {
+  if (!g.eng) return 0;
+  int n = 0;
+  for (int i = 0; i < g.ntr; i++) n += g.eng->launches_per_tracer_step(i);
+  return n;
+}
+
+long long tracer_device_bytes(void) { return g.eng ? (long long)g.eng->device_bytes() : 0; }
+
+const char *tracer_last_error(void) { return last_error(); }
+
+}  // extern "C"

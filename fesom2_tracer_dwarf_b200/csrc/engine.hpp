@@ -1,0 +1,74 @@
+// Tracer advection engine: owns the device copy of one mesh, its velocity
+// and any number of tracers, and advances them with the CUDA kernels.
+//
+// Host arrays cross this interface in the reference's Fortran layouts
+// (column-major, level fastest): tracers (nl-1, nod2D), uv (2, nl-1, elem2D),
+// w (nl, nod2D).  On the device every column is padded to a level stride S.
+#pragma once
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "mesh.hpp"
+
+namespace fesom {
+
+struct TracerScheme {
+  int hor = 0;      // 0 UPW1, 1 MUSCL, 2 MFCT
+  int ver = 0;      // 0 UPW1, 1 PPM, 2 QR4C, 3 CDIFF
+  int lim = 0;      // 0 NONE, 1 FCT
+  double ph = 1.0;  // tra_adv_ph
+  double pv = 1.0;  // tra_adv_pv
+};
+
+struct EngineImpl;
+
+class Engine {
+ public:
+  explicit Engine(const MeshHost &mesh);
+  ~Engine();
+  Engine(const Engine &) = delete;
+  Engine &operator=(const Engine &) = delete;
+
+  const MeshHost &mesh() const;
+  int level_stride() const;
+
+  void set_velocity(const double *uv, const double *w);
+  void set_velocity_zero();
+  // (Re)allocate ntr tracers, all zero, default scheme UPW1/UPW1/NONE.
+  void allocate_tracers(int ntr);
+  int num_tracers() const;
+  // values -> tracer id (0-based); valuesAB follows when also_ab.
+  void set_values(int id, const double *v, bool also_ab);
+  void set_values_ab(int id, const double *v);
+  void get_values(int id, double *out) const;
+  void set_scheme(int id, const TracerScheme &s);
+  TracerScheme scheme(int id) const;
+  // Advance every tracer one step.  refresh_ab: valuesAB := values first.
+  void step(double dt, bool refresh_ab);
+  // Advance one tracer one step (the reference's tracer_advect_step on id).
+  void step_tracer(int id, double dt, bool refresh_ab);
+  // Device pointers / stream for benchmarking and tests.
+  void *stream() const;
+  void synchronize() const;
+  // Kernel launches issued per step_tracer call with the tracer's scheme.
+  int launches_per_tracer_step(int id) const;
+  // min, max, sum and NaN count of tracer id over (nl-1, nod2D) incl. dry
+  // cells, in the reference's sequential order (src/fesom_analytic.F90:441-446).
+  void stats(int id, double out4[4]) const;
+  size_t device_bytes() const;
+  // Per-kernel device time: run nsteps steps of every tracer with a CUDA
+  // event pair around each launch and add the milliseconds of each kernel
+  // kind into ms[kind] (kinds: kernel_kind_names()).  Returns launches done.
+  int profile_steps(int nsteps, double dt, bool refresh_ab, double *ms, int nkinds);
+  static const char *const *kernel_kind_names(int *n);
+
+ private:
+  EngineImpl *p_;
+};
+
+// Last CUDA / engine error message of this thread ("" if none).
+const char *last_error();
+void set_last_error(const std::string &s);
+
+}  // namespace fesom

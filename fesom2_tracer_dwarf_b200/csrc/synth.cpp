@@ -1,0 +1,172 @@
+// Seeded synthetic inputs for the large analytic configurations: bathymetry,
+// a discretely consistent layered flow, and tracer fields.  All arithmetic is
+// host FP64; the generator is deterministic for a given seed.
+#include <algorithm>
+#include <cmath>
+#include <random>
+
+#include "mesh.hpp"
+
+namespace fesom {
+
+namespace {
+
+struct Rng {
+  std::mt19937_64 g;
+  explicit Rng(uint64_t s) : g(s) {}
+  double uni() { return (double)(g() >> 11) * 0x1.0p-53; }  // [0, 1)
+  double normal() {
+    double u1 = uni(), u2 = uni();
+    if (u1 < 1e-300) u1 = 1e-300;
+    return std::sqrt(-2.0 * std::log(u1)) * std::cos(2.0 * kPiRef * u2);
+  }
+};
+
+// Smooth field periodic on [0,Lx) x [0,Ly): a few Fourier modes with integer
+// wave numbers (so it is continuous across the periodic wrap).
+struct Modes {
+  int kx[6], ky[6];
+  double amp[6], ph[6];
+  void draw(Rng &r) {
+    for (int q = 0; q < 6; q++) {
+      kx[q] = 1 + (int)(r.g() % 4);
+      ky[q] = 1 + (int)(r.g() % 4);
+      amp[q] = 0.5 + r.uni();
+      ph[q] = 2.0 * kPiRef * r.uni();
+    }
+  }
+  double eval(double x, double y, double Lx, double Ly) const {
+    double s = 0.0;
+    for (int q = 0; q < 6; q++) s += amp[q] * std::sin(2.0 * kPiRef * (kx[q] * x / Lx + ky[q] * y / Ly) + ph[q]);
+    return s;
+  }
+};
+
+}  // namespace
+
+std::vector<int> synth_bathymetry(int nnodes, int nl, uint64_t seed) {
+  std::mt19937_64 g(seed);
+  std::vector<int> K(nnodes);
+  const uint64_t span = (uint64_t)(nl - 2);  // values 3..nl
+  for (int n = 0; n < nnodes; n++) K[n] = 3 + (int)(g() % span);
+  return K;
+}
+
+void synth_velocity(const MeshHost &m, uint64_t seed, double umax, double mode2_frac,
+                    std::vector<double> &uv, std::vector<double> &W) {
+  const int N = m.nod2D, T = m.elem2D, E = m.edge2D, nl = m.nl, L = nl - 1;
+  Rng rng(seed);
+  std::vector<double> xm(N), ym(N);
+  for (int n = 0; n < N; n++) { xm[n] = m.coord[2 * n] * kREarth; ym[n] = m.coord[2 * n + 1] * kREarth; }
+  // two smooth horizontal patterns per element: U1 = curl(psi1),
+  // U2 = curl(psi2) + grad(chi)
+  Modes p1, p2, chi;
+  p1.draw(rng);
+  p2.draw(rng);
+  chi.draw(rng);
+  std::vector<double> f1(N), f2(N), f3(N);
+  for (int n = 0; n < N; n++) {
+    f1[n] = p1.eval(xm[n], ym[n], m.Lx, m.Ly);
+    f2[n] = p2.eval(xm[n], ym[n], m.Lx, m.Ly);
+    f3[n] = chi.eval(xm[n], ym[n], m.Lx, m.Ly);
+  }
+  uv.assign((size_t)2 * L * T, 0.0);
+  for (int e = 0; e < T; e++) {
+    const int *en = &m.elem_nodes[3 * e];
+    const double *gs = &m.grad_sca[6 * e];
+    auto gx = [&](const std::vector<double> &f) { return gs[0] * f[en[0]] + gs[1] * f[en[1]] + gs[2] * f[en[2]]; };
+    auto gy = [&](const std::vector<double> &f) { return gs[3] * f[en[0]] + gs[4] * f[en[1]] + gs[5] * f[en[2]]; };
+    const double u1 = -gy(f1), v1 = gx(f1);
+    const double u2 = -gy(f2) + gx(f3), v2 = gx(f2) + gy(f3);
+    // vertical modes with zero mean over the element's own water column, so
+    // the column integral of every edge flux vanishes
+    const int M = m.nlev_elem[e] - 1;
+    for (int k = 0; k < M; k++) {
+      const double a1 = std::cos(kPiRef * ((double)k + 0.5) / (double)M);
+      const double a2 = mode2_frac * std::cos(2.0 * kPiRef * ((double)k + 0.5) / (double)M);
+      uv[2 * ((size_t)e * L + k)] = a1 * u1 + a2 * u2;
+      uv[2 * ((size_t)e * L + k) + 1] = a1 * v1 + a2 * v2;
+    }
+  }
+  double vmax = 0.0;
+  for (size_t i = 0; i < uv.size() / 2; i++) vmax = std::max(vmax, std::hypot(uv[2 * i], uv[2 * i + 1]));
+  const double scale = vmax > 0.0 ? umax / vmax : 0.0;
+  for (double &v : uv) v *= scale;
+
+  // horizontal divergence D(n,k) of the edge volume fluxes, with the same
+  // segment rule the advection kernels use
+  std::vector<double> D((size_t)L * N, 0.0);
+  for (int e = 0; e < E; e++) {
+    const int n1 = m.edge_nodes[2 * e], n2 = m.edge_nodes[2 * e + 1];
+    const int t1 = m.edge_tri[2 * e], t2 = m.edge_tri[2 * e + 1];
+    const int nl1 = m.nlev_elem[t1] - 1, nl2 = t2 >= 0 ? m.nlev_elem[t2] - 1 : 0;
+    const double *c = &m.edge_cross[4 * e];
+    for (int k = 0; k < std::max(nl1, nl2); k++) {
+      double v = 0.0;
+      if (k < nl1) v += (-uv[2 * ((size_t)t1 * L + k) + 1] * c[0] + uv[2 * ((size_t)t1 * L + k)] * c[1]) * m.helem[(size_t)t1 * L + k];
+      if (k < nl2) v += (uv[2 * ((size_t)t2 * L + k) + 1] * c[2] - uv[2 * ((size_t)t2 * L + k)] * c[3]) * m.helem[(size_t)t2 * L + k];
+      D[(size_t)n1 * L + k] += v;
+      D[(size_t)n2 * L + k] -= v;
+    }
+  }
+  // W from bottom to top: W(k) A(k) = W(k+1) A(k+1) - D(k); W = 0 at the
+  // bottom and at the surface
+  W.assign((size_t)nl * N, 0.0);
+  for (int n = 0; n < N; n++) {
+    const int nlev = m.nlev_node[n];
+    for (int i = nlev - 1; i >= 2; i--) {  // 1-based interface i, top of layer i
+      const double Ai = m.area[(size_t)n * nl + i - 1], Ai1 = m.area[(size_t)n * nl + i];
+      const double flux_below = W[(size_t)n * nl + i] * Ai1;
+      W[(size_t)n * nl + i - 1] = Ai > 0.0 ? (flux_below - D[(size_t)n * L + i - 1]) / Ai : 0.0;
+    }
+    W[(size_t)n * nl + 0] = 0.0;
+  }
+}
+
+void synth_tracer(const MeshHost &m, uint64_t seed, int kind, std::vector<double> &T) {
+  const int N = m.nod2D, L = m.nl - 1;
+  Rng r(seed);
+  T.assign((size_t)L * N, 0.0);
+  if (kind == 0) {
+    double bx[8], by[8], bs[8], ba[8];
+    for (int b = 0; b < 8; b++) {
+      bx[b] = r.uni() * m.Lx; by[b] = r.uni() * m.Ly;
+      bs[b] = (0.03 + 0.07 * r.uni()) * m.Lx; ba[b] = 5.0 + 10.0 * r.uni();
+    }
+    for (int n = 0; n < N; n++) {
+      const double x = m.coord[2 * n] * kREarth, y = m.coord[2 * n + 1] * kREarth;
+      double blob = 0.0;
+      for (int b = 0; b < 8; b++) {
+        double dx = std::fabs(x - bx[b]), dy = std::fabs(y - by[b]);
+        if (m.periodic) { dx = std::min(dx, m.Lx - dx); dy = std::min(dy, m.Ly - dy); }
+        blob += ba[b] * std::exp(-(dx * dx + dy * dy) / (bs[b] * bs[b]));
+      }
+      for (int k = 0; k < m.nlev_node[n] - 1; k++) T[(size_t)n * L + k] = 20.0 * r.uni() + blob;
+    }
+  } else {
+    for (int n = 0; n < N; n++)
+      for (int k = 0; k < m.nlev_node[n] - 1; k++) T[(size_t)n * L + k] = 35.0 + 0.5 * r.normal();
+  }
+}
+
+void analytic_driver_fields(const MeshHost &m, std::vector<double> &T, std::vector<double> &S,
+                            std::vector<double> &uv, std::vector<double> &W) {
+  const int N = m.nod2D, nz = m.nl - 1;
+  const double Lx = m.Lx, Ly = m.Ly, xc = 0.5 * Lx, yc = 0.5 * Ly;
+  T.assign((size_t)nz * N, 0.0);
+  S.assign((size_t)nz * N, 0.0);
+  for (int n = 0; n < N; n++) {
+    const double xn = m.coord[2 * n] * kREarth, yn = m.coord[2 * n + 1] * kREarth;
+    const double r = std::sqrt((xn - xc) * (xn - xc) + (yn - yc) * (yn - yc));
+    for (int k = 1; k <= nz; k++) {
+      const double zn = (double)(k - 1) / (double)(nz - 1);
+      T[(size_t)n * nz + k - 1] = 15.0 + 5.0 * std::sin(2.0 * kPiRef * xn / Lx) * std::cos(2.0 * kPiRef * yn / Ly) - 10.0 * zn;
+      S[(size_t)n * nz + k - 1] = 34.0 + 2.0 * std::exp(-(r * r) / ((0.1 * Lx) * (0.1 * Lx))) * (1.0 - zn);
+    }
+  }
+  uv.assign((size_t)2 * nz * m.elem2D, 0.0);
+  for (size_t i = 0; i < (size_t)nz * m.elem2D; i++) uv[2 * i] = 0.1;
+  W.assign((size_t)m.nl * N, 0.0);
+}
+
+}  // namespace fesom

@@ -1,0 +1,175 @@
+"""Python host of the B200 tracer advection library.
+
+``FESOMTracerAdvection`` keeps the method names, arguments and return values
+of the reference's ctypes wrapper (python/demo_tracer.py:40-208 in
+suvarchal/fesom2_tracer_dwarf) and adds the analytic-mesh, scheme, velocity
+and multi-tracer calls of include/fesom_tracer.h.  Arrays are numpy float64 in
+Fortran order, shaped like the reference's: tracers (nl-1, nod2D), element
+velocity (2, nl-1, elem2D), vertical velocity (nl, nod2D).
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _lib
+
+
+_INT_MESH_ARRAYS = {"elem2D_nodes", "edges", "edge_tri", "nlevels", "nlevels_nod2D", "nlevels_nod2D_min",
+                    "edge_up_dn_tri", "nboundary_lay", "ring_num"}
+
+
+def _f64(a, shape):
+    a = np.asfortranarray(np.asarray(a, dtype=np.float64))
+    if a.shape != tuple(shape):
+        raise ValueError(f"expected shape {tuple(shape)}, got {a.shape}")
+    return a
+
+
+class FESOMTracerAdvection:
+    """Drop-in for the reference's FESOMTracerAdvection, backed by sm_100a kernels."""
+
+    def __init__(self, lib_path=None):
+        self.lib = _lib.load(lib_path)
+
+    # ---- methods of python/demo_tracer.py ---------------------------------
+    def initialize_mpi(self, mpi_comm=0):
+        return self.lib.tracer_init_mpi(mpi_comm)
+
+    def initialize(self, restart_path="./fesom_bin_restart"):
+        return self.lib.tracer_init(restart_path.encode())
+
+    def advect_step(self, dt=1.0e-3):
+        return self.lib.tracer_advect_step(dt)
+
+    def get_tracer_values(self, tracer_id=1):
+        nz, nn = ctypes.c_int(), ctypes.c_int()
+        ret = self.lib.tracer_get_size(ctypes.byref(nz), ctypes.byref(nn))
+        if ret != 0:
+            raise RuntimeError(f"tracer_get_size failed with code {ret}")
+        values = np.zeros((nz.value, nn.value), dtype=np.float64, order="F")
+        ret = self.lib.tracer_get_values_id(tracer_id, _lib.ptr(values), nz, nn)
+        if ret != 0:
+            raise RuntimeError(f"tracer_get_values failed with code {ret}")
+        return values
+
+    def get_statistics(self, tracer_id=1):
+        s = np.zeros(4)
+        ret = self.lib.tracer_get_stats_id(tracer_id, _lib.ptr(s))
+        if ret != 0:
+            raise RuntimeError(f"tracer_get_stats failed with code {ret}")
+        return {"min": s[0], "max": s[1], "sum": s[2], "nan": int(s[3])}
+
+    def finalize(self, output_path="./fesom_bin_restart"):
+        return self.lib.tracer_finalize(output_path.encode())
+
+    def finalize_mpi(self):
+        return self.lib.tracer_finalize_mpi()
+
+    # ---- extensions ---------------------------------------------------------
+    def init_analytic(self, nx, ny, nl, Lx=1.0e5, Ly=1.0e5, max_depth=1000.0, periodic=True,
+                      full_rings=True, node_K=None):
+        """Analytic mesh of the reference's generate_analytic_mesh (+ optional bathymetry)."""
+        K = None
+        if node_K is not None:
+            K = np.ascontiguousarray(node_K, dtype=np.int32)
+            if K.size != self.lib.tracer_analytic_nodes(nx, ny, int(periodic)):
+                raise ValueError("node_K must have one entry per mesh node")
+        rc = self.lib.tracer_init_analytic(nx, ny, nl, Lx, Ly, max_depth, int(periodic), int(full_rings),
+                                           _lib.ptr(K))
+        _lib.check(self.lib, rc, "tracer_init_analytic")
+        self.dims = self.mesh_dims()
+        return rc
+
+    def mesh_dims(self):
+        d = np.zeros(6, dtype=np.int32)
+        _lib.check(self.lib, self.lib.tracer_mesh_dims(_lib.ptr(d)), "tracer_mesh_dims")
+        return {"nl": int(d[0]), "nod2D": int(d[1]), "elem2D": int(d[2]), "edge2D": int(d[3]),
+                "level_stride": int(d[5])}
+
+    def allocate_tracers(self, num_tracers, ab_order=2):
+        d = self.mesh_dims()
+        _lib.check(self.lib, self.lib.tracer_allocate_tracers(num_tracers, d["nl"], d["nod2D"], ab_order),
+                   "tracer_allocate_tracers")
+
+    def set_values(self, tracer_id, values, values_ab=None):
+        d = self.mesh_dims()
+        v = _f64(values, (d["nl"] - 1, d["nod2D"]))
+        _lib.check(self.lib, self.lib.tracer_set_values(tracer_id, _lib.ptr(v), d["nl"], d["nod2D"]),
+                   "tracer_set_values")
+        if values_ab is not None:
+            a = _f64(values_ab, (d["nl"] - 1, d["nod2D"]))
+            _lib.check(self.lib, self.lib.tracer_set_values_ab(tracer_id, _lib.ptr(a), d["nl"], d["nod2D"]),
+                       "tracer_set_values_ab")
+
+    def set_scheme(self, tracer_id, hor="MUSCL", ver="PPM", lim="FCT", ph=1.0, pv=1.0):
+        rc = self.lib.tracer_set_scheme(tracer_id, hor.encode(), ver.encode(), lim.encode(), ph, pv)
+        _lib.check(self.lib, rc, "tracer_set_scheme")
+
+    def set_velocity(self, uv, w):
+        """uv (2, nl-1, elem2D) element velocity, w (nl, nod2D)."""
+        d = self.mesh_dims()
+        u = _f64(uv, (2, d["nl"] - 1, d["elem2D"]))
+        ww = _f64(w, (d["nl"], d["nod2D"]))
+        rc = self.lib.tracer_set_velocity_elem(_lib.ptr(u), _lib.ptr(ww), d["nl"], d["nod2D"], d["elem2D"])
+        _lib.check(self.lib, rc, "tracer_set_velocity_elem")
+
+    def set_ab_refresh(self, on):
+        self.lib.tracer_set_ab_refresh(int(bool(on)))
+
+    def advect_steps(self, nsteps, dt):
+        _lib.check(self.lib, self.lib.tracer_advect_steps(nsteps, dt), "tracer_advect_steps")
+
+    def analytic_fields(self):
+        """T, S, uv, w of the analytic driver (src/fesom_analytic.F90:251-331)."""
+        d = self.mesh_dims()
+        L, N, T = d["nl"] - 1, d["nod2D"], d["elem2D"]
+        Tt = np.zeros((L, N), order="F")
+        S = np.zeros((L, N), order="F")
+        uv = np.zeros((2, L, T), order="F")
+        w = np.zeros((d["nl"], N), order="F")
+        _lib.check(self.lib, self.lib.tracer_analytic_fields(_lib.ptr(Tt), _lib.ptr(S), _lib.ptr(uv), _lib.ptr(w)),
+                   "tracer_analytic_fields")
+        return Tt, S, uv, w
+
+    def synth_velocity(self, seed=0, umax=1.0, mode2=0.5):
+        d = self.mesh_dims()
+        uv = np.zeros((2, d["nl"] - 1, d["elem2D"]), order="F")
+        w = np.zeros((d["nl"], d["nod2D"]), order="F")
+        _lib.check(self.lib, self.lib.tracer_synth_velocity(seed, umax, mode2, _lib.ptr(uv), _lib.ptr(w)),
+                   "tracer_synth_velocity")
+        return uv, w
+
+    def synth_tracer(self, seed=0, kind=0):
+        d = self.mesh_dims()
+        v = np.zeros((d["nl"] - 1, d["nod2D"]), order="F")
+        _lib.check(self.lib, self.lib.tracer_synth_tracer(seed, kind, _lib.ptr(v)), "tracer_synth_tracer")
+        return v
+
+    def mesh_array(self, name):
+        n = self.lib.tracer_mesh_len(name.encode())
+        if n < 0:
+            raise KeyError(name)
+        if name in _INT_MESH_ARRAYS:
+            out = np.zeros(n, dtype=np.int32)
+            _lib.check(self.lib, self.lib.tracer_mesh_get_int(name.encode(), _lib.ptr(out)), "tracer_mesh_get_int")
+            return out
+        out = np.zeros(n, dtype=np.float64)
+        _lib.check(self.lib, self.lib.tracer_mesh_get_dbl(name.encode(), _lib.ptr(out)), "tracer_mesh_get_dbl")
+        return out
+
+    def time_steps(self, nsteps, dt):
+        ms = ctypes.c_float()
+        _lib.check(self.lib, self.lib.tracer_time_steps(nsteps, dt, ctypes.byref(ms)), "tracer_time_steps")
+        return ms.value
+
+    def cleanup(self):
+        return self.lib.tracer_cleanup()
+
+
+def synth_bathymetry(nnodes, nl, seed=0):
+    lib = _lib.load()
+    K = np.zeros(nnodes, dtype=np.int32)
+    _lib.check(lib, lib.tracer_synth_bathymetry(nnodes, nl, seed, _lib.ptr(K)), "tracer_synth_bathymetry")
+    return K

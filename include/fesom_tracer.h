@@ -1,0 +1,168 @@
+/*
+ * fesom_tracer.h -- C ABI of libfesom_tracer.so, the B200 (sm_100a) tracer
+ * advection library.
+ *
+ * The first group of entry points keeps the names, argument meaning, value /
+ * pointer passing and return convention (0 = success, -1 = not initialised,
+ * bad id or unsupported input, message on stderr prefixed "### error:") of the
+ * reference's Fortran bind(C) interface, lib/tracer_c_interface.F90 in
+ * suvarchal/fesom2_tracer_dwarf; each declaration cites the function it
+ * replaces.  Arrays are Fortran column-major doubles, copied in and out, never
+ * aliased.  One global instance, not thread-safe, as in the reference.
+ *
+ * Behaviour that differs from the reference on purpose (reference bugs):
+ *  - tracer_advect_step advances every allocated tracer (the reference
+ *    advanced tracer 1 only, lib/tracer_c_interface.F90:188-190,210) and
+ *    zeroes the tendency each step (the reference accumulated del_ttf,
+ *    :177-203);
+ *  - w is used as w, w_i and w_e (use_wsplit = .false.); the reference's
+ *    array path left w_e zero and sized by edges (:711-712);
+ *  - tracer_set_velocity reads uv as (nl-1, n, 2) with n the number of
+ *    ELEMENTS, the mesh entity velocity lives on; the reference allocated it
+ *    by edges and the kernels then read it as (2, nl-1, elem) (:694-725).
+ * Restart files (tracer_init, tracer_finalize, tracer_run_workflow,
+ * tracer_load_mesh_partition) and the ASCII mesh reader
+ * (tracer_load_mesh_from_files) are not provided by this build: they return
+ * -1 with a message.  Meshes come from tracer_init_analytic or
+ * tracer_set_mesh_arrays.
+ */
+#ifndef FESOM_TRACER_H
+#define FESOM_TRACER_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- reference interface (lib/tracer_c_interface.F90) ------------------ */
+
+/* :46 tracer_init_mpi -- no MPI in a one-GPU build; always 0. */
+int tracer_init_mpi(int mpi_comm);
+/* :89 tracer_finalize_mpi -- always 0. */
+int tracer_finalize_mpi(void);
+/* :113 tracer_init -- binary restarts are not supported: -1. */
+int tracer_init(const char *restart_dir);
+/* :163 tracer_advect_step -- one step of every tracer. */
+int tracer_advect_step(double dt);
+/* :228 tracer_get_stats -- min, max, sum of tracer 1 over (nl-1, nod2D). */
+int tracer_get_stats(double *tmin, double *tmax, double *tsum);
+/* :255 tracer_get_size -- nz = nl-1, nn = nod2D. */
+int tracer_get_size(int *nz, int *nn);
+/* :280 tracer_get_values -- tracer 1 into values(nz, nn). */
+int tracer_get_values(double *values, int nz, int nn);
+/* :308 tracer_finalize -- restart output is not supported: -1. */
+int tracer_finalize(const char *output_dir);
+/* :356 tracer_run_workflow -- needs restart input: -1. */
+int tracer_run_workflow(const char *restart_dir, int nsteps, double dt);
+/* :391 tracer_cleanup -- releases every host and device resource. */
+int tracer_cleanup(void);
+/* :415 tracer_set_mesh_dims */
+int tracer_set_mesh_dims(int nl, int nod2D, int edge2D, int elem2D);
+/* :441 tracer_set_levels -- nlevels_nod2D and ulevels_nod2D (ulevels must be 1). */
+int tracer_set_levels(const int *nlevels, const int *ulevels, int nod2D);
+/* :477 tracer_set_thickness -- hnode_new(nl-1, nod2D). */
+int tracer_set_thickness(const double *hnode, int nl, int nod2D);
+/* :510 tracer_set_partition -- one GPU: eDim_nod2D must be 0. */
+int tracer_set_partition(int myDim_nod2D, int eDim_nod2D);
+/* :539 tracer_allocate_tracers -- defaults UPW1/UPW1/NONE, ph = pv = 1. */
+int tracer_allocate_tracers(int num_tracers, int nl, int nod2D, int AB_order);
+/* :613 tracer_set_values -- values, valuesAB (and valuesold) of one tracer. */
+int tracer_set_values(int tracer_id, const double *values, int nl, int nod2D);
+/* :652 tracer_set_velocity_zero */
+int tracer_set_velocity_zero(int nl, int nod2D, int edge2D);
+/* :694 tracer_set_velocity -- uv(nl-1, elem2D, 2), w(nl, nod2D). */
+int tracer_set_velocity(const double *uv, const double *w, int nl, int nod2D, int nelem);
+/* :749 tracer_init_complete */
+int tracer_init_complete(void);
+/* :769 tracer_load_mesh_partition -- binary restarts are not supported: -1. */
+int tracer_load_mesh_partition(const char *restart_dir);
+/* :830 tracer_load_mesh_from_files -- the ASCII mesh reader is not part of this build: -1. */
+int tracer_load_mesh_from_files(const char *mesh_path);
+/* :875 tracer_init_ale_arrays -- hnode = hnode_new = zbar(k)-zbar(k+1). */
+int tracer_init_ale_arrays(void);
+/* :931 tracer_init_for_advection -- allocates the device state. */
+int tracer_init_for_advection(void);
+
+/* ---- additive extensions ------------------------------------------------ */
+
+/* Analytic mesh of lib/analytic_mesh.F90:114 (generate_analytic_mesh) with
+ * the ALE arrays of src/fesom_analytic.F90:206-244.  node_K (nullable,
+ * length nod2D) is a per-node bottom level index in [3, nl].  full_rings = 0
+ * keeps the reference's incomplete periodic nod_in_elem2D lists. */
+int tracer_init_analytic(int nx, int ny, int nl, double Lx, double Ly, double max_depth,
+                         int periodic, int full_rings, const int *node_K);
+/* Number of nodes of the analytic mesh (nx, ny, periodic). */
+int tracer_analytic_nodes(int nx, int ny, int periodic);
+/* Generic mesh from arrays (1-based Fortran indices, 0 = no element):
+ * elem2D_nodes(3, elem2D), edges(2, edge2D), edge_tri(2, edge2D),
+ * nlevels(elem2D), nlevels_nod2D(nod2D), nod_in_elem2D given by
+ * ring_num(nod2D) and ring(max_ring, nod2D), elem_area(elem2D),
+ * area(nl, nod2D), areasvol(nl, nod2D), edge_dxdy(2, edge2D),
+ * edge_cross_dxdy(4, edge2D), gradient_sca(6, elem2D), elem_cos(elem2D),
+ * zbar(nl), hnode(nl-1, nod2D), hnode_new(nl-1, nod2D), helem(nl-1, elem2D),
+ * coord_nod2D(2, nod2D) (radians).  Up/down-wind triangles, nboundary_lay and
+ * the edge tables are derived.  Lx, Ly > 0 mark a doubly periodic domain. */
+int tracer_set_mesh_arrays(int nl, int nod2D, int elem2D, int edge2D, int max_ring,
+                           const int *elem2D_nodes, const int *edges, const int *edge_tri,
+                           const int *nlevels, const int *nlevels_nod2D, const int *ring_num,
+                           const int *ring, const double *elem_area, const double *area,
+                           const double *areasvol, const double *edge_dxdy,
+                           const double *edge_cross_dxdy, const double *gradient_sca,
+                           const double *elem_cos, const double *zbar, const double *hnode,
+                           const double *hnode_new, const double *helem,
+                           const double *coord_nod2D, double Lx, double Ly);
+/* Per-tracer schemes, as the strings of lib/MOD_TRACER.F90:18-20:
+ * hor "UPW1"|"MUSCL"|"MFCT", ver "UPW1"|"PPM"|"QR4C"|"CDIFF", lim "NONE"|"FCT". */
+int tracer_set_scheme(int tracer_id, const char *hor, const char *ver, const char *lim,
+                      double ph, double pv);
+/* Element velocity in the kernels' own layout uv(2, nl-1, elem2D), w(nl, nod2D). */
+int tracer_set_velocity_elem(const double *uv, const double *w, int nl, int nod2D, int elem2D);
+/* valuesAB of one tracer (the field the high-order fluxes are built from). */
+int tracer_set_values_ab(int tracer_id, const double *values, int nl, int nod2D);
+/* 1: valuesAB := values before every step; 0 (default, as the reference
+ * drivers): valuesAB stays as set. */
+int tracer_set_ab_refresh(int on);
+/* nsteps steps of every tracer. */
+int tracer_advect_steps(int nsteps, double dt);
+/* Values / stats of tracer tracer_id (1-based). stats4 = min, max, sum, nan. */
+int tracer_get_values_id(int tracer_id, double *values, int nz, int nn);
+int tracer_get_stats_id(int tracer_id, double *stats4);
+/* Fields of the analytic driver for the current analytic mesh:
+ * T, S (nl-1, nod2D), uv (2, nl-1, elem2D), w (nl, nod2D); any may be NULL. */
+int tracer_analytic_fields(double *T, double *S, double *uv, double *w);
+/* Seeded synthetic inputs: bathymetry K(nnodes) in [3, nl]; a layered flow
+ * for the current mesh; a tracer field (kind 0 temperature-like, 1
+ * salinity-like). */
+int tracer_synth_bathymetry(int nnodes, int nl, uint64_t seed, int *K);
+int tracer_synth_velocity(uint64_t seed, double umax, double mode2_frac, double *uv, double *w);
+int tracer_synth_tracer(uint64_t seed, int kind, double *values);
+/* Mesh sizes: nl, nod2D, elem2D, edge2D, wet cells (low 31 bits), level stride. */
+int tracer_mesh_dims(int *dims6);
+/* Copy a named mesh array out in the reference's layout (1-based indices):
+ * int: "elem2D_nodes", "edges", "edge_tri", "nlevels", "nlevels_nod2D",
+ * "nlevels_nod2D_min", "edge_up_dn_tri", "nboundary_lay", "ring_num";
+ * double: "coord", "elem_area", "area", "areasvol", "edge_dxdy",
+ * "edge_cross_dxdy", "gradient_sca", "hnode", "hnode_new", "helem", "zbar". */
+long tracer_mesh_len(const char *name);
+int tracer_mesh_get_int(const char *name, int *out);
+int tracer_mesh_get_dbl(const char *name, double *out);
+/* Device time of nsteps steps of every tracer, CUDA events on the engine's
+ * stream (inputs already resident). */
+int tracer_time_steps(int nsteps, double dt, float *ms);
+/* Per-kernel device time over nsteps steps (an event pair around every
+ * launch): ms[kind] summed per kernel kind, names[kind] its name (up to
+ * nkinds entries); *launches = kernel launches issued. */
+int tracer_profile_steps(int nsteps, double dt, double *ms, const char **names, int nkinds, int *launches);
+/* CUDA device the engine runs on (before the first step; default 0). */
+int tracer_set_device(int device);
+/* Number of kernel launches one tracer_advect_step issues. */
+int tracer_launches_per_step(void);
+/* Device memory held by the engine, in bytes. */
+long long tracer_device_bytes(void);
+/* Last error message of this thread ("" if none). */
+const char *tracer_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,136 @@
+"""ctypes wrapper of the CPU oracle (oracle/fesom_oracle.c).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
+CPU-baseline leg of bench.py to check / time against the reference algorithm.
+The product library never loads it.
+"""
+from __future__ import annotations
+
+import ctypes
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+SERIAL = HERE / "_build" / "libfesom_oracle.so"
+OPENMP = HERE / "_build" / "libfesom_oracle_omp.so"
+
+HOR = {"UPW1": 0, "MUSCL": 1, "MFCT": 2}
+VER = {"UPW1": 0, "PPM": 1, "QR4C": 2, "CDIFF": 3}
+LIM = {"NONE": 0, "FCT": 1}
+
+_INT_FIELDS = {"elem2D_nodes", "edges", "edge_tri", "nlevels", "ulevels", "nlevels_nod2D", "ulevels_nod2D",
+               "nlevels_nod2D_min", "ulevels_nod2D_max", "nod_in_elem2D_num", "nod_in_elem2D",
+               "edge_up_dn_tri", "nboundary_lay"}
+
+
+def build() -> None:
+    """Compile both oracle flavours (make -C oracle)."""
+    subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+
+
+class Oracle:
+    def __init__(self, openmp: bool = False):
+        path = OPENMP if openmp else SERIAL
+        if not path.exists():
+            build()
+        lib = ctypes.CDLL(str(path))
+        vp, ci, cd = ctypes.c_void_p, ctypes.c_int, ctypes.c_double
+        lib.om_mesh_analytic.restype = vp
+        lib.om_mesh_analytic.argtypes = [ci, ci, ci, cd, cd, cd, ci, ci, vp]
+        lib.om_mesh_free.argtypes = [vp]
+        lib.om_mesh_dims.argtypes = [vp, vp]
+        lib.om_mesh_len.restype = ctypes.c_long
+        lib.om_mesh_len.argtypes = [vp, ctypes.c_char_p]
+        lib.om_mesh_get_int.argtypes = [vp, ctypes.c_char_p, vp]
+        lib.om_mesh_get_dbl.argtypes = [vp, ctypes.c_char_p, vp]
+        lib.om_analytic_fields.argtypes = [vp] * 5
+        lib.om_tracer_step.argtypes = [vp, ci, ci, ci, cd, cd, cd] + [vp] * 7
+        lib.om_run.argtypes = [vp, ci, ci, ci, cd, cd, cd, vp, vp, ci, ci, vp, vp, ci]
+        lib.om_stats.argtypes = [vp, vp, vp]
+        lib.om_set_threads.argtypes = [ci]
+        lib.om_get_threads.restype = ci
+        self.lib = lib
+
+    def set_threads(self, n: int) -> None:
+        self.lib.om_set_threads(n)
+
+    def threads(self) -> int:
+        return self.lib.om_get_threads()
+
+
+class OracleMesh:
+    """An analytic mesh built by the oracle (lib/analytic_mesh.F90 restated)."""
+
+    def __init__(self, oracle: Oracle, nx, ny, nl, Lx=1.0e5, Ly=1.0e5, max_depth=1000.0, periodic=True,
+                 full_rings=True, node_K=None):
+        self.o = oracle
+        K = None if node_K is None else np.ascontiguousarray(node_K, dtype=np.int32)
+        h = oracle.lib.om_mesh_analytic(nx, ny, nl, Lx, Ly, max_depth, int(periodic), int(full_rings), _p(K))
+        if not h:
+            raise ValueError("oracle mesh construction failed")
+        self.h = ctypes.c_void_p(h)
+        d = np.zeros(6, dtype=np.int32)
+        oracle.lib.om_mesh_dims(self.h, _p(d))
+        self.nl, self.nod2D, self.elem2D, self.edge2D, self.max_nie = (int(x) for x in d[:5])
+
+    def __del__(self):
+        try:
+            self.o.lib.om_mesh_free(self.h)
+        except Exception:
+            pass
+
+    def array(self, name: str) -> np.ndarray:
+        n = self.o.lib.om_mesh_len(self.h, name.encode())
+        if n < 0:
+            raise KeyError(name)
+        if name in _INT_FIELDS:
+            a = np.zeros(n, dtype=np.int32)
+            self.o.lib.om_mesh_get_int(self.h, name.encode(), _p(a))
+        else:
+            a = np.zeros(n, dtype=np.float64)
+            self.o.lib.om_mesh_get_dbl(self.h, name.encode(), _p(a))
+        return a
+
+    def shape_tracer(self):
+        return (self.nl - 1, self.nod2D)
+
+    def analytic_fields(self):
+        L, N, T = self.nl - 1, self.nod2D, self.elem2D
+        Tt = np.zeros((L, N), order="F")
+        S = np.zeros((L, N), order="F")
+        uv = np.zeros((2, L, T), order="F")
+        w = np.zeros((self.nl, N), order="F")
+        self.o.lib.om_analytic_fields(self.h, _p(Tt), _p(S), _p(uv), _p(w))
+        return Tt, S, uv, w
+
+    def step(self, values, values_ab, uv, w, dt, hor="MUSCL", ver="PPM", lim="FCT", ph=1.0, pv=1.0,
+             want_terms=False):
+        """One oracle step; values updated in place (Fortran-ordered float64)."""
+        for a in (values, values_ab, uv, w):
+            assert a.dtype == np.float64 and a.flags["F_CONTIGUOUS"]
+        dh = dv = lo = None
+        if want_terms:
+            dh = np.zeros(self.shape_tracer(), order="F")
+            dv = np.zeros(self.shape_tracer(), order="F")
+            lo = np.zeros(self.shape_tracer(), order="F")
+        self.o.lib.om_tracer_step(self.h, HOR[hor], VER[ver], LIM[lim], ph, pv, dt, _p(uv), _p(w), _p(values),
+                                  _p(values_ab), _p(dh), _p(dv), _p(lo))
+        return (dh, dv, lo) if want_terms else None
+
+    def run(self, values, values_ab, uv, w, dt, nsteps, hor="MUSCL", ver="PPM", lim="FCT", ph=1.0, pv=1.0,
+            refresh_ab=True):
+        """nsteps steps of ntracers = values.shape[0] tracers stacked as (ntr, nl-1, nod2D)."""
+        ntr = values.shape[0]
+        self.o.lib.om_run(self.h, HOR[hor], VER[ver], LIM[lim], ph, pv, dt, _p(uv), _p(w), ntr, nsteps,
+                          _p(values), _p(values_ab), int(refresh_ab))
+
+    def stats(self, values):
+        s = np.zeros(4)
+        self.o.lib.om_stats(self.h, _p(np.asfortranarray(values)), _p(s))
+        return s

@@ -1,0 +1,152 @@
+"""The CPU oracle against the reference's published numbers and the
+invariants that pin the schemes no reference test covers."""
+import json
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import pyoracle
+
+GOLDEN = Path(__file__).resolve().parent / "golden"
+
+
+def fmt_e(x, w, d):
+    """Fortran Ew.d rendering, as the analytic driver prints (src/fesom_analytic.F90:446-447)."""
+    s = f"{x:.{d - 1}E}"          # d significant digits
+    mant, exp = s.split("E")
+    digits = mant.replace("-", "").replace(".", "")
+    e = int(exp) + 1
+    sign = "-" if x < 0 else ""
+    return f"{sign}0.{digits}E{e:+03d}".rjust(w)
+
+
+def test_upw1_golden_readme(oracle):
+    """UPW1/UPW1/NONE on the 20x20x10 periodic mesh reproduces README.md:51-52."""
+    gold = json.loads((GOLDEN / "readme_upw1.json").read_text())
+    m = pyoracle.OracleMesh(oracle, 20, 20, 10, periodic=True, full_rings=False)
+    T, S, uv, w = m.analytic_fields()
+    TAB = T.copy(order="F")
+    for rec in gold["steps"]:
+        m.step(T, TAB, uv, w, 1000.0, "UPW1", "UPW1", "NONE")
+        mn, mx, sm, nan = m.stats(T)
+        assert fmt_e(mn, 14, 6) == rec["min"].rjust(14)
+        assert fmt_e(mx, 14, 6) == rec["max"].rjust(14)
+        assert fmt_e(sm, 18, 10) == rec["sum"].rjust(18)
+        assert nan == 0
+
+
+def test_upw1_golden_all_steps_sum_conserved(oracle):
+    """Sum conserved at 0.3249000000E+05 with 0 NaN at every step (CLAUDE.md:13)."""
+    m = pyoracle.OracleMesh(oracle, 20, 20, 10, periodic=True, full_rings=False)
+    T, S, uv, w = m.analytic_fields()
+    TAB = T.copy(order="F")
+    for _ in range(10):
+        m.step(T, TAB, uv, w, 1000.0, "UPW1", "UPW1", "NONE")
+        mn, mx, sm, nan = m.stats(T)
+        assert fmt_e(sm, 18, 10).strip() == "0.3249000000E+05"
+        assert nan == 0
+
+
+def test_fixture_regression(oracle):
+    """Committed MUSCL/PPM/FCT fixture of the 20x20x10 analytic run (made by
+    tests/golden/make_fixtures.py) still reproduces bit for bit."""
+    data = np.load(GOLDEN / "c1_muscl_ppm_fct.npz")
+    m = pyoracle.OracleMesh(oracle, 20, 20, 10, periodic=True, full_rings=False)
+    T, S, uv, w = m.analytic_fields()
+    TAB = T.copy(order="F")
+    for step in range(int(data["nsteps"])):
+        m.step(T, TAB, uv, w, 1000.0, "MUSCL", "PPM", "FCT")
+    assert np.array_equal(T, data["T_final"])
+
+
+def _volume_sum(m, T):
+    asv = m.array("areasvol").reshape(m.nl, -1, order="F")[: m.nl - 1, :]
+    h = m.array("hnode_new").reshape(m.nl - 1, -1, order="F")
+    nlev = m.array("nlevels_nod2D")
+    wet = np.arange(m.nl - 1)[:, None] < (nlev[None, :] - 1)
+    return float(np.sum(np.where(wet, T * asv * h, 0.0)))
+
+
+@pytest.mark.parametrize("hor,ver", [("MUSCL", "PPM"), ("MFCT", "QR4C"), ("UPW1", "CDIFF"), ("MUSCL", "UPW1")])
+def test_fct_conserves_and_bounds(oracle, hor, ver):
+    """Sum(T*vol) conserved to round-off and the FCT solution stays inside
+    the local min/max of the old and low-order fields (lib/oce_adv_tra_fct.F90)."""
+    import ctypes
+    lib = pytest.importorskip("fesom2_tracer_dwarf_b200._lib").load()
+    nx, ny, nl = 18, 14, 9
+    N = lib.tracer_analytic_nodes(nx, ny, 1)
+    K = np.zeros(N, dtype=np.int32)
+    lib.tracer_synth_bathymetry(N, nl, 3, K.ctypes.data_as(ctypes.c_void_p))
+    m = pyoracle.OracleMesh(oracle, nx, ny, nl, periodic=True, full_rings=True, node_K=K)
+    from fesom2_tracer_dwarf_b200 import FESOMTracerAdvection
+    api = FESOMTracerAdvection()
+    api.cleanup()
+    api.init_analytic(nx, ny, nl, periodic=True, full_rings=True, node_K=K)
+    uv, w = api.synth_velocity(seed=1, umax=1.0, mode2=0.4)
+    T = np.asfortranarray(api.synth_tracer(seed=2, kind=0))
+    api.cleanup()
+    dt = 0.5 * (1.0e5 / (nx - 1)) / 1.0
+    s0 = _volume_sum(m, T)
+    for _ in range(4):
+        Told = T.copy(order="F")
+        dh, dv, lo = m.step(T, Told.copy(order="F"), uv, w, dt, hor, ver, "FCT", want_terms=True)
+        # every new value lies within the cluster bounds of (Told, LO) over the ring
+        nlev = m.array("nlevels_nod2D")
+        wet = np.arange(nl - 1)[:, None] < (nlev[None, :] - 1)
+        big = np.where(wet, np.maximum(Told, lo), -np.inf)
+        small = np.where(wet, np.minimum(Told, lo), np.inf)
+        en = m.array("elem2D_nodes").reshape(3, -1, order="F") - 1
+        lvl = m.array("nlevels")
+        emax = np.full((nl - 1, m.elem2D), -np.inf)
+        emin = np.full((nl - 1, m.elem2D), np.inf)
+        for q in range(3):
+            emax = np.maximum(emax, big[:, en[q]])
+            emin = np.minimum(emin, small[:, en[q]])
+        ewet = np.arange(nl - 1)[:, None] < (lvl[None, :] - 1)
+        emax = np.where(ewet, emax, -np.inf)
+        emin = np.where(ewet, emin, np.inf)
+        nmax = np.full((nl - 1, m.nod2D), -np.inf)
+        nmin = np.full((nl - 1, m.nod2D), np.inf)
+        for q in range(3):
+            np.maximum.at(nmax.T, en[q], emax.T)
+            np.minimum.at(nmin.T, en[q], emin.T)
+        up = np.vstack([nmax[:1], nmax[:-1]])
+        dn = np.vstack([nmax[1:], nmax[-1:]])
+        hi = np.maximum(np.maximum(up, nmax), dn)
+        up = np.vstack([nmin[:1], nmin[:-1]])
+        dn = np.vstack([nmin[1:], nmin[-1:]])
+        lo_b = np.minimum(np.minimum(up, nmin), dn)
+        tol = 1e-9 * np.max(np.abs(T[wet]))
+        assert np.all(T[wet] <= hi[wet] + tol)
+        assert np.all(T[wet] >= lo_b[wet] - tol)
+    s1 = _volume_sum(m, T)
+    assert abs(s1 - s0) <= 1e-12 * abs(s0)
+
+
+def test_constant_field_stays_constant(oracle):
+    """With a discretely non-divergent flow a constant tracer stays constant."""
+    import ctypes
+    from fesom2_tracer_dwarf_b200 import FESOMTracerAdvection
+    nx, ny, nl = 16, 16, 8
+    api = FESOMTracerAdvection()
+    api.cleanup()
+    api.init_analytic(nx, ny, nl, periodic=True, full_rings=True)
+    uv, w = api.synth_velocity(seed=5, umax=1.0, mode2=0.0)
+    api.cleanup()
+    m = pyoracle.OracleMesh(oracle, nx, ny, nl, periodic=True, full_rings=True)
+    T = np.full((nl - 1, m.nod2D), 7.25, order="F")
+    for _ in range(3):
+        m.step(T, T.copy(order="F"), uv, w, 40.0, "MUSCL", "PPM", "FCT")
+    assert np.max(np.abs(T - 7.25)) < 1e-12
+
+
+def test_upw1_as_high_order_gives_zero_antidiffusion(oracle):
+    """With UPW1 as the high-order scheme and T_AB = T, the antidiffusive flux
+    is exactly 0, so FCT returns the low-order solution (to the round-off of
+    T + (LO*h - T*h)/h)."""
+    m = pyoracle.OracleMesh(oracle, 12, 12, 6, periodic=True, full_rings=True)
+    T, S, uv, w = m.analytic_fields()
+    T1 = T.copy(order="F")
+    dh, dv, lo = m.step(T1, T.copy(order="F"), uv, w, 1000.0, "UPW1", "UPW1", "FCT", want_terms=True)
+    assert np.max(np.abs(T1 - lo)) <= 1e-13 * np.max(np.abs(lo))
