@@ -70,6 +70,7 @@ SIGNATURES = {
     "tracer_set_device": (ctypes.c_int, [ctypes.c_int]),
     "tracer_launches_per_step": (ctypes.c_int, []),
     "tracer_device_bytes": (ctypes.c_longlong, []),
+    "tracer_selftest_division": (ctypes.c_int, [ctypes.c_longlong, ctypes.c_uint64, _vp, _vp]),
     "tracer_last_error": (ctypes.c_char_p, []),
 }
 

@@ -1,0 +1,574 @@
+// Kernels of the tracer advection step (do_oce_adv_tra,
+// lib/oce_adv_tra_driver.F90:23-294, FCT of lib/oce_adv_tra_fct.F90), fused
+// into four passes and batched over up to NTMAX tracers that share a mesh,
+// a flow and a scheme.
+//
+//   k_edge  [edge cells]  volume flux of every edge level (stored once for all
+//                         tracers) and, per tracer, the antidiffusive flux
+//                         HO(T_AB) - LO(T) (MUSCL/MFCT/UPW1), or HO alone
+//                         without FCT
+//   k_col1  [node cells]  horizontal LO gather, vertical LO and HO fluxes
+//                         (PPM slopes and interface values staged in shared
+//                         memory, geometry coefficients shared by the tracers),
+//                         LO solution
+//   k_col2  [node cells]  FCT cluster bounds (a1-a3), antidiffusive in/out
+//                         sums (b1) and limiter ratios (b2)
+//   k_col3  [node cells]  limiting (b3), flux2dtracer, T += del / h_new
+//
+// Edge scatters of the reference become node-centric gathers over the
+// node's incident edges in ascending edge id: every node sums its
+// contributions in the order of the reference's serial edge loop, with no
+// float atomics.  The FP64 build has no FMA contraction and keeps every
+// operation of the reference in its order; divisions by a static geometric
+// quantity use a once-per-cell reciprocal with Markstein's correction, which
+// returns the correctly rounded quotient, i.e. the same bits as a division.
+#pragma once
+#include <cstdint>
+
+#include "advect_ops.cuh"
+
+namespace fesom {
+
+constexpr int NTMAX = 4;
+constexpr int kThreads = 256;
+constexpr int kCellsPerBlock = 512;      // schedule target: wet cells per block
+constexpr int kMaxCellsPerBlock = 576;   // upper bound (target + deepest column)
+constexpr int kMaxItemsPerBlock = 512;
+
+// ---------------------------------------------------------------------------
+// Correctly rounded division a / b given y = RN(1/b).
+//
+// Markstein's theorem (P. Markstein, "Computation of elementary functions on
+// the IBM RISC System/6000 processor", IBM J. Res. Dev. 34, 1990; see also
+// Muller et al., Handbook of Floating-Point Arithmetic, Sec. 4.7): if y is
+// within half an ulp of 1/b and q is a faithful approximation of a/b, then
+// r = a - b q is exact when computed with one FMA and RN(q + r y) = RN(a/b).
+// q0 = RN(a y) can be 1.5 ulp off, so one correction first makes it faithful,
+// the second rounds correctly.  Zero and extreme magnitudes (where r could
+// underflow or overflow) take the plain division.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double div_rcp(double a, double b, double y) {
+  const double aa = fabs(a);
+  if (!(aa > 0x1p-900 && aa < 0x1p900)) return a / b;
+  double q = a * y;
+  double r = __fma_rn(-b, q, a);
+  if (r == 0.0) return q;
+  q = __fma_rn(r, y, q);
+  r = __fma_rn(-b, q, a);
+  return __fma_rn(r, y, q);
+}
+__device__ __forceinline__ float div_rcp(float a, float b, float y) {
+  const float aa = fabsf(a);
+  if (!(aa > 0x1p-100f && aa < 0x1p100f)) return a / b;
+  float q = a * y;
+  float r = __fmaf_rn(-b, q, a);
+  if (r == 0.0f) return q;
+  q = __fmaf_rn(r, y, q);
+  r = __fmaf_rn(-b, q, a);
+  return __fmaf_rn(r, y, q);
+}
+
+template <typename R>
+struct FusedArgs {
+  const R *T[NTMAX];      // values
+  const R *TAB[NTMAX];    // valuesAB (high-order fluxes)
+  R *T_out[NTMAX];
+  R *adf_h[NTMAX];        // (S, edge)
+  R *adf_v[NTMAX];        // (S, node) interfaces
+  R *lo[NTMAX];           // (S, node)
+  R *rp[NTMAX], *rm[NTMAX];
+  R *vflux;               // (S, edge), shared by the tracers
+  const R *vel;           // (2, S, elem)
+  const R *W;             // (S, node) interfaces
+  R dt, ph, pv;
+};
+
+// ---------------------------------------------------------------------------
+// block cell maps: a block owns a range of items (nodes or edges); every wet
+// cell of those items gets the local item index in shared memory
+// ---------------------------------------------------------------------------
+struct CellMap {
+  int i0, ni, c0, nc;
+};
+
+__device__ __forceinline__ CellMap map_cells(const DSched &sc, int *s_off, int *s_item) {
+  CellMap cm;
+  cm.i0 = sc.blk[blockIdx.x];
+  cm.ni = sc.blk[blockIdx.x + 1] - cm.i0;
+  for (int t = threadIdx.x; t <= cm.ni; t += blockDim.x) s_off[t] = sc.cell_off[cm.i0 + t];
+  __syncthreads();
+  cm.c0 = s_off[0];
+  cm.nc = s_off[cm.ni] - cm.c0;
+  for (int j = threadIdx.x; j < cm.ni; j += blockDim.x) {
+    const int a = s_off[j] - cm.c0, b = s_off[j + 1] - cm.c0;
+    for (int q = a; q < b; q++) s_item[q] = j;
+  }
+  __syncthreads();
+  return cm;
+}
+
+// ---------------------------------------------------------------------------
+// k_edge
+// ---------------------------------------------------------------------------
+template <typename R>
+__device__ __forceinline__ void trxy_n(const DMeshT<R> &m, const R *const *tab, int NT, int elem, int k, R *gx, R *gy) {
+  const int *en = m.elem_nodes + 3 * elem;
+  const int a = en[0], b = en[1], c = en[2];
+  const R *gs = m.grad_sca + 6 * elem;
+  const R g0 = gs[0], g1 = gs[1], g2 = gs[2], g3 = gs[3], g4 = gs[4], g5 = gs[5];
+  for (int t = 0; t < NT; t++) {
+    const R t1 = tab[t][(size_t)a * m.S + k], t2 = tab[t][(size_t)b * m.S + k], t3 = tab[t][(size_t)c * m.S + k];
+    gx[t] = (g0 * t1 + g1 * t2) + g2 * t3;
+    gy[t] = (g3 * t1 + g4 * t2) + g5 * t3;
+  }
+}
+
+template <typename R>
+__device__ __forceinline__ void ring_mean_n(const DMeshT<R> &m, const R *const *tab, int NT, int n, int k, R *gx, R *gy) {
+  R tvol = R(0), tx[NTMAX], ty[NTMAX];
+  for (int t = 0; t < NT; t++) { tx[t] = R(0); ty[t] = R(0); }
+  const int nz = k + 1;
+  for (int p = m.ring_ptr[n]; p < m.ring_ptr[n + 1]; p++) {
+    const int el = m.ring_elem[p];
+    if (m.nlev_elem[el] - 1 < nz) continue;
+    R ax[NTMAX], ay[NTMAX];
+    trxy_n(m, tab, NT, el, k, ax, ay);
+    const R a = m.elem_area[el];
+    tvol = tvol + a;
+    for (int t = 0; t < NT; t++) {
+      tx[t] = tx[t] + ax[t] * a;
+      ty[t] = ty[t] + ay[t] * a;
+    }
+  }
+  for (int t = 0; t < NT; t++) {
+    gx[t] = tx[t] / tvol;
+    gy[t] = ty[t] / tvol;
+  }
+}
+
+template <typename R, int NT, int HOR, int LIM>
+__global__ void __launch_bounds__(kThreads) k_edge(DMeshT<R> m, FusedArgs<R> a) {
+  extern __shared__ int smem[];
+  int *s_off = smem, *s_item = smem + kMaxItemsPerBlock + 1;
+  const CellMap cm = map_cells(m.edge_sched, s_off, s_item);
+  const R re = R(kREarthD), sixth = R(1.0 / 6.0);
+  for (int lc = threadIdx.x; lc < cm.nc; lc += blockDim.x) {
+    const int j = s_item[lc], e = cm.i0 + j, k = lc - (s_off[j] - cm.c0);
+    const EdgeCtx<R> c = edge_ctx(m, e);
+    const R vflux = edge_vflux(m, c, a.vel, k);
+    const size_t o = (size_t)e * m.S + k;
+    if (LIM == LIM_FCT) a.vflux[o] = vflux;
+    const size_t o1 = (size_t)c.n1 * m.S + k, o2 = (size_t)c.n2 * m.S + k;
+    if (HOR == HOR_UPW1) {
+      for (int t = 0; t < NT; t++) {
+        const R flo = (LIM == LIM_FCT) ? upw1_flux(vflux, a.T[t][o1], a.T[t][o2]) : R(0);
+        a.adf_h[t][o] = upw1_flux(vflux, a.TAB[t][o1], a.TAB[t][o2]) - flo;
+      }
+      continue;
+    }
+    // edge_up_dn_grad (lib/oce_muscl_adv.F90:383-527)
+    R gux[NTMAX], guy[NTMAX], gdx[NTMAX], gdy[NTMAX];
+    const int2 ud = m.up_dn[e];
+    bool shared = false;
+    if (ud.x >= 0 && ud.y >= 0) shared = (k + 1) <= min(m.nlev_node_min[c.n1], m.nlev_node_min[c.n2]) - 1;
+    if (shared) {
+      trxy_n(m, a.TAB, NT, ud.x, k, gux, guy);
+      trxy_n(m, a.TAB, NT, ud.y, k, gdx, gdy);
+    } else {
+      ring_mean_n(m, a.TAB, NT, c.n1, k, gux, guy);
+      ring_mean_n(m, a.TAB, NT, c.n2, k, gdx, gdy);
+    }
+    const R ex = m.edge_dxdy[2 * e], ey = m.edge_dxdy[2 * e + 1], aa = m.edge_a[e];
+    R c_lo1 = R(1), c_lo2 = R(1);
+    if (HOR == HOR_MUSCL) {
+      c_lo1 = (m.nbl[c.n1] - (k + 1) >= 0) ? R(1) : R(0);
+      c_lo2 = (m.nbl[c.n2] - (k + 1) >= 0) ? R(1) : R(0);
+    }
+    for (int t = 0; t < NT; t++) {
+      const R t1 = a.TAB[t][o1], t2 = a.TAB[t][o2];
+      R Tmean2, Tmean1;
+      // lib/oce_adv_tra_hor.F90:454-469 (MUSCL), :743-753 (MFCT, no c_lo)
+      const R x2 = R(2) * (t2 - t1) + ex * aa * gdx[t] + ey * re * gdy[t];
+      const R x1 = R(2) * (t2 - t1) + ex * aa * gux[t] + ey * re * guy[t];
+      if (HOR == HOR_MUSCL) {
+        Tmean2 = t2 - div_rcp(x2, R(6), sixth) * c_lo2;
+        Tmean1 = t1 + div_rcp(x1, R(6), sixth) * c_lo1;
+      } else {
+        Tmean2 = t2 - div_rcp(x2, R(6), sixth);
+        Tmean1 = t1 + div_rcp(x1, R(6), sixth);
+      }
+      const R cHO = (vflux + fabs(vflux)) * Tmean1 + (vflux - fabs(vflux)) * Tmean2;
+      const R ho = -(R(0.5) * (R(1) - a.ph) * cHO) - vflux * a.ph * R(0.5) * (Tmean1 + Tmean2);
+      const R flo = (LIM == LIM_FCT) ? upw1_flux(vflux, a.T[t][o1], a.T[t][o2]) : R(0);
+      a.adf_h[t][o] = ho - flo;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// k_col1: LO solution and vertical fluxes
+// ---------------------------------------------------------------------------
+// PPM slope of layer j (1-based) with the limiter of lib/oce_adv_tra_ver.F90:
+// 525-540; c1, c2, c3 are the geometric factors of that layer.
+template <typename R>
+__device__ __forceinline__ R ppm_slope(R Tm1, R T0, R Tp1, R c1, R c2, R c3) {
+  R d = c1 * (c2 * (Tp1 - T0) + c3 * (T0 - Tm1));
+  if ((Tp1 - T0) * (T0 - Tm1) > R(0))
+    d = fmin3(fabs(d), R(2) * fabs(Tp1 - T0), R(2) * fabs(T0 - Tm1)) * sgn1(d);
+  else
+    d = R(0);
+  return d;
+}
+
+template <typename R, int NT, int VER, int LIM>
+__global__ void __launch_bounds__(kThreads) k_col1(DMeshT<R> m, FusedArgs<R> a) {
+  extern __shared__ int smem[];
+  int *s_off = smem, *s_item = smem + kMaxItemsPerBlock + 1;
+  R *s_acc = (R *)(smem + kMaxItemsPerBlock + 1 + kMaxCellsPerBlock + 1);  // 8-byte aligned below
+  s_acc = (R *)(((uintptr_t)s_acc + 15) & ~(uintptr_t)15);
+  R *s_slope = s_acc + NT * kMaxCellsPerBlock;
+  R *s_tv = s_slope + NT * kMaxCellsPerBlock;
+  R *s_fv = s_tv + NT * kMaxCellsPerBlock;
+  const CellMap cm = map_cells(m.node_sched, s_off, s_item);
+  const int S = m.S;
+
+  // stage A: horizontal LO gather and PPM slopes
+  for (int lc = threadIdx.x; lc < cm.nc; lc += blockDim.x) {
+    const int j = s_item[lc], n = cm.i0 + j, k = lc - (s_off[j] - cm.c0), nz = k + 1;
+    if (LIM == LIM_FCT) {
+      R acc[NTMAX];
+      for (int t = 0; t < NT; t++) acc[t] = R(0);
+      for (int p = m.ne_ptr[n]; p < m.ne_ptr[n + 1]; p++) {
+        const int code = m.ne[p], e = code >> 1;
+        if (nz > m.edge_lev[e].y) continue;
+        const R vf = a.vflux[(size_t)e * S + k];
+        const int2 nn = m.edge_nodes[e];
+        for (int t = 0; t < NT; t++) {
+          const R F = upw1_flux(vf, a.T[t][(size_t)nn.x * S + k], a.T[t][(size_t)nn.y * S + k]);
+          acc[t] = (code & 1) ? acc[t] - F : acc[t] + F;
+        }
+      }
+      for (int t = 0; t < NT; t++) s_acc[t * kMaxCellsPerBlock + lc] = acc[t];
+    }
+    if (VER == VER_PPM) {
+      const int nlev = m.nlev_node[n];
+      if (nz >= 2 && nz <= nlev - 2) {
+        const R *HN = m.hnode_new + (size_t)n * S;
+        const R dzjm1 = HN[k - 1], dzj = HN[k], dzjp1 = HN[k + 1];
+        const R c1 = dzj / (dzjm1 + dzj + dzjp1);
+        const R c2 = (R(2) * dzjm1 + dzj) / (dzjp1 + dzj);
+        const R c3 = (dzj + R(2) * dzjp1) / (dzjm1 + dzj);
+        for (int t = 0; t < NT; t++) {
+          const R *Tc = a.TAB[t] + (size_t)n * S;
+          s_slope[t * kMaxCellsPerBlock + lc] = ppm_slope(Tc[k - 1], Tc[k], Tc[k + 1], c1, c2, c3);
+        }
+      }
+    }
+  }
+  __syncthreads();
+
+  // stage B: PPM interface values tv(i), interface i = nz (top of layer nz)
+  if (VER == VER_PPM) {
+    for (int lc = threadIdx.x; lc < cm.nc; lc += blockDim.x) {
+      const int j = s_item[lc], n = cm.i0 + j, k = lc - (s_off[j] - cm.c0), i = k + 1;
+      const int nlev = m.nlev_node[n];
+      const R *HN = m.hnode_new + (size_t)n * S;
+      const R *Wc = a.W + (size_t)n * S;
+      if (i == 1) {
+        for (int t = 0; t < NT; t++) s_tv[t * kMaxCellsPerBlock + lc] = a.TAB[t][(size_t)n * S];
+      } else if (i == nlev - 1) {
+        const R s = sgn1(Wc[nlev - 2]);
+        for (int t = 0; t < NT; t++) {
+          const R *Tc = a.TAB[t] + (size_t)n * S;
+          s_tv[t * kMaxCellsPerBlock + lc] = -Tc[nlev - 3] * fmin2(s, R(0)) + Tc[nlev - 2] * fmax2(s, R(0));
+        }
+      } else if (i == 2) {
+        for (int t = 0; t < NT; t++) {
+          const R *Tc = a.TAB[t] + (size_t)n * S;
+          s_tv[t * kMaxCellsPerBlock + lc] = R(0.5) * (Tc[0] + Tc[1]);
+        }
+      } else {
+        // lib/oce_adv_tra_ver.F90:545-553 with nz = i - 1
+        const int nzz = i - 1;  // 1-based layer above the interface
+        const R dzjm1 = HN[nzz - 2], dzj = HN[nzz - 1], dzjp1 = HN[nzz], dzjp2 = HN[nzz + 1];
+        const R A = dzj / (dzj + dzjp1);
+        const R B = R(1) / (dzjm1 + dzj + dzjp1 + dzjp2);
+        const R C = (R(2) * dzjp1 * dzj) / (dzj + dzjp1) *
+                    ((dzjm1 + dzj) / (R(2) * dzj + dzjp1) - (dzjp2 + dzjp1) / (R(2) * dzjp1 + dzj));
+        const R D = dzj * (dzjm1 + dzj) / (R(2) * dzj + dzjp1);
+        const R E = dzjp1 * (dzjp1 + dzjp2) / (dzj + R(2) * dzjp1);
+        for (int t = 0; t < NT; t++) {
+          const R *Tc = a.TAB[t] + (size_t)n * S;
+          const R T0 = Tc[nzz - 1], T1 = Tc[nzz];
+          const R dj = s_slope[t * kMaxCellsPerBlock + lc - 1];   // layer nzz
+          const R djp1 = s_slope[t * kMaxCellsPerBlock + lc];     // layer nzz + 1
+          s_tv[t * kMaxCellsPerBlock + lc] = T0 + A * (T1 - T0) + B * (C * (T1 - T0) - D * djp1 + E * dj);
+        }
+      }
+    }
+    __syncthreads();
+  }
+
+  // stage C: fluxes at interface i = nz (and the bottom one for the deepest layer)
+  for (int lc = threadIdx.x; lc < cm.nc; lc += blockDim.x) {
+    const int j = s_item[lc], n = cm.i0 + j, k = lc - (s_off[j] - cm.c0);
+    const size_t col = (size_t)n * S;
+    const int nlev = m.nlev_node[n];
+    const R *Wc = a.W + col, *Ac = m.area + col;
+    const int i_last = (k + 2 == nlev) ? k + 2 : k + 1;
+    for (int i = k + 1; i <= i_last; i++) {
+      R lov[NTMAX], hov[NTMAX];
+      for (int t = 0; t < NT; t++) lov[t] = R(0);
+      if (LIM == LIM_FCT) {
+        for (int t = 0; t < NT; t++) {
+          Col<R> cT;
+          cT.T = a.T[t] + col; cT.W = Wc; cT.A = Ac; cT.nlev = nlev;
+          lov[t] = ver_upw1(cT, i);
+        }
+      }
+      if (VER == VER_PPM) {
+        // lib/oce_adv_tra_ver.F90:597-639
+        if (i == nlev) {
+          for (int t = 0; t < NT; t++) hov[t] = R(0) - lov[t];
+        } else if (i == 1) {
+          for (int t = 0; t < NT; t++) hov[t] = -(s_tv[t * kMaxCellsPerBlock + lc] * Wc[0] * Ac[0]) - lov[t];
+        } else {
+          const R w = Wc[i - 1];
+          if (!(w > R(0)) && !(w < R(0))) {
+            for (int t = 0; t < NT; t++) hov[t] = R(0) - lov[t];
+          } else {
+            const int jl = (w > R(0)) ? i : i - 1;              // supplying layer (1-based)
+            const int sl = lc + (jl - i);                        // its cell slot
+            const R dzj = m.hnode[col + jl - 1];
+            const R x = (w > R(0)) ? fmin2(w * a.dt / dzj, R(1)) : fmin2(-(w * a.dt / dzj), R(1));
+            const R two3 = R(2.0 / 3.0);
+            for (int t = 0; t < NT; t++) {
+              const R Tc = a.TAB[t][col + jl - 1];
+              R aL = s_tv[t * kMaxCellsPerBlock + sl];
+              R aR = (jl + 1 == nlev) ? a.TAB[t][col + nlev - 2] : s_tv[t * kMaxCellsPerBlock + sl + 1];
+              if ((aR - Tc) * (Tc - aL) <= R(0)) { aL = Tc; aR = Tc; }
+              if ((aR - aL) * (Tc - R(0.5) * (aL + aR)) > (aR - aL) * (aR - aL) / R(6)) aL = R(3) * Tc - R(2) * aR;
+              if ((aR - aL) * (Tc - R(0.5) * (aR + aL)) < -((aR - aL) * (aR - aL) / R(6))) aR = R(3) * Tc - R(2) * aL;
+              const R aj = R(6) * (Tc - R(0.5) * (aL + aR));
+              R tt;
+              if (w > R(0)) tt = (-aL - R(0.5) * x * (aR - aL + (R(1) - two3 * x) * aj));
+              else tt = (-aR + R(0.5) * x * (aR - aL - (R(1) - two3 * x) * aj));
+              hov[t] = tt * Ac[i - 1] * w - lov[t];
+            }
+          }
+        }
+      } else {
+        for (int t = 0; t < NT; t++) {
+          Col<R> cA;
+          cA.T = a.TAB[t] + col; cA.W = Wc; cA.A = Ac; cA.nlev = nlev;
+          if (VER == VER_QR4C) hov[t] = ver_qr4c(cA, m.zbar, m.Z, i, a.pv, lov[t]);
+          else if (VER == VER_CDIFF) hov[t] = ver_cdiff(cA, i, lov[t]);
+          else hov[t] = ver_upw1(cA, i) - lov[t];
+        }
+      }
+      for (int t = 0; t < NT; t++) {
+        a.adf_v[t][col + i - 1] = hov[t];
+        if (LIM == LIM_FCT && i == k + 1) s_fv[t * kMaxCellsPerBlock + lc] = lov[t];
+      }
+    }
+  }
+  if (LIM != LIM_FCT) return;
+  __syncthreads();
+
+  // stage D: LO solution (lib/oce_adv_tra_driver.F90:202-211)
+  for (int lc = threadIdx.x; lc < cm.nc; lc += blockDim.x) {
+    const int j = s_item[lc], n = cm.i0 + j, k = lc - (s_off[j] - cm.c0);
+    const size_t o = (size_t)n * S + k;
+    const int nlev = m.nlev_node[n];
+    const R asv = m.areasvol[o], hn = m.hnode_new[o], h = m.hnode[o];
+    const R yasv = R(1) / asv, yhn = R(1) / hn;
+    for (int t = 0; t < NT; t++) {
+      const R fk = s_fv[t * kMaxCellsPerBlock + lc];
+      const R fk1 = (k + 2 == nlev) ? R(0) : s_fv[t * kMaxCellsPerBlock + lc + 1];
+      const R acc = s_acc[t * kMaxCellsPerBlock + lc];
+      const R num = a.T[t][o] * h + div_rcp((acc + (fk - fk1)) * a.dt, asv, yasv);
+      a.lo[t][o] = div_rcp(num, hn, yhn);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// k_col2: bounds, in/out sums, ratios (lib/oce_adv_tra_fct.F90:105-374)
+// ---------------------------------------------------------------------------
+template <typename R, int NT>
+__global__ void __launch_bounds__(kThreads) k_col2(DMeshT<R> m, FusedArgs<R> a) {
+  extern __shared__ int smem[];
+  int *s_off = smem, *s_item = smem + kMaxItemsPerBlock + 1;
+  R *s_mx = (R *)(smem + kMaxItemsPerBlock + 1 + kMaxCellsPerBlock + 1);
+  s_mx = (R *)(((uintptr_t)s_mx + 15) & ~(uintptr_t)15);
+  R *s_mn = s_mx + NT * kMaxCellsPerBlock;
+  const CellMap cm = map_cells(m.node_sched, s_off, s_item);
+  const int S = m.S;
+  const R big = R(1e3);
+
+  for (int lc = threadIdx.x; lc < cm.nc; lc += blockDim.x) {
+    const int j = s_item[lc], n = cm.i0 + j, k = lc - (s_off[j] - cm.c0), nz = k + 1;
+    R tmx[NTMAX], tmn[NTMAX];
+    for (int p = m.ring_ptr[n]; p < m.ring_ptr[n + 1]; p++) {
+      const int el = m.ring_elem[p];
+      const bool wet = nz <= m.nlev_elem[el] - 1;
+      int e0 = 0, e1 = 0, e2 = 0;
+      if (wet) {
+        const int *en = m.elem_nodes + 3 * el;
+        e0 = en[0]; e1 = en[1]; e2 = en[2];
+      }
+      for (int t = 0; t < NT; t++) {
+        R amx, amn;
+        if (wet) {
+          const size_t o0 = (size_t)e0 * S + k, o1 = (size_t)e1 * S + k, o2 = (size_t)e2 * S + k;
+          const R l0 = a.lo[t][o0], l1 = a.lo[t][o1], l2 = a.lo[t][o2];
+          const R t0 = a.T[t][o0], t1 = a.T[t][o1], t2 = a.T[t][o2];
+          amx = fmax3(fmax2(l0, t0), fmax2(l1, t1), fmax2(l2, t2));
+          amn = fmin3(fmin2(l0, t0), fmin2(l1, t1), fmin2(l2, t2));
+        } else {
+          amx = -big;
+          amn = big;
+        }
+        if (p == m.ring_ptr[n]) { tmx[t] = amx; tmn[t] = amn; }
+        else { tmx[t] = fmax2(tmx[t], amx); tmn[t] = fmin2(tmn[t], amn); }
+      }
+    }
+    for (int t = 0; t < NT; t++) {
+      s_mx[t * kMaxCellsPerBlock + lc] = tmx[t];
+      s_mn[t * kMaxCellsPerBlock + lc] = tmn[t];
+    }
+  }
+  __syncthreads();
+
+  const R eps = R((double)1e-16f);  // real(MP) :: flux_eps = 1e-16 (default-real literal)
+  for (int lc = threadIdx.x; lc < cm.nc; lc += blockDim.x) {
+    const int j = s_item[lc], n = cm.i0 + j, k = lc - (s_off[j] - cm.c0), nz = k + 1;
+    const size_t col = (size_t)n * S, o = col + k;
+    const int nl1 = m.nlev_node[n];
+    const bool edge_lev = (nz == 1 || nz == nl1 - 1);
+    R fp[NTMAX], fm[NTMAX];
+    for (int t = 0; t < NT; t++) {
+      const R *av = a.adf_v[t] + col;
+      fp[t] = R(0) + (fmax2(R(0), av[k]) + fmax2(R(0), -av[k + 1]));
+      fm[t] = R(0) + (fmin2(R(0), av[k]) + fmin2(R(0), -av[k + 1]));
+    }
+    for (int p = m.ne_ptr[n]; p < m.ne_ptr[n + 1]; p++) {
+      const int code = m.ne[p], e = code >> 1;
+      if (nz > m.edge_lev[e].y) continue;
+      for (int t = 0; t < NT; t++) {
+        const R f = a.adf_h[t][(size_t)e * S + k];
+        if (code & 1) {
+          fp[t] = fp[t] + fmax2(R(0), -f);
+          fm[t] = fm[t] + fmin2(R(0), -f);
+        } else {
+          fp[t] = fp[t] + fmax2(R(0), f);
+          fm[t] = fm[t] + fmin2(R(0), f);
+        }
+      }
+    }
+    const R asv = m.areasvol[o];
+    const R yasv = R(1) / asv;
+    for (int t = 0; t < NT; t++) {
+      const int b = t * kMaxCellsPerBlock + lc;
+      const R LO = a.lo[t][o];
+      R bmax, bmin;
+      if (edge_lev) {
+        bmax = s_mx[b] - LO;
+        bmin = s_mn[b] - LO;
+      } else {
+        bmax = fmax3(s_mx[b - 1], s_mx[b], s_mx[b + 1]) - LO;
+        bmin = fmin3(s_mn[b - 1], s_mn[b], s_mn[b + 1]) - LO;
+      }
+      R flux = div_rcp(fp[t] * a.dt, asv, yasv) + eps;
+      a.rp[t][o] = fmin2(R(1), bmax / flux);
+      flux = div_rcp(fm[t] * a.dt, asv, yasv) - eps;
+      a.rm[t][o] = fmin2(R(1), bmin / flux);
+    }
+  }
+}
+
+// limited vertical flux at interface i (lib/oce_adv_tra_fct.F90:396-427)
+template <typename R>
+__device__ __forceinline__ R limit_v(const R *av, const R *rp, const R *rm, int i, int nlev) {
+  const R f = av[i - 1];
+  if (i == nlev) return f;
+  R ae = R(1);
+  if (i == 1) {
+    ae = (f >= R(0)) ? fmin2(ae, rp[0]) : fmin2(ae, rm[0]);
+  } else if (f >= R(0)) {
+    ae = fmin2(ae, rm[i - 2]);
+    ae = fmin2(ae, rp[i - 1]);
+  } else {
+    ae = fmin2(ae, rp[i - 2]);
+    ae = fmin2(ae, rm[i - 1]);
+  }
+  return ae * f;
+}
+
+// ---------------------------------------------------------------------------
+// k_col3: limiting + flux2dtracer + update
+// ---------------------------------------------------------------------------
+template <typename R, int NT, int LIM>
+__global__ void __launch_bounds__(kThreads) k_col3(DMeshT<R> m, FusedArgs<R> a) {
+  extern __shared__ int smem[];
+  int *s_off = smem, *s_item = smem + kMaxItemsPerBlock + 1;
+  const CellMap cm = map_cells(m.node_sched, s_off, s_item);
+  const int S = m.S;
+  for (int lc = threadIdx.x; lc < cm.nc; lc += blockDim.x) {
+    const int j = s_item[lc], n = cm.i0 + j, k = lc - (s_off[j] - cm.c0), nz = k + 1;
+    const size_t col = (size_t)n * S, o = col + k;
+    const int nlev = m.nlev_node[n];
+    const R asv = m.areasvol[o], hn = m.hnode_new[o];
+    const R yasv = R(1) / asv, yhn = R(1) / hn;
+    R dv[NTMAX], dh[NTMAX];
+    for (int t = 0; t < NT; t++) {
+      const R *av = a.adf_v[t] + col;
+      dv[t] = R(0);
+      if (LIM == LIM_FCT) {
+        dv[t] = dv[t] - a.T[t][o] * m.hnode[o] + a.lo[t][o] * hn;
+        const R fk = limit_v(av, a.rp[t] + col, a.rm[t] + col, nz, nlev);
+        const R fk1 = limit_v(av, a.rp[t] + col, a.rm[t] + col, nz + 1, nlev);
+        dv[t] = dv[t] + div_rcp((fk - fk1) * a.dt, asv, yasv);
+      } else {
+        dv[t] = dv[t] + div_rcp((av[k] - av[k + 1]) * a.dt, asv, yasv);
+      }
+      dh[t] = R(0);
+    }
+    for (int p = m.ne_ptr[n]; p < m.ne_ptr[n + 1]; p++) {
+      const int code = m.ne[p], e = code >> 1;
+      if (nz > m.edge_lev[e].y) continue;
+      const int2 nn = m.edge_nodes[e];
+      const size_t o1 = (size_t)nn.x * S + k, o2 = (size_t)nn.y * S + k;
+      for (int t = 0; t < NT; t++) {
+        R f = a.adf_h[t][(size_t)e * S + k];
+        if (LIM == LIM_FCT) {
+          R ae = R(1);
+          if (f >= R(0)) {
+            ae = fmin2(ae, a.rp[t][o1]);
+            ae = fmin2(ae, a.rm[t][o2]);
+          } else {
+            ae = fmin2(ae, a.rm[t][o1]);
+            ae = fmin2(ae, a.rp[t][o2]);
+          }
+          f = ae * f;
+        }
+        const R term = div_rcp(f * a.dt, asv, yasv);
+        dh[t] = (code & 1) ? dh[t] - term : dh[t] + term;
+      }
+    }
+    for (int t = 0; t < NT; t++) {
+      const R del = R(0) + dh[t] + dv[t];
+      a.T_out[t][o] = a.T[t][o] + div_rcp(del, hn, yhn);
+    }
+  }
+}
+
+// dynamic shared memory of each kernel
+template <typename R>
+constexpr size_t smem_edge() { return sizeof(int) * (kMaxItemsPerBlock + 1 + kMaxCellsPerBlock + 1); }
+template <typename R>
+constexpr size_t smem_col(int nt, int arrays) {
+  return sizeof(int) * (kMaxItemsPerBlock + 1 + kMaxCellsPerBlock + 1) + 16 + sizeof(R) * (size_t)arrays * nt * kMaxCellsPerBlock;
+}
+
+}  // namespace fesom

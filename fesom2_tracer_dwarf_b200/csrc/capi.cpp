@@ -603,9 +603,7 @@ int tracer_set_device(int device) {
 
 int tracer_launches_per_step(void) {
   if (!g.eng) return 0;
-  int n = 0;
-  for (int i = 0; i < g.ntr; i++) n += g.eng->launches_per_tracer_step(i);
-  return n;
+  return g.eng->launches_per_step();
 }
 
 long long tracer_device_bytes(void) { return g.eng ? (long long)g.eng->device_bytes() : 0; }

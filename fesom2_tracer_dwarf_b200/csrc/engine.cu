@@ -1,10 +1,12 @@
 // Engine: device memory, layout conversion, schedules and kernel dispatch.
 #include <algorithm>
+#include <mutex>
+#include <unordered_map>
 #include <cstring>
 #include <stdexcept>
 #include <string>
 
-#include "advect_kernels.cuh"
+#include "advect_fused.cuh"
 #include "engine.hpp"
 
 namespace fesom {
@@ -23,9 +25,6 @@ void set_last_error(const std::string &s) { g_err = s; }
 
 namespace {
 
-constexpr int kBlock = 256;
-constexpr int kCellsPerBlock = 1024;
-constexpr int kMaxItemsPerBlock = 1024;
 
 void build_sched(const std::vector<int> &counts, std::vector<int> &off, std::vector<int> &blk, int &max_items) {
   const int n = (int)counts.size();
@@ -44,6 +43,9 @@ void build_sched(const std::vector<int> &counts, std::vector<int> &off, std::vec
     }
   }
   if (n == 0) blk.push_back(0);
+  for (size_t b = 0; b + 1 < blk.size(); b++)
+    if (off[blk[b + 1]] - off[blk[b]] > kMaxCellsPerBlock)
+      throw std::runtime_error("schedule block exceeds the per-block cell capacity");
 }
 
 }  // namespace
@@ -61,8 +63,23 @@ struct EngineImpl {
     TracerScheme sch;
   };
   std::vector<Tracer> tr;
-  double *flo = nullptr, *adfh = nullptr, *adfv = nullptr, *lo = nullptr;
-  double *tmax = nullptr, *tmin = nullptr, *rp = nullptr, *rm = nullptr;
+  // work arrays, one slot per tracer of a batch
+  int slots = 0;
+  double *vflux = nullptr;
+  double *adfh[NTMAX] = {}, *adfv[NTMAX] = {}, *lo[NTMAX] = {}, *rp[NTMAX] = {}, *rm[NTMAX] = {};
+  void ensure_slots(int n) {
+    if (n <= slots) return;
+    const size_t ns = (size_t)mesh.nod2D * S, es = (size_t)mesh.edge2D * S;
+    if (!vflux) vflux = dalloc<double>(es);
+    for (int t = slots; t < n; t++) {
+      adfh[t] = dalloc<double>(es);
+      adfv[t] = dalloc<double>(ns);
+      lo[t] = dalloc<double>(ns);
+      rp[t] = dalloc<double>(ns);
+      rm[t] = dalloc<double>(ns);
+    }
+    slots = n;
+  }
   // launch profiling: when prof is set, every launch is bracketed by events
   struct ProfRec { int kind; cudaEvent_t a, b; };
   std::vector<ProfRec> *prof = nullptr;
@@ -95,10 +112,28 @@ struct EngineImpl {
     if (it != allocs.end()) allocs.erase(it);
     cudaFree(p);
   }
+  // Every transfer is ordered on the engine's stream (which does not
+  // synchronise with the legacy default stream) and completes before the call
+  // returns, so host staging buffers may be released right after.
+  void h2d(void *d, const void *h, size_t bytes) {
+    if (!bytes) return;
+    CK(cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, stream));
+    CK(cudaStreamSynchronize(stream));
+  }
+  void d2h(void *h, const void *d, size_t bytes) {
+    if (!bytes) return;
+    CK(cudaMemcpyAsync(h, d, bytes, cudaMemcpyDeviceToHost, stream));
+    CK(cudaStreamSynchronize(stream));
+  }
+  void d2d(void *dst, const void *src, size_t bytes) {
+    if (!bytes) return;
+    CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, stream));
+    CK(cudaStreamSynchronize(stream));
+  }
   template <typename T>
   T *upload(const std::vector<T> &h) {
     T *d = dalloc<T>(h.size());
-    if (!h.empty()) CK(cudaMemcpy(d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice));
+    h2d(d, h.data(), h.size() * sizeof(T));
     return d;
   }
   // (ld, ncol) column-major host array -> device columns of stride S
@@ -110,7 +145,7 @@ struct EngineImpl {
   void copy_cols_to(double *d, const double *h, int ld, int ncol) {
     std::vector<double> st((size_t)ncol * S, 0.0);
     for (int c = 0; c < ncol; c++) std::memcpy(&st[(size_t)c * S], h + (size_t)c * ld, sizeof(double) * ld);
-    CK(cudaMemcpy(d, st.data(), st.size() * sizeof(double), cudaMemcpyHostToDevice));
+    h2d(d, st.data(), st.size() * sizeof(double));
   }
 };
 
@@ -174,14 +209,6 @@ Engine::Engine(const MeshHost &mesh) : p_(new EngineImpl) {
 
   P.vel = P.dalloc<double>((size_t)2 * T * P.S);
   P.W = P.dalloc<double>((size_t)N * P.S);
-  P.flo = P.dalloc<double>((size_t)E * P.S);
-  P.adfh = P.dalloc<double>((size_t)E * P.S);
-  P.adfv = P.dalloc<double>((size_t)N * P.S);
-  P.lo = P.dalloc<double>((size_t)N * P.S);
-  P.tmax = P.dalloc<double>((size_t)N * P.S);
-  P.tmin = P.dalloc<double>((size_t)N * P.S);
-  P.rp = P.dalloc<double>((size_t)N * P.S);
-  P.rm = P.dalloc<double>((size_t)N * P.S);
   CK(cudaStreamSynchronize(P.stream));
 }
 
@@ -210,14 +237,15 @@ void Engine::set_velocity(const double *uv, const double *w) {
       st[2 * ((size_t)e * P.S + k)] = uv[2 * ((size_t)e * L + k)];
       st[2 * ((size_t)e * P.S + k) + 1] = uv[2 * ((size_t)e * L + k) + 1];
     }
-  CK(cudaMemcpy(P.vel, st.data(), st.size() * sizeof(double), cudaMemcpyHostToDevice));
+  P.h2d(P.vel, st.data(), st.size() * sizeof(double));
   P.copy_cols_to(P.W, w, M.nl, N);
 }
 
 void Engine::set_velocity_zero() {
   EngineImpl &P = *p_;
-  CK(cudaMemset(P.vel, 0, sizeof(double) * 2 * P.mesh.elem2D * P.S));
-  CK(cudaMemset(P.W, 0, sizeof(double) * P.mesh.nod2D * P.S));
+  CK(cudaMemsetAsync(P.vel, 0, sizeof(double) * 2 * P.mesh.elem2D * P.S, P.stream));
+  CK(cudaMemsetAsync(P.W, 0, sizeof(double) * P.mesh.nod2D * P.S, P.stream));
+  CK(cudaStreamSynchronize(P.stream));
 }
 
 void Engine::allocate_tracers(int ntr) {
@@ -244,8 +272,8 @@ void Engine::set_values(int id, const double *v, bool also_ab) {
   const int L = P.mesh.nl - 1;
   CK(cudaStreamSynchronize(P.stream));
   P.copy_cols_to(P.tr[id].T, v, L, P.mesh.nod2D);
-  CK(cudaMemcpy(P.tr[id].Tout, P.tr[id].T, sizeof(double) * P.mesh.nod2D * P.S, cudaMemcpyDeviceToDevice));
-  if (also_ab) CK(cudaMemcpy(P.tr[id].TAB, P.tr[id].T, sizeof(double) * P.mesh.nod2D * P.S, cudaMemcpyDeviceToDevice));
+  P.d2d(P.tr[id].Tout, P.tr[id].T, sizeof(double) * P.mesh.nod2D * P.S);
+  if (also_ab) P.d2d(P.tr[id].TAB, P.tr[id].T, sizeof(double) * P.mesh.nod2D * P.S);
 }
 
 void Engine::set_values_ab(int id, const double *v) {
@@ -260,8 +288,7 @@ void Engine::get_values(int id, double *out) const {
   check_id(P, id);
   const int L = P.mesh.nl - 1, N = P.mesh.nod2D;
   std::vector<double> st((size_t)N * P.S);
-  CK(cudaStreamSynchronize(P.stream));
-  CK(cudaMemcpy(st.data(), P.tr[id].T, st.size() * sizeof(double), cudaMemcpyDeviceToHost));
+  P.d2h(st.data(), P.tr[id].T, st.size() * sizeof(double));
   for (int n = 0; n < N; n++) std::memcpy(out + (size_t)n * L, &st[(size_t)n * P.S], sizeof(double) * L);
 }
 
@@ -276,93 +303,145 @@ TracerScheme Engine::scheme(int id) const {
   return p_->tr[id].sch;
 }
 
-int Engine::launches_per_tracer_step(int id) const {
-  check_id(*p_, id);
-  return p_->tr[id].sch.lim == 1 ? 6 : 3;
-}
-
 namespace {
 
-enum { KK_EDGE = 0, KK_LO, KK_VERT, KK_BOUNDS, KK_RATIO, KK_APPLY, KK_COUNT };
-const char *const kKindNames[KK_COUNT] = {"edge_flux", "node_lo", "node_vert", "node_bounds", "node_ratio",
-                                          "node_apply"};
+enum { KK_EDGE = 0, KK_COL1, KK_COL2, KK_COL3, KK_COUNT };
+const char *const kKindNames[KK_COUNT] = {"k_edge", "k_col1", "k_col2", "k_col3"};
 
-template <int HOR, int LIM>
-void launch_edge(EngineImpl &P, const StepArgs<double> &a) {
+// Raise the dynamic shared-memory limit of a kernel once (per kernel
+// function; all kernels share one C++ function-pointer type).
+template <typename K>
+void set_smem(K kernel, size_t bytes) {
+  static std::mutex mu;
+  static std::unordered_map<const void *, size_t> done;
+  std::lock_guard<std::mutex> lock(mu);
+  auto it = done.find((const void *)kernel);
+  if (it != done.end() && it->second >= bytes) return;
+  CK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+  done[(const void *)kernel] = bytes;
+}
+
+template <int NT, int HOR, int LIM>
+void launch_edge(EngineImpl &P, const FusedArgs<double> &a) {
   const DSched &s = P.dm.edge_sched;
   if (s.nblk <= 0) return;
+  const size_t sm = smem_edge<double>();
   P.mark_begin(KK_EDGE);
-  k_edge_flux<double, HOR, LIM><<<s.nblk, kBlock, (s.max_items + 1) * sizeof(int), P.stream>>>(P.dm, a);
-  P.mark_end();
-}
-template <int VER, int LIM>
-void launch_vert(EngineImpl &P, const StepArgs<double> &a) {
-  const DSched &s = P.dm.node_sched;
-  P.mark_begin(KK_VERT);
-  k_node_vert<double, VER, LIM><<<s.nblk, kBlock, (s.max_items + 1) * sizeof(int), P.stream>>>(P.dm, a);
+  k_edge<double, NT, HOR, LIM><<<s.nblk, kThreads, sm, P.stream>>>(P.dm, a);
   P.mark_end();
 }
 
-template <int LIM>
-void run_step(EngineImpl &P, const TracerScheme &sc, const StepArgs<double> &a) {
-  switch (sc.hor) {
-    case 1: launch_edge<HOR_MUSCL, LIM>(P, a); break;
-    case 2: launch_edge<HOR_MFCT, LIM>(P, a); break;
-    default: launch_edge<HOR_UPW1, LIM>(P, a); break;
-  }
+template <int NT, int VER, int LIM>
+void launch_col1(EngineImpl &P, const FusedArgs<double> &a) {
   const DSched &s = P.dm.node_sched;
-  const size_t sm = (s.max_items + 1) * sizeof(int);
-  if (LIM == LIM_FCT) {
-    P.mark_begin(KK_LO);
-    k_node_lo<double><<<s.nblk, kBlock, sm, P.stream>>>(P.dm, a);
-    P.mark_end();
+  const size_t sm = smem_col<double>(NT, 4);
+  set_smem(k_col1<double, NT, VER, LIM>, sm);
+  P.mark_begin(KK_COL1);
+  k_col1<double, NT, VER, LIM><<<s.nblk, kThreads, sm, P.stream>>>(P.dm, a);
+  P.mark_end();
+}
+
+template <int NT, int LIM>
+void run_group(EngineImpl &P, const TracerScheme &sc, const FusedArgs<double> &a) {
+  switch (sc.hor) {
+    case 1: launch_edge<NT, HOR_MUSCL, LIM>(P, a); break;
+    case 2: launch_edge<NT, HOR_MFCT, LIM>(P, a); break;
+    default: launch_edge<NT, HOR_UPW1, LIM>(P, a); break;
   }
   switch (sc.ver) {
-    case 1: launch_vert<VER_PPM, LIM>(P, a); break;
-    case 2: launch_vert<VER_QR4C, LIM>(P, a); break;
-    case 3: launch_vert<VER_CDIFF, LIM>(P, a); break;
-    default: launch_vert<VER_UPW1, LIM>(P, a); break;
+    case 1: launch_col1<NT, VER_PPM, LIM>(P, a); break;
+    case 2: launch_col1<NT, VER_QR4C, LIM>(P, a); break;
+    case 3: launch_col1<NT, VER_CDIFF, LIM>(P, a); break;
+    default: launch_col1<NT, VER_UPW1, LIM>(P, a); break;
   }
+  const DSched &s = P.dm.node_sched;
   if (LIM == LIM_FCT) {
-    P.mark_begin(KK_BOUNDS);
-    k_node_bounds<double><<<s.nblk, kBlock, sm, P.stream>>>(P.dm, a);
-    P.mark_end();
-    P.mark_begin(KK_RATIO);
-    k_node_ratio<double><<<s.nblk, kBlock, sm, P.stream>>>(P.dm, a);
+    const size_t sm2 = smem_col<double>(NT, 2);
+    set_smem(k_col2<double, NT>, sm2);
+    P.mark_begin(KK_COL2);
+    k_col2<double, NT><<<s.nblk, kThreads, sm2, P.stream>>>(P.dm, a);
     P.mark_end();
   }
-  P.mark_begin(KK_APPLY);
-  k_node_apply<double, LIM><<<s.nblk, kBlock, sm, P.stream>>>(P.dm, a);
+  const size_t sm3 = smem_col<double>(NT, 0);
+  P.mark_begin(KK_COL3);
+  k_col3<double, NT, LIM><<<s.nblk, kThreads, sm3, P.stream>>>(P.dm, a);
   P.mark_end();
+}
+
+template <int NT>
+void run_group_nt(EngineImpl &P, const TracerScheme &sc, const FusedArgs<double> &a) {
+  if (sc.lim == 1) run_group<NT, LIM_FCT>(P, sc, a);
+  else run_group<NT, LIM_NONE>(P, sc, a);
 }
 
 }  // namespace
 
-void Engine::step_tracer(int id, double dt, bool refresh_ab) {
-  EngineImpl &P = *p_;
-  check_id(P, id);
-  auto &t = P.tr[id];
-  StepArgs<double> a;
-  a.T = t.T;
-  a.TAB = refresh_ab ? t.T : t.TAB;
+// Tracers are advanced in batches of up to NTMAX consecutive tracers with
+// the same scheme; a batch shares the edge volume fluxes, the geometry loads
+// and every geometry-only division.
+static void run_batch(EngineImpl &P, int first, int nt, double dt, bool refresh_ab) {
+  P.ensure_slots(nt);
+  FusedArgs<double> a{};
+  const TracerScheme &sc = P.tr[first].sch;
+  for (int t = 0; t < nt; t++) {
+    auto &tr = P.tr[first + t];
+    a.T[t] = tr.T;
+    a.TAB[t] = refresh_ab ? tr.T : tr.TAB;
+    a.T_out[t] = tr.Tout;
+    a.adf_h[t] = P.adfh[t];
+    a.adf_v[t] = P.adfv[t];
+    a.lo[t] = P.lo[t];
+    a.rp[t] = P.rp[t];
+    a.rm[t] = P.rm[t];
+  }
+  a.vflux = P.vflux;
   a.vel = P.vel;
   a.W = P.W;
   a.dt = dt;
-  a.ph = t.sch.ph;
-  a.pv = t.sch.pv;
-  a.flo = P.flo; a.adf_h = P.adfh; a.adf_v = P.adfv; a.lo = P.lo;
-  a.tmax = P.tmax; a.tmin = P.tmin; a.rp = P.rp; a.rm = P.rm;
-  a.T_out = t.Tout;
+  a.ph = sc.ph;
+  a.pv = sc.pv;
   if (P.mesh.nod2D > 0) {
-    if (t.sch.lim == 1) run_step<LIM_FCT>(P, t.sch, a);
-    else run_step<LIM_NONE>(P, t.sch, a);
+    if (nt == 4) run_group_nt<4>(P, sc, a);
+    else if (nt == 2) run_group_nt<2>(P, sc, a);
+    else run_group_nt<1>(P, sc, a);
     CK(cudaGetLastError());
   }
-  std::swap(t.T, t.Tout);
+  for (int t = 0; t < nt; t++) std::swap(P.tr[first + t].T, P.tr[first + t].Tout);
+}
+
+static bool same_scheme(const TracerScheme &a, const TracerScheme &b) {
+  return a.hor == b.hor && a.ver == b.ver && a.lim == b.lim && a.ph == b.ph && a.pv == b.pv;
+}
+
+// batch sizes the engine launches: 4, 2 or 1 tracers
+static int batch_size(const EngineImpl &P, int first) {
+  int run = 1;
+  while (first + run < (int)P.tr.size() && run < NTMAX && same_scheme(P.tr[first].sch, P.tr[first + run].sch)) run++;
+  return run >= 4 ? 4 : (run >= 2 ? 2 : 1);
+}
+
+int Engine::launches_per_step() const {
+  const EngineImpl &P = *p_;
+  int n = 0;
+  for (int i = 0; i < (int)P.tr.size();) {
+    const int nt = batch_size(P, i);
+    n += P.tr[i].sch.lim == 1 ? 4 : 3;
+    i += nt;
+  }
+  return n;
+}
+
+void Engine::step_tracer(int id, double dt, bool refresh_ab) {
+  check_id(*p_, id);
+  run_batch(*p_, id, 1, dt, refresh_ab);
 }
 
 void Engine::step(double dt, bool refresh_ab) {
-  for (int i = 0; i < (int)p_->tr.size(); i++) step_tracer(i, dt, refresh_ab);
+  for (int i = 0; i < (int)p_->tr.size();) {
+    const int nt = batch_size(*p_, i);
+    run_batch(*p_, i, nt, dt, refresh_ab);
+    i += nt;
+  }
 }
 
 const char *const *Engine::kernel_kind_names(int *n) {

@@ -51,8 +51,8 @@ class Engine {
   // Device pointers / stream for benchmarking and tests.
   void *stream() const;
   void synchronize() const;
-  // Kernel launches issued per step_tracer call with the tracer's scheme.
-  int launches_per_tracer_step(int id) const;
+  // Kernel launches issued by one step() of every tracer.
+  int launches_per_step() const;
   // min, max, sum and NaN count of tracer id over (nl-1, nod2D) incl. dry
   // cells, in the reference's sequential order (src/fesom_analytic.F90:441-446).
   void stats(int id, double out4[4]) const;

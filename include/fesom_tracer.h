@@ -159,6 +159,11 @@ int tracer_set_device(int device);
 int tracer_launches_per_step(void);
 /* Device memory held by the engine, in bytes. */
 long long tracer_device_bytes(void);
+/* Checks on the GPU that the reciprocal-based division of the FP64 kernels
+ * returns the same bits as IEEE a / b for n random operand pairs;
+ * *mismatches = number of differing results, example4 = (a, b, got,
+ * expected) of the first one. */
+int tracer_selftest_division(long long n, uint64_t seed, long long *mismatches, double *example4);
 /* Last error message of this thread ("" if none). */
 const char *tracer_last_error(void);
 

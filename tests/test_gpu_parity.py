@@ -216,3 +216,14 @@ def test_c2_size_one_step_bitwise_and_conservation(api):
     assert np.all(np.isfinite(G[wet]))
     s1, _ = volume_sum(api, G)
     assert abs(s1 - s0) <= 1e-12 * abs(s0)
+
+
+def test_reciprocal_division_is_correctly_rounded(lib):
+    """div_rcp (Markstein's correction from a once-per-cell reciprocal)
+    returns the bits of the IEEE quotient on 2^28 random operand pairs
+    spanning general, /6, area-like and thickness-like divisors."""
+    import ctypes
+    bad = ctypes.c_longlong(-1)
+    ex = np.zeros(4)
+    assert lib.tracer_selftest_division(1 << 28, 12345, ctypes.byref(bad), ex.ctypes.data_as(ctypes.c_void_p)) == 0
+    assert bad.value == 0, f"a={ex[0]!r} b={ex[1]!r} got={ex[2]!r} expected={ex[3]!r}"
