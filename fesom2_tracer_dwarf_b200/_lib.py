@@ -71,6 +71,8 @@ SIGNATURES = {
     "tracer_launches_per_step": (ctypes.c_int, []),
     "tracer_device_bytes": (ctypes.c_longlong, []),
     "tracer_selftest_division": (ctypes.c_int, [ctypes.c_longlong, ctypes.c_uint64, _vp, _vp]),
+    "tracer_advect_device_noalloc": (ctypes.c_int, [ctypes.c_int, _vp, _vp, _vp, ctypes.c_double]),
+    "tracer_noalloc_scratch_bytes": (ctypes.c_longlong, []),
     "tracer_last_error": (ctypes.c_char_p, []),
 }
 

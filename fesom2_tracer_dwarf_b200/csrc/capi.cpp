@@ -105,6 +105,16 @@ int check_ready() {
 
 }  // namespace
 
+namespace fesom {
+// The engine of the C ABI's global instance (nullptr before the first step or
+// tracer_init_for_advection) and its tracer count, for the allocation-free
+// entry point in noalloc.cu.
+Engine *capi_engine() { return g.eng.get(); }
+int capi_num_tracers() { return g.ntr; }
+bool capi_initialized() { return g.initialized; }
+int capi_fail(const std::string &msg) { return fail(msg); }
+}  // namespace fesom
+
 extern "C" {
 
 int tracer_init_mpi(int) { return 0; }

@@ -436,6 +436,43 @@ void Engine::step_tracer(int id, double dt, bool refresh_ab) {
   run_batch(*p_, id, 1, dt, refresh_ab);
 }
 
+size_t Engine::step_scratch_doubles() const {
+  const EngineImpl &P = *p_;
+  auto up = [](size_t n) { return (n + 31) / 32 * 32; };  // 256-byte pieces
+  const size_t es = up((size_t)P.mesh.edge2D * P.S), ns = up((size_t)P.mesh.nod2D * P.S);
+  return 2 * es + 4 * ns;
+}
+
+void Engine::step_with_scratch(int id, const double *T, const double *TAB, double *T_out, double dt,
+                               double *scratch, size_t scratch_doubles) {
+  EngineImpl &P = *p_;
+  check_id(P, id);
+  if (scratch_doubles < step_scratch_doubles()) throw std::length_error("scratch too small for this mesh");
+  auto up = [](size_t n) { return (n + 31) / 32 * 32; };
+  const size_t es = up((size_t)P.mesh.edge2D * P.S), ns = up((size_t)P.mesh.nod2D * P.S);
+  const TracerScheme &sc = P.tr[id].sch;
+  FusedArgs<double> a{};
+  a.T[0] = T;
+  a.TAB[0] = TAB;
+  a.T_out[0] = T_out;
+  a.vflux = scratch;
+  a.adf_h[0] = scratch + es;
+  a.adf_v[0] = scratch + 2 * es;
+  a.lo[0] = scratch + 2 * es + ns;
+  a.rp[0] = scratch + 2 * es + 2 * ns;
+  a.rm[0] = scratch + 2 * es + 3 * ns;
+  a.vel = P.vel;
+  a.W = P.W;
+  a.dt = dt;
+  a.ph = sc.ph;
+  a.pv = sc.pv;
+  if (P.mesh.nod2D > 0) {
+    run_group_nt<1>(P, sc, a);
+    CK(cudaGetLastError());
+  }
+  CK(cudaStreamSynchronize(P.stream));
+}
+
 void Engine::step(double dt, bool refresh_ab) {
   for (int i = 0; i < (int)p_->tr.size();) {
     const int nt = batch_size(*p_, i);

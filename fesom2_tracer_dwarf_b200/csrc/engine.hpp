@@ -62,6 +62,16 @@ class Engine {
   // kind into ms[kind] (kinds: kernel_kind_names()).  Returns launches done.
   int profile_steps(int nsteps, double dt, bool refresh_ab, double *ms, int nkinds);
   static const char *const *kernel_kind_names(int *n);
+  // Doubles of work space one tracer step needs (edge volume fluxes,
+  // antidiffusive fluxes, LO solution, limiter ratios).
+  size_t step_scratch_doubles() const;
+  // One step of tracer id's scheme on caller-owned device buffers in the
+  // engine's layout (nod2D columns of level stride S): T and TAB in, T_out
+  // out, with every work array carved from `scratch` (step_scratch_doubles()
+  // doubles, 256-byte aligned).  Allocates nothing; returns when the step is
+  // done.
+  void step_with_scratch(int id, const double *T, const double *TAB, double *T_out, double dt, double *scratch,
+                         size_t scratch_doubles);
 
  private:
   EngineImpl *p_;

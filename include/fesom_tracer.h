@@ -164,6 +164,21 @@ long long tracer_device_bytes(void);
  * *mismatches = number of differing results, example4 = (a, b, got,
  * expected) of the first one. */
 int tracer_selftest_division(long long n, uint64_t seed, long long *mismatches, double *example4);
+/* No counterpart in the reference.  One step of tracer tracer_id (its scheme,
+ * the loaded mesh and flow) on caller-owned DEVICE buffers, allocating no
+ * device memory: for callers whose runtime has reserved the GPU's memory for
+ * its own pool, or whose time loop must not allocate.  T_dev, TAB_dev (in) and
+ * T_out_dev (out, not aliasing either) hold nod2D columns of level stride S
+ * (tracer_mesh_dims()[5]) of doubles.  Work space comes from a 64 MiB
+ * static device array (tracer_noalloc_scratch_bytes()) shared by every call:
+ * meshes needing more are rejected with -1; calls that overlap on the GPU
+ * race.  The device state must exist (tracer_init_for_advection); the first
+ * call on a device looks up the array's device address and should come
+ * before any stream capture.  Returns after the step has finished. */
+int tracer_advect_device_noalloc(int tracer_id, const double *T_dev, const double *TAB_dev,
+                                 double *T_out_dev, double dt);
+/* Size in bytes of the static work array of tracer_advect_device_noalloc. */
+long long tracer_noalloc_scratch_bytes(void);
 /* Last error message of this thread ("" if none). */
 const char *tracer_last_error(void);
 
