@@ -147,7 +147,7 @@ __device__ __forceinline__ void ring_mean_n(const DMeshT<R> &m, const R *const *
 }
 
 template <typename R, int NT, int HOR, int LIM>
-__global__ void __launch_bounds__(kThreads) k_edge(DMeshT<R> m, FusedArgs<R> a) {
+__global__ void __launch_bounds__(kThreads, 4) k_edge(DMeshT<R> m, FusedArgs<R> a) {
   extern __shared__ int smem[];
   int *s_off = smem, *s_item = smem + kMaxItemsPerBlock + 1;
   const CellMap cm = map_cells(m.edge_sched, s_off, s_item);
@@ -221,7 +221,7 @@ __device__ __forceinline__ R ppm_slope(R Tm1, R T0, R Tp1, R c1, R c2, R c3) {
 }
 
 template <typename R, int NT, int VER, int LIM>
-__global__ void __launch_bounds__(kThreads) k_col1(DMeshT<R> m, FusedArgs<R> a) {
+__global__ void __launch_bounds__(kThreads, 4) k_col1(DMeshT<R> m, FusedArgs<R> a) {
   extern __shared__ int smem[];
   int *s_off = smem, *s_item = smem + kMaxItemsPerBlock + 1;
   R *s_acc = (R *)(smem + kMaxItemsPerBlock + 1 + kMaxCellsPerBlock + 1);  // 8-byte aligned below
@@ -239,13 +239,14 @@ __global__ void __launch_bounds__(kThreads) k_col1(DMeshT<R> m, FusedArgs<R> a) 
       R acc[NTMAX];
       for (int t = 0; t < NT; t++) acc[t] = R(0);
       for (int p = m.ne_ptr[n]; p < m.ne_ptr[n + 1]; p++) {
-        const int code = m.ne[p], e = code >> 1;
-        if (nz > m.edge_lev[e].y) continue;
-        const R vf = a.vflux[(size_t)e * S + k];
-        const int2 nn = m.edge_nodes[e];
+        const int4 q = m.ne4[p];
+        if (nz > q.z) continue;
+        const bool second = q.x & 1;
+        const R vf = a.vflux[(size_t)(q.x >> 1) * S + k];
+        const size_t o1 = (size_t)(second ? q.y : n) * S + k, o2 = (size_t)(second ? n : q.y) * S + k;
         for (int t = 0; t < NT; t++) {
-          const R F = upw1_flux(vf, a.T[t][(size_t)nn.x * S + k], a.T[t][(size_t)nn.y * S + k]);
-          acc[t] = (code & 1) ? acc[t] - F : acc[t] + F;
+          const R F = upw1_flux(vf, a.T[t][o1], a.T[t][o2]);
+          acc[t] = second ? acc[t] - F : acc[t] + F;
         }
       }
       for (int t = 0; t < NT; t++) s_acc[t * kMaxCellsPerBlock + lc] = acc[t];
@@ -453,11 +454,11 @@ __global__ void __launch_bounds__(kThreads) k_col2(DMeshT<R> m, FusedArgs<R> a) 
       fm[t] = R(0) + (fmin2(R(0), av[k]) + fmin2(R(0), -av[k + 1]));
     }
     for (int p = m.ne_ptr[n]; p < m.ne_ptr[n + 1]; p++) {
-      const int code = m.ne[p], e = code >> 1;
-      if (nz > m.edge_lev[e].y) continue;
+      const int4 q = m.ne4[p];
+      if (nz > q.z) continue;
       for (int t = 0; t < NT; t++) {
-        const R f = a.adf_h[t][(size_t)e * S + k];
-        if (code & 1) {
+        const R f = a.adf_h[t][(size_t)(q.x >> 1) * S + k];
+        if (q.x & 1) {
           fp[t] = fp[t] + fmax2(R(0), -f);
           fm[t] = fm[t] + fmin2(R(0), -f);
         } else {
@@ -509,7 +510,7 @@ __device__ __forceinline__ R limit_v(const R *av, const R *rp, const R *rm, int 
 // k_col3: limiting + flux2dtracer + update
 // ---------------------------------------------------------------------------
 template <typename R, int NT, int LIM>
-__global__ void __launch_bounds__(kThreads) k_col3(DMeshT<R> m, FusedArgs<R> a) {
+__global__ void __launch_bounds__(kThreads, 4) k_col3(DMeshT<R> m, FusedArgs<R> a) {
   extern __shared__ int smem[];
   int *s_off = smem, *s_item = smem + kMaxItemsPerBlock + 1;
   const CellMap cm = map_cells(m.node_sched, s_off, s_item);
@@ -535,12 +536,12 @@ __global__ void __launch_bounds__(kThreads) k_col3(DMeshT<R> m, FusedArgs<R> a) 
       dh[t] = R(0);
     }
     for (int p = m.ne_ptr[n]; p < m.ne_ptr[n + 1]; p++) {
-      const int code = m.ne[p], e = code >> 1;
-      if (nz > m.edge_lev[e].y) continue;
-      const int2 nn = m.edge_nodes[e];
-      const size_t o1 = (size_t)nn.x * S + k, o2 = (size_t)nn.y * S + k;
+      const int4 q = m.ne4[p];
+      if (nz > q.z) continue;
+      const bool second = q.x & 1;
+      const size_t o1 = (size_t)(second ? q.y : n) * S + k, o2 = (size_t)(second ? n : q.y) * S + k;
       for (int t = 0; t < NT; t++) {
-        R f = a.adf_h[t][(size_t)e * S + k];
+        R f = a.adf_h[t][(size_t)(q.x >> 1) * S + k];
         if (LIM == LIM_FCT) {
           R ae = R(1);
           if (f >= R(0)) {
@@ -553,7 +554,7 @@ __global__ void __launch_bounds__(kThreads) k_col3(DMeshT<R> m, FusedArgs<R> a) 
           f = ae * f;
         }
         const R term = div_rcp(f * a.dt, asv, yasv);
-        dh[t] = (code & 1) ? dh[t] - term : dh[t] + term;
+        dh[t] = second ? dh[t] - term : dh[t] + term;
       }
     }
     for (int t = 0; t < NT; t++) {

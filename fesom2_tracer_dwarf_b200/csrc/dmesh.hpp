@@ -1,5 +1,10 @@
 // Device-resident mesh tables and work schedules.
 //
+// Edge arrays are stored in "slot" order -- edges sorted by their first node,
+// so the edges of neighbouring nodes sit next to each other -- while every
+// node-side gather still walks its edges in ascending edge id, the order of
+// the reference's serial scatters.
+//
 // HBM layout: every 3D field is column-major per node (or element, or edge)
 // with the level index fastest and a padded level stride S (multiple of 4
 // levels, so every column starts on a 32-byte sector for FP64).  A cell
@@ -45,7 +50,8 @@ struct DMeshT {
   const int *ring_ptr;      // (N+1)
   const int *ring_elem;
   const int *ne_ptr;        // (N+1)
-  const int *ne;            // (edge << 1) | second
+  const int4 *ne4;          // per incidence, in ascending edge id:
+                            // (slot << 1 | node is the edge's 2nd node, other node, edge levels, 0)
   const R *zbar;            // (nl)
   const R *Z;               // (nl-1)
   // 3D geometry, stride S

@@ -161,20 +161,33 @@ Engine::Engine(const MeshHost &mesh) : p_(new EngineImpl) {
   DMeshT<double> &d = P.dm;
   d.N = N; d.T = T; d.E = E; d.nl = nl; d.S = P.S;
 
+  // slot order: edges sorted by their smaller node id (stable in edge id)
+  std::vector<int> slot_edge(E), edge_slot(E);
+  for (int e = 0; e < E; e++) slot_edge[e] = e;
+  std::stable_sort(slot_edge.begin(), slot_edge.end(), [&](int a, int b) {
+    return std::min(M.edge_nodes[2 * a], M.edge_nodes[2 * a + 1]) <
+           std::min(M.edge_nodes[2 * b], M.edge_nodes[2 * b + 1]);
+  });
+  for (int s = 0; s < E; s++) edge_slot[slot_edge[s]] = s;
   std::vector<int2> en(E), et(E), el(E), ud(E);
-  for (int e = 0; e < E; e++) {
-    en[e] = make_int2(M.edge_nodes[2 * e], M.edge_nodes[2 * e + 1]);
-    et[e] = make_int2(M.edge_tri[2 * e], M.edge_tri[2 * e + 1]);
-    el[e] = make_int2(M.edge_shared_levels(e), M.edge_levels(e));
-    ud[e] = make_int2(M.up_dn_tri[2 * e], M.up_dn_tri[2 * e + 1]);
+  std::vector<double> ecross(4 * (size_t)E), edxdy(2 * (size_t)E), ea(E);
+  for (int s = 0; s < E; s++) {
+    const int e = slot_edge[s];
+    en[s] = make_int2(M.edge_nodes[2 * e], M.edge_nodes[2 * e + 1]);
+    et[s] = make_int2(M.edge_tri[2 * e], M.edge_tri[2 * e + 1]);
+    el[s] = make_int2(M.edge_shared_levels(e), M.edge_levels(e));
+    ud[s] = make_int2(M.up_dn_tri[2 * e], M.up_dn_tri[2 * e + 1]);
+    for (int q = 0; q < 4; q++) ecross[4 * (size_t)s + q] = M.edge_cross[4 * (size_t)e + q];
+    for (int q = 0; q < 2; q++) edxdy[2 * (size_t)s + q] = M.edge_dxdy[2 * (size_t)e + q];
+    ea[s] = M.edge_a[e];
   }
   d.edge_nodes = P.upload(en);
   d.edge_tri = P.upload(et);
   d.edge_lev = P.upload(el);
   d.up_dn = P.upload(ud);
-  d.edge_cross = P.upload(M.edge_cross);
-  d.edge_dxdy = P.upload(M.edge_dxdy);
-  d.edge_a = P.upload(M.edge_a);
+  d.edge_cross = P.upload(ecross);
+  d.edge_dxdy = P.upload(edxdy);
+  d.edge_a = P.upload(ea);
   d.nlev_elem = P.upload(M.nlev_elem);
   d.nlev_node = P.upload(M.nlev_node);
   d.nlev_node_min = P.upload(M.nlev_node_min);
@@ -185,7 +198,16 @@ Engine::Engine(const MeshHost &mesh) : p_(new EngineImpl) {
   d.ring_ptr = P.upload(M.ring_ptr);
   d.ring_elem = P.upload(M.ring_elem);
   d.ne_ptr = P.upload(M.node_edge_ptr);
-  d.ne = P.upload(M.node_edge);
+  {
+    std::vector<int4> ne4(M.node_edge.size());
+    for (int n = 0; n < N; n++)
+      for (int p = M.node_edge_ptr[n]; p < M.node_edge_ptr[n + 1]; p++) {
+        const int code = M.node_edge[p], e = code >> 1, second = code & 1;
+        const int other = M.edge_nodes[2 * e + (second ? 0 : 1)];
+        ne4[p] = make_int4((edge_slot[e] << 1) | second, other, M.edge_levels(e), 0);
+      }
+    d.ne4 = P.upload(ne4);
+  }
   d.zbar = P.upload(M.zbar);
   d.Z = P.upload(M.Z);
   d.area = P.upload_cols(M.area.data(), nl, N, nl);
@@ -201,7 +223,7 @@ Engine::Engine(const MeshHost &mesh) : p_(new EngineImpl) {
   d.node_sched.blk = P.upload(blk);
   d.node_sched.nblk = (int)blk.size() - 1;
   cnt.assign(E, 0);
-  for (int e = 0; e < E; e++) cnt[e] = M.edge_levels(e);
+  for (int s = 0; s < E; s++) cnt[s] = M.edge_levels(slot_edge[s]);
   build_sched(cnt, off, blk, d.edge_sched.max_items);
   d.edge_sched.cell_off = P.upload(off);
   d.edge_sched.blk = P.upload(blk);
