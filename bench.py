@@ -3,10 +3,13 @@
 
 Workload (the plain method at scale): doubly periodic analytic mesh
 nx = ny = 1000 (998,001 nodes, 2,994,003 edges, 1,996,002 triangles), 64
-levels, per-node bottom level uniform in [3, 64] (seed 0), a seeded layered
-flow with |u| <= 1 m/s at CFL 0.5 (dt = 0.5 dx / 1 m/s), two tracers
+levels, smooth seeded bathymetry with per-node bottom level uniform in
+[3, 64] (seed 0), a seeded smooth layered flow that is discretely
+divergence-free (|u| <= 1 m/s, w from continuity, dt at CFL 0.5 of the
+faster of the horizontal and vertical crossings), two tracers
 (temperature-like U[0,20] + Gaussian blobs, salinity-like 35 + N(0, 0.5)),
-MUSCL + PPM + FCT in FP64, valuesAB := values each step.  One "step" advances
+MUSCL + PPM + FCT in FP64, valuesAB := values each step
+(fesom2_tracer_dwarf_b200.workloads.layered_flow_case).  One "step" advances
 both tracers once.  Metric: tracer cell-updates/s = wet cells x tracers /
 step time.
 
@@ -41,7 +44,10 @@ import numpy as np
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
-BYTES_PER_CELL = {"fp64": 112}  # 14 words per wet cell at storage precision
+# 14 words per wet cell and tracer at storage precision: 3 tracer words
+# (T read, T_AB read, T write) + 11 geometry / flow words
+BYTES_PER_CELL = {"fp64": 112, "fp32": 56, "bf16": 3 * 2 + 11 * 4, "fp16": 3 * 2 + 11 * 4}
+DTYPE = {"fp64": "f64", "fp32": "f32", "bf16": "bf16 storage / f32 compute", "fp16": "f16 storage / f32 compute"}
 L2_BYTES = 126 * 2**20
 
 
@@ -55,24 +61,19 @@ def parse():
     p.add_argument("--nl", type=int, default=64)
     p.add_argument("--e2e-steps", type=int, default=3)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--precision", default="fp64", choices=["fp64", "fp32", "bf16", "fp16"])
     return p.parse_args()
 
 
 def workload_name(nx, nl):
-    return f"periodic {nx}x{nx}x{nl}, bathymetry U[3,{nl}] seed 0, MUSCL+PPM+FCT, 2 tracers"
+    return (f"periodic {nx}x{nx}x{nl} (left-oriented edges), smooth bathymetry U[3,{nl}] seed 0, "
+            "divergence-free layered flow CFL 0.5, MUSCL+PPM+FCT, 2 tracers")
 
 
 def make_inputs(api, nx, nl):
-    from fesom2_tracer_dwarf_b200 import synth_bathymetry
-    N = api.lib.tracer_analytic_nodes(nx, nx, 1)
-    K = synth_bathymetry(N, nl, 0)
-    api.init_analytic(nx, nx, nl, periodic=True, full_rings=True, node_K=K)
-    uv, w = api.synth_velocity(seed=1, umax=1.0, mode2=0.5)
-    T = api.synth_tracer(seed=2, kind=0)
-    S = api.synth_tracer(seed=3, kind=1)
-    dt = 0.5 * (1.0e5 / (nx - 1)) / 1.0
-    cells = int((api.mesh_array("nlevels_nod2D") - 1).sum())
-    return K, uv, w, T, S, dt, cells
+    from fesom2_tracer_dwarf_b200.workloads import layered_flow_case
+    c = layered_flow_case(api, nx, nl, seed=0)
+    return c.K, c.uv, c.w, c.T, c.S, c.dt, c.wet_cells
 
 
 # ---------------------------------------------------------------------------
@@ -168,7 +169,8 @@ def cpu_rate(nx_sample, nl, steps, warmup=1):
     api.cleanup()
     o = pyoracle.Oracle(openmp=True)
     o.set_threads(os.cpu_count() or 1)
-    m = pyoracle.OracleMesh(o, nx_sample, nx_sample, nl, periodic=True, full_rings=True, node_K=K)
+    m = pyoracle.OracleMesh(o, nx_sample, nx_sample, nl, periodic=True, full_rings=True, node_K=K,
+                            left_oriented=True)
     N = m.nod2D
     vals = np.ascontiguousarray(np.stack([T.T, S.T]))  # (2, nod2D, nl-1): each tracer a Fortran (nl-1, nod2D) block
     ab = vals.copy()
@@ -229,6 +231,7 @@ def run_ours(args):
     if api.lib.tracer_set_device(local) != 0:
         raise RuntimeError(api.lib.tracer_last_error().decode())
     K, uv, w, T, S, dt, cells = make_inputs(api, args.nx, args.nl)
+    api.set_precision(args.precision)
     api.allocate_tracers(2)
     api.set_values(1, T)
     api.set_values(2, S)
@@ -293,25 +296,25 @@ def run_ours(args):
         t = torch.tensor([e2e_sec], dtype=torch.float64, device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_sec = float(t.item())
-    h2d = 2 * L * N * 8
+    h2d = 2 * L * N * 8  # the C ABI exchanges FP64 arrays whatever the device precision
     d2h = 2 * L * N * 8
 
     result = None
     if rank == 0:
         peak, peak_kind = measured_peaks()
-        alg_bytes_step = BYTES_PER_CELL["fp64"] * cells * 2
+        alg_bytes_step = BYTES_PER_CELL[args.precision] * cells * 2
         achieved = alg_bytes_step / (ms_per_step / 1e3) / 1e9
         traffic = committed_traffic()
         result = {
             "metric": "tracer cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "scaling": "weak", "vs_baseline": None, "dtype": DTYPE[args.precision], "data": "synthetic",
             "config": {"workload": workload_name(args.nx, args.nl), "wet_cells": cells, "tracers": 2,
                        "dt_s": dt, "parallelism": f"replicas x{world}",
                        "l2": f"inputs larger than L2 ({dev_bytes / 1e9:.1f} GB resident vs 0.13 GB L2)"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
-                         "kernel": "full step (all kernels of one step, 112 B/cell algorithmic)",
+                         "kernel": f"full step (all kernels of one step, {BYTES_PER_CELL[args.precision]} B/cell algorithmic)",
                          "peak_source": f"{peak_kind} hbm_gbs"},
             "kernel_ms_per_step": kernel_ms,
             "e2e": {"value": world * 2 * cells / e2e_sec, "unit": "cell-updates/s", "h2d_bytes_per_step": h2d,

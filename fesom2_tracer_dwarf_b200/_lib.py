@@ -54,12 +54,17 @@ SIGNATURES = {
     "tracer_set_velocity_elem": (ctypes.c_int, [_vp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     "tracer_set_values_ab": (ctypes.c_int, [ctypes.c_int, _vp, ctypes.c_int, ctypes.c_int]),
     "tracer_set_ab_refresh": (ctypes.c_int, [ctypes.c_int]),
+    "tracer_set_precision": (ctypes.c_int, [ctypes.c_int]),
+    "tracer_volume_sum": (ctypes.c_int, [ctypes.c_int, _vp]),
     "tracer_advect_steps": (ctypes.c_int, [ctypes.c_int, ctypes.c_double]),
     "tracer_get_values_id": (ctypes.c_int, [ctypes.c_int, _vp, ctypes.c_int, ctypes.c_int]),
     "tracer_get_stats_id": (ctypes.c_int, [ctypes.c_int, _vp]),
     "tracer_analytic_fields": (ctypes.c_int, [_vp] * 4),
     "tracer_synth_bathymetry": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_uint64, _vp]),
-    "tracer_synth_velocity": (ctypes.c_int, [ctypes.c_uint64, ctypes.c_double, ctypes.c_double, _vp, _vp]),
+    "tracer_synth_velocity": (ctypes.c_int, [ctypes.c_uint64, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                             _vp, _vp]),
+    "tracer_synth_bathymetry_smooth": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                                      ctypes.c_double, ctypes.c_uint64, _vp]),
     "tracer_synth_tracer": (ctypes.c_int, [ctypes.c_uint64, ctypes.c_int, _vp]),
     "tracer_mesh_dims": (ctypes.c_int, [_vp]),
     "tracer_mesh_len": (ctypes.c_long, [ctypes.c_char_p]),

@@ -68,11 +68,13 @@ __device__ __forceinline__ float div_rcp(float a, float b, float y) {
   return __fmaf_rn(r, y, q);
 }
 
-template <typename R>
+// R: compute and geometry type; TS: tracer storage type (R itself, or a
+// 16-bit float with R = float)
+template <typename R, typename TS>
 struct FusedArgs {
-  const R *T[NTMAX];      // values
-  const R *TAB[NTMAX];    // valuesAB (high-order fluxes)
-  R *T_out[NTMAX];
+  const TS *T[NTMAX];     // values
+  const TS *TAB[NTMAX];   // valuesAB (high-order fluxes)
+  TS *T_out[NTMAX];
   R *adf_h[NTMAX];        // (S, edge)
   R *adf_v[NTMAX];        // (S, node) interfaces
   R *lo[NTMAX];           // (S, node)
@@ -110,21 +112,21 @@ __device__ __forceinline__ CellMap map_cells(const DSched &sc, int *s_off, int *
 // ---------------------------------------------------------------------------
 // k_edge
 // ---------------------------------------------------------------------------
-template <typename R>
-__device__ __forceinline__ void trxy_n(const DMeshT<R> &m, const R *const *tab, int NT, int elem, int k, R *gx, R *gy) {
+template <typename R, typename TS>
+__device__ __forceinline__ void trxy_n(const DMeshT<R> &m, const TS *const *tab, int NT, int elem, int k, R *gx, R *gy) {
   const int *en = m.elem_nodes + 3 * elem;
   const int a = en[0], b = en[1], c = en[2];
   const R *gs = m.grad_sca + 6 * elem;
   const R g0 = gs[0], g1 = gs[1], g2 = gs[2], g3 = gs[3], g4 = gs[4], g5 = gs[5];
   for (int t = 0; t < NT; t++) {
-    const R t1 = tab[t][(size_t)a * m.S + k], t2 = tab[t][(size_t)b * m.S + k], t3 = tab[t][(size_t)c * m.S + k];
+    const R t1 = R(tab[t][(size_t)a * m.S + k]), t2 = R(tab[t][(size_t)b * m.S + k]), t3 = R(tab[t][(size_t)c * m.S + k]);
     gx[t] = (g0 * t1 + g1 * t2) + g2 * t3;
     gy[t] = (g3 * t1 + g4 * t2) + g5 * t3;
   }
 }
 
-template <typename R>
-__device__ __forceinline__ void ring_mean_n(const DMeshT<R> &m, const R *const *tab, int NT, int n, int k, R *gx, R *gy) {
+template <typename R, typename TS>
+__device__ __forceinline__ void ring_mean_n(const DMeshT<R> &m, const TS *const *tab, int NT, int n, int k, R *gx, R *gy) {
   R tvol = R(0), tx[NTMAX], ty[NTMAX];
   for (int t = 0; t < NT; t++) { tx[t] = R(0); ty[t] = R(0); }
   const int nz = k + 1;
@@ -146,8 +148,8 @@ __device__ __forceinline__ void ring_mean_n(const DMeshT<R> &m, const R *const *
   }
 }
 
-template <typename R, int NT, int HOR, int LIM>
-__global__ void __launch_bounds__(kThreads, 4) k_edge(DMeshT<R> m, FusedArgs<R> a) {
+template <typename R, typename TS, int NT, int HOR, int LIM>
+__global__ void __launch_bounds__(kThreads, 4) k_edge(DMeshT<R> m, FusedArgs<R, TS> a) {
   extern __shared__ int smem[];
   int *s_off = smem, *s_item = smem + kMaxItemsPerBlock + 1;
   const CellMap cm = map_cells(m.edge_sched, s_off, s_item);
@@ -161,8 +163,8 @@ __global__ void __launch_bounds__(kThreads, 4) k_edge(DMeshT<R> m, FusedArgs<R> 
     const size_t o1 = (size_t)c.n1 * m.S + k, o2 = (size_t)c.n2 * m.S + k;
     if (HOR == HOR_UPW1) {
       for (int t = 0; t < NT; t++) {
-        const R flo = (LIM == LIM_FCT) ? upw1_flux(vflux, a.T[t][o1], a.T[t][o2]) : R(0);
-        a.adf_h[t][o] = upw1_flux(vflux, a.TAB[t][o1], a.TAB[t][o2]) - flo;
+        const R flo = (LIM == LIM_FCT) ? upw1_flux(vflux, R(a.T[t][o1]), R(a.T[t][o2])) : R(0);
+        a.adf_h[t][o] = upw1_flux(vflux, R(a.TAB[t][o1]), R(a.TAB[t][o2])) - flo;
       }
       continue;
     }
@@ -185,7 +187,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_edge(DMeshT<R> m, FusedArgs<R> 
       c_lo2 = (m.nbl[c.n2] - (k + 1) >= 0) ? R(1) : R(0);
     }
     for (int t = 0; t < NT; t++) {
-      const R t1 = a.TAB[t][o1], t2 = a.TAB[t][o2];
+      const R t1 = R(a.TAB[t][o1]), t2 = R(a.TAB[t][o2]);
       R Tmean2, Tmean1;
       // lib/oce_adv_tra_hor.F90:454-469 (MUSCL), :743-753 (MFCT, no c_lo)
       const R x2 = R(2) * (t2 - t1) + ex * aa * gdx[t] + ey * re * gdy[t];
@@ -199,7 +201,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_edge(DMeshT<R> m, FusedArgs<R> 
       }
       const R cHO = (vflux + fabs(vflux)) * Tmean1 + (vflux - fabs(vflux)) * Tmean2;
       const R ho = -(R(0.5) * (R(1) - a.ph) * cHO) - vflux * a.ph * R(0.5) * (Tmean1 + Tmean2);
-      const R flo = (LIM == LIM_FCT) ? upw1_flux(vflux, a.T[t][o1], a.T[t][o2]) : R(0);
+      const R flo = (LIM == LIM_FCT) ? upw1_flux(vflux, R(a.T[t][o1]), R(a.T[t][o2])) : R(0);
       a.adf_h[t][o] = ho - flo;
     }
   }
@@ -220,8 +222,8 @@ __device__ __forceinline__ R ppm_slope(R Tm1, R T0, R Tp1, R c1, R c2, R c3) {
   return d;
 }
 
-template <typename R, int NT, int VER, int LIM>
-__global__ void __launch_bounds__(kThreads, 4) k_col1(DMeshT<R> m, FusedArgs<R> a) {
+template <typename R, typename TS, int NT, int VER, int LIM>
+__global__ void __launch_bounds__(kThreads, 4) k_col1(DMeshT<R> m, FusedArgs<R, TS> a) {
   extern __shared__ int smem[];
   int *s_off = smem, *s_item = smem + kMaxItemsPerBlock + 1;
   R *s_acc = (R *)(smem + kMaxItemsPerBlock + 1 + kMaxCellsPerBlock + 1);  // 8-byte aligned below
@@ -245,7 +247,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_col1(DMeshT<R> m, FusedArgs<R> 
         const R vf = a.vflux[(size_t)(q.x >> 1) * S + k];
         const size_t o1 = (size_t)(second ? q.y : n) * S + k, o2 = (size_t)(second ? n : q.y) * S + k;
         for (int t = 0; t < NT; t++) {
-          const R F = upw1_flux(vf, a.T[t][o1], a.T[t][o2]);
+          const R F = upw1_flux(vf, R(a.T[t][o1]), R(a.T[t][o2]));
           acc[t] = second ? acc[t] - F : acc[t] + F;
         }
       }
@@ -260,8 +262,8 @@ __global__ void __launch_bounds__(kThreads, 4) k_col1(DMeshT<R> m, FusedArgs<R> 
         const R c2 = (R(2) * dzjm1 + dzj) / (dzjp1 + dzj);
         const R c3 = (dzj + R(2) * dzjp1) / (dzjm1 + dzj);
         for (int t = 0; t < NT; t++) {
-          const R *Tc = a.TAB[t] + (size_t)n * S;
-          s_slope[t * kMaxCellsPerBlock + lc] = ppm_slope(Tc[k - 1], Tc[k], Tc[k + 1], c1, c2, c3);
+          const TS *Tc = a.TAB[t] + (size_t)n * S;
+          s_slope[t * kMaxCellsPerBlock + lc] = ppm_slope(R(Tc[k - 1]), R(Tc[k]), R(Tc[k + 1]), c1, c2, c3);
         }
       }
     }
@@ -276,17 +278,17 @@ __global__ void __launch_bounds__(kThreads, 4) k_col1(DMeshT<R> m, FusedArgs<R> 
       const R *HN = m.hnode_new + (size_t)n * S;
       const R *Wc = a.W + (size_t)n * S;
       if (i == 1) {
-        for (int t = 0; t < NT; t++) s_tv[t * kMaxCellsPerBlock + lc] = a.TAB[t][(size_t)n * S];
+        for (int t = 0; t < NT; t++) s_tv[t * kMaxCellsPerBlock + lc] = R(a.TAB[t][(size_t)n * S]);
       } else if (i == nlev - 1) {
         const R s = sgn1(Wc[nlev - 2]);
         for (int t = 0; t < NT; t++) {
-          const R *Tc = a.TAB[t] + (size_t)n * S;
-          s_tv[t * kMaxCellsPerBlock + lc] = -Tc[nlev - 3] * fmin2(s, R(0)) + Tc[nlev - 2] * fmax2(s, R(0));
+          const TS *Tc = a.TAB[t] + (size_t)n * S;
+          s_tv[t * kMaxCellsPerBlock + lc] = -R(Tc[nlev - 3]) * fmin2(s, R(0)) + R(Tc[nlev - 2]) * fmax2(s, R(0));
         }
       } else if (i == 2) {
         for (int t = 0; t < NT; t++) {
-          const R *Tc = a.TAB[t] + (size_t)n * S;
-          s_tv[t * kMaxCellsPerBlock + lc] = R(0.5) * (Tc[0] + Tc[1]);
+          const TS *Tc = a.TAB[t] + (size_t)n * S;
+          s_tv[t * kMaxCellsPerBlock + lc] = R(0.5) * (R(Tc[0]) + R(Tc[1]));
         }
       } else {
         // lib/oce_adv_tra_ver.F90:545-553 with nz = i - 1
@@ -299,8 +301,8 @@ __global__ void __launch_bounds__(kThreads, 4) k_col1(DMeshT<R> m, FusedArgs<R> 
         const R D = dzj * (dzjm1 + dzj) / (R(2) * dzj + dzjp1);
         const R E = dzjp1 * (dzjp1 + dzjp2) / (dzj + R(2) * dzjp1);
         for (int t = 0; t < NT; t++) {
-          const R *Tc = a.TAB[t] + (size_t)n * S;
-          const R T0 = Tc[nzz - 1], T1 = Tc[nzz];
+          const TS *Tc = a.TAB[t] + (size_t)n * S;
+          const R T0 = R(Tc[nzz - 1]), T1 = R(Tc[nzz]);
           const R dj = s_slope[t * kMaxCellsPerBlock + lc - 1];   // layer nzz
           const R djp1 = s_slope[t * kMaxCellsPerBlock + lc];     // layer nzz + 1
           s_tv[t * kMaxCellsPerBlock + lc] = T0 + A * (T1 - T0) + B * (C * (T1 - T0) - D * djp1 + E * dj);
@@ -322,7 +324,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_col1(DMeshT<R> m, FusedArgs<R> 
       for (int t = 0; t < NT; t++) lov[t] = R(0);
       if (LIM == LIM_FCT) {
         for (int t = 0; t < NT; t++) {
-          Col<R> cT;
+          Col<R, TS> cT;
           cT.T = a.T[t] + col; cT.W = Wc; cT.A = Ac; cT.nlev = nlev;
           lov[t] = ver_upw1(cT, i);
         }
@@ -344,9 +346,9 @@ __global__ void __launch_bounds__(kThreads, 4) k_col1(DMeshT<R> m, FusedArgs<R> 
             const R x = (w > R(0)) ? fmin2(w * a.dt / dzj, R(1)) : fmin2(-(w * a.dt / dzj), R(1));
             const R two3 = R(2.0 / 3.0);
             for (int t = 0; t < NT; t++) {
-              const R Tc = a.TAB[t][col + jl - 1];
+              const R Tc = R(a.TAB[t][col + jl - 1]);
               R aL = s_tv[t * kMaxCellsPerBlock + sl];
-              R aR = (jl + 1 == nlev) ? a.TAB[t][col + nlev - 2] : s_tv[t * kMaxCellsPerBlock + sl + 1];
+              R aR = (jl + 1 == nlev) ? R(a.TAB[t][col + nlev - 2]) : s_tv[t * kMaxCellsPerBlock + sl + 1];
               if ((aR - Tc) * (Tc - aL) <= R(0)) { aL = Tc; aR = Tc; }
               if ((aR - aL) * (Tc - R(0.5) * (aL + aR)) > (aR - aL) * (aR - aL) / R(6)) aL = R(3) * Tc - R(2) * aR;
               if ((aR - aL) * (Tc - R(0.5) * (aR + aL)) < -((aR - aL) * (aR - aL) / R(6))) aR = R(3) * Tc - R(2) * aL;
@@ -360,7 +362,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_col1(DMeshT<R> m, FusedArgs<R> 
         }
       } else {
         for (int t = 0; t < NT; t++) {
-          Col<R> cA;
+          Col<R, TS> cA;
           cA.T = a.TAB[t] + col; cA.W = Wc; cA.A = Ac; cA.nlev = nlev;
           if (VER == VER_QR4C) hov[t] = ver_qr4c(cA, m.zbar, m.Z, i, a.pv, lov[t]);
           else if (VER == VER_CDIFF) hov[t] = ver_cdiff(cA, i, lov[t]);
@@ -387,7 +389,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_col1(DMeshT<R> m, FusedArgs<R> 
       const R fk = s_fv[t * kMaxCellsPerBlock + lc];
       const R fk1 = (k + 2 == nlev) ? R(0) : s_fv[t * kMaxCellsPerBlock + lc + 1];
       const R acc = s_acc[t * kMaxCellsPerBlock + lc];
-      const R num = a.T[t][o] * h + div_rcp((acc + (fk - fk1)) * a.dt, asv, yasv);
+      const R num = R(a.T[t][o]) * h + div_rcp((acc + (fk - fk1)) * a.dt, asv, yasv);
       a.lo[t][o] = div_rcp(num, hn, yhn);
     }
   }
@@ -396,8 +398,8 @@ __global__ void __launch_bounds__(kThreads, 4) k_col1(DMeshT<R> m, FusedArgs<R> 
 // ---------------------------------------------------------------------------
 // k_col2: bounds, in/out sums, ratios (lib/oce_adv_tra_fct.F90:105-374)
 // ---------------------------------------------------------------------------
-template <typename R, int NT>
-__global__ void __launch_bounds__(kThreads) k_col2(DMeshT<R> m, FusedArgs<R> a) {
+template <typename R, typename TS, int NT>
+__global__ void __launch_bounds__(kThreads) k_col2(DMeshT<R> m, FusedArgs<R, TS> a) {
   extern __shared__ int smem[];
   int *s_off = smem, *s_item = smem + kMaxItemsPerBlock + 1;
   R *s_mx = (R *)(smem + kMaxItemsPerBlock + 1 + kMaxCellsPerBlock + 1);
@@ -423,7 +425,7 @@ __global__ void __launch_bounds__(kThreads) k_col2(DMeshT<R> m, FusedArgs<R> a) 
         if (wet) {
           const size_t o0 = (size_t)e0 * S + k, o1 = (size_t)e1 * S + k, o2 = (size_t)e2 * S + k;
           const R l0 = a.lo[t][o0], l1 = a.lo[t][o1], l2 = a.lo[t][o2];
-          const R t0 = a.T[t][o0], t1 = a.T[t][o1], t2 = a.T[t][o2];
+          const R t0 = R(a.T[t][o0]), t1 = R(a.T[t][o1]), t2 = R(a.T[t][o2]);
           amx = fmax3(fmax2(l0, t0), fmax2(l1, t1), fmax2(l2, t2));
           amn = fmin3(fmin2(l0, t0), fmin2(l1, t1), fmin2(l2, t2));
         } else {
@@ -480,10 +482,20 @@ __global__ void __launch_bounds__(kThreads) k_col2(DMeshT<R> m, FusedArgs<R> a) 
         bmax = fmax3(s_mx[b - 1], s_mx[b], s_mx[b + 1]) - LO;
         bmin = fmin3(s_mn[b - 1], s_mn[b], s_mn[b + 1]) - LO;
       }
-      R flux = div_rcp(fp[t] * a.dt, asv, yasv) + eps;
-      a.rp[t][o] = fmin2(R(1), bmax / flux);
-      flux = div_rcp(fm[t] * a.dt, asv, yasv) - eps;
-      a.rm[t][o] = fmin2(R(1), bmin / flux);
+      if constexpr (sizeof(R) == 8) {
+        R flux = div_rcp(fp[t] * a.dt, asv, yasv) + eps;
+        a.rp[t][o] = fmin2(R(1), bmax / flux);
+        flux = div_rcp(fm[t] * a.dt, asv, yasv) - eps;
+        a.rm[t][o] = fmin2(R(1), bmin / flux);
+      } else {
+        // FP32 arithmetic: the ratio denominators, where cancellation with
+        // flux_eps matters, are formed and divided in FP64
+        const double e64 = (double)1e-16f, dt64 = (double)a.dt, asv64 = (double)asv;
+        double flux = (double)fp[t] * dt64 / asv64 + e64;
+        a.rp[t][o] = (R)fmin2(1.0, (double)bmax / flux);
+        flux = (double)fm[t] * dt64 / asv64 - e64;
+        a.rm[t][o] = (R)fmin2(1.0, (double)bmin / flux);
+      }
     }
   }
 }
@@ -509,8 +521,8 @@ __device__ __forceinline__ R limit_v(const R *av, const R *rp, const R *rm, int 
 // ---------------------------------------------------------------------------
 // k_col3: limiting + flux2dtracer + update
 // ---------------------------------------------------------------------------
-template <typename R, int NT, int LIM>
-__global__ void __launch_bounds__(kThreads, 4) k_col3(DMeshT<R> m, FusedArgs<R> a) {
+template <typename R, typename TS, int NT, int LIM>
+__global__ void __launch_bounds__(kThreads, 4) k_col3(DMeshT<R> m, FusedArgs<R, TS> a) {
   extern __shared__ int smem[];
   int *s_off = smem, *s_item = smem + kMaxItemsPerBlock + 1;
   const CellMap cm = map_cells(m.node_sched, s_off, s_item);
@@ -526,7 +538,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_col3(DMeshT<R> m, FusedArgs<R> 
       const R *av = a.adf_v[t] + col;
       dv[t] = R(0);
       if (LIM == LIM_FCT) {
-        dv[t] = dv[t] - a.T[t][o] * m.hnode[o] + a.lo[t][o] * hn;
+        dv[t] = dv[t] - R(a.T[t][o]) * m.hnode[o] + a.lo[t][o] * hn;
         const R fk = limit_v(av, a.rp[t] + col, a.rm[t] + col, nz, nlev);
         const R fk1 = limit_v(av, a.rp[t] + col, a.rm[t] + col, nz + 1, nlev);
         dv[t] = dv[t] + div_rcp((fk - fk1) * a.dt, asv, yasv);
@@ -559,13 +571,12 @@ __global__ void __launch_bounds__(kThreads, 4) k_col3(DMeshT<R> m, FusedArgs<R> 
     }
     for (int t = 0; t < NT; t++) {
       const R del = R(0) + dh[t] + dv[t];
-      a.T_out[t][o] = a.T[t][o] + div_rcp(del, hn, yhn);
+      a.T_out[t][o] = TS(R(a.T[t][o]) + div_rcp(del, hn, yhn));
     }
   }
 }
 
 // dynamic shared memory of each kernel
-template <typename R>
 constexpr size_t smem_edge() { return sizeof(int) * (kMaxItemsPerBlock + 1 + kMaxCellsPerBlock + 1); }
 template <typename R>
 constexpr size_t smem_col(int nt, int arrays) {

@@ -32,6 +32,7 @@ struct State {
   std::vector<std::vector<double>> pend_values, pend_ab;
   std::vector<double> pend_uv, pend_w;  // uv in (2, nl-1, elem2D)
   bool pend_vel = false;
+  Precision prec = Precision::FP64;
 };
 State g;
 
@@ -56,7 +57,7 @@ int guarded(F &&f) {
 void ensure_engine() {
   if (g.eng) return;
   if (!g.mesh) throw std::runtime_error("no mesh connectivity: use tracer_init_analytic or tracer_set_mesh_arrays");
-  g.eng.reset(new Engine(*g.mesh));
+  g.eng.reset(new Engine(*g.mesh, g.prec));
   if (g.ntr > 0) {
     g.eng->allocate_tracers(g.ntr);
     for (int i = 0; i < g.ntr; i++) {
@@ -285,14 +286,15 @@ int tracer_init_for_advection(void) {
 }
 
 int tracer_init_analytic(int nx, int ny, int nl, double Lx, double Ly, double max_depth, int periodic,
-                         int full_rings, const int *node_K) {
+                         int options, const int *node_K) {
   return guarded([&] {
     if (node_K) {
       int nn = analytic_nodes(nx, ny, periodic != 0);
       for (int i = 0; i < nn; i++)
         if (node_K[i] < 3 || node_K[i] > nl) return fail("node_K outside [3, nl]");
     }
-    install_mesh(build_analytic_mesh(nx, ny, nl, Lx, Ly, max_depth, periodic != 0, full_rings != 0, node_K));
+    install_mesh(build_analytic_mesh(nx, ny, nl, Lx, Ly, max_depth, periodic != 0, (options & 1) != 0, node_K,
+                                     (options & 2) != 0));
     g.initialized = true;
     return 0;
   });
@@ -372,6 +374,35 @@ int tracer_set_scheme(int tracer_id, const char *hor, const char *ver, const cha
     if (tracer_id < 1 || tracer_id > g.ntr) return fail("invalid tracer_id " + std::to_string(tracer_id));
     g.schemes[tracer_id - 1] = parse_scheme(hor, ver, lim, ph, pv);
     if (g.eng) g.eng->set_scheme(tracer_id - 1, g.schemes[tracer_id - 1]);
+    return 0;
+  });
+}
+
+int tracer_set_precision(int mode) {
+  if (mode < 0 || mode > 3) return fail("precision mode must be 0 (FP64), 1 (FP32), 2 (BF16 storage) or 3 (FP16 storage)");
+  const Precision p = (Precision)mode;
+  if (g.eng && g.eng->precision() != p) {
+    // rebuild the device state in the new mode, keeping the tracer values
+    std::vector<std::vector<double>> keep(g.ntr);
+    for (int i = 0; i < g.ntr; i++) {
+      keep[i].resize((size_t)(g.nl - 1) * g.nod2D);
+      g.eng->get_values(i, keep[i].data());
+    }
+    g.eng.reset();
+    g.pend_values = keep;
+    for (auto &ab : g.pend_ab) ab.clear();
+  }
+  g.prec = p;
+  return 0;
+}
+
+int tracer_volume_sum(int tracer_id, double *out2) {
+  return guarded([&] {
+    if (check_ready()) return -1;
+    if (tracer_id < 1 || tracer_id > g.ntr) return fail("invalid tracer_id " + std::to_string(tracer_id));
+    if (!out2) return fail("null output");
+    ensure_engine();
+    g.eng->volume_sum(tracer_id - 1, out2);
     return 0;
   });
 }
@@ -472,13 +503,21 @@ int tracer_synth_bathymetry(int nnodes, int nl, uint64_t seed, int *K) {
   });
 }
 
-int tracer_synth_velocity(uint64_t seed, double umax, double frac, double *uv, double *w) {
+int tracer_synth_bathymetry_smooth(int nx, int ny, int periodic, int nl, double corr_cells, uint64_t seed, int *K) {
+  return guarded([&] {
+    if (!K || nx < 2 || ny < 2 || nl < 3) return fail("invalid bathymetry request");
+    std::vector<int> k = synth_bathymetry_smooth(nx, ny, periodic != 0, nl, corr_cells, seed);
+    std::memcpy(K, k.data(), sizeof(int) * k.size());
+    return 0;
+  });
+}
+
+int tracer_synth_velocity(uint64_t seed, double umax, double frac, double baro, double *uv, double *w) {
   return guarded([&] {
     if (!g.mesh) return fail("no mesh");
-    std::vector<double> u, ww;
-    synth_velocity(*g.mesh, seed, umax, frac, u, ww);
-    if (uv) std::memcpy(uv, u.data(), u.size() * 8);
-    if (w) std::memcpy(w, ww.data(), ww.size() * 8);
+    const MeshHost &m = *g.mesh;
+    HugeArray<double> u(uv ? 0 : (size_t)2 * (m.nl - 1) * m.elem2D), ww(w ? 0 : (size_t)m.nl * m.nod2D);
+    synth_velocity(m, seed, umax, frac, baro, uv ? uv : u.data(), w ? w : ww.data());
     return 0;
   });
 }
@@ -486,9 +525,8 @@ int tracer_synth_velocity(uint64_t seed, double umax, double frac, double *uv, d
 int tracer_synth_tracer(uint64_t seed, int kind, double *values) {
   return guarded([&] {
     if (!g.mesh) return fail("no mesh");
-    std::vector<double> t;
-    synth_tracer(*g.mesh, seed, kind, t);
-    std::memcpy(values, t.data(), t.size() * 8);
+    if (!values) return fail("values is NULL");
+    synth_tracer(*g.mesh, seed, kind, values);
     return 0;
   });
 }

@@ -1,13 +1,15 @@
-// Engine: device memory, layout conversion, schedules and kernel dispatch.
+// Engine: device memory, layout conversion, schedules, batching and
+// dispatch to the per-precision kernel units (step_f64.cu, step_f32.cu).
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
 #include <algorithm>
-#include <mutex>
-#include <unordered_map>
 #include <cstring>
 #include <stdexcept>
 #include <string>
 
 #include "advect_fused.cuh"
-#include "engine.hpp"
+#include "engine_impl.hpp"
 
 namespace fesom {
 
@@ -17,14 +19,7 @@ thread_local std::string g_err;
 const char *last_error() { return g_err.c_str(); }
 void set_last_error(const std::string &s) { g_err = s; }
 
-#define CK(x)                                                                                 \
-  do {                                                                                        \
-    cudaError_t e_ = (x);                                                                     \
-    if (e_ != cudaSuccess) throw std::runtime_error(std::string(#x) + ": " + cudaGetErrorString(e_)); \
-  } while (0)
-
 namespace {
-
 
 void build_sched(const std::vector<int> &counts, std::vector<int> &off, std::vector<int> &blk, int &max_items) {
   const int n = (int)counts.size();
@@ -48,127 +43,44 @@ void build_sched(const std::vector<int> &counts, std::vector<int> &off, std::vec
       throw std::runtime_error("schedule block exceeds the per-block cell capacity");
 }
 
-}  // namespace
+// host conversions between double and the tracer storage type
+void to_storage(Precision p, const double *src, void *dst, size_t n) {
+  switch (p) {
+    case Precision::FP64: std::memcpy(dst, src, n * sizeof(double)); break;
+    case Precision::FP32: for (size_t i = 0; i < n; i++) ((float *)dst)[i] = (float)src[i]; break;
+    case Precision::BF16: for (size_t i = 0; i < n; i++) ((__nv_bfloat16 *)dst)[i] = __float2bfloat16((float)src[i]); break;
+    case Precision::FP16: for (size_t i = 0; i < n; i++) ((__half *)dst)[i] = __float2half((float)src[i]); break;
+  }
+}
+void from_storage(Precision p, const void *src, double *dst, size_t n) {
+  switch (p) {
+    case Precision::FP64: std::memcpy(dst, src, n * sizeof(double)); break;
+    case Precision::FP32: for (size_t i = 0; i < n; i++) dst[i] = ((const float *)src)[i]; break;
+    case Precision::BF16: for (size_t i = 0; i < n; i++) dst[i] = __bfloat162float(((const __nv_bfloat16 *)src)[i]); break;
+    case Precision::FP16: for (size_t i = 0; i < n; i++) dst[i] = __half2float(((const __half *)src)[i]); break;
+  }
+}
 
-struct EngineImpl {
-  MeshHost mesh;
-  int S = 0;
-  cudaStream_t stream = nullptr;
-  std::vector<void *> allocs;
-  size_t bytes = 0;
-  DMeshT<double> dm{};
-  double *vel = nullptr, *W = nullptr;
-  struct Tracer {
-    double *T = nullptr, *Tout = nullptr, *TAB = nullptr;
-    TracerScheme sch;
-  };
-  std::vector<Tracer> tr;
-  // work arrays, one slot per tracer of a batch
-  int slots = 0;
-  double *vflux = nullptr;
-  double *adfh[NTMAX] = {}, *adfv[NTMAX] = {}, *lo[NTMAX] = {}, *rp[NTMAX] = {}, *rm[NTMAX] = {};
-  void ensure_slots(int n) {
-    if (n <= slots) return;
-    const size_t ns = (size_t)mesh.nod2D * S, es = (size_t)mesh.edge2D * S;
-    if (!vflux) vflux = dalloc<double>(es);
-    for (int t = slots; t < n; t++) {
-      adfh[t] = dalloc<double>(es);
-      adfv[t] = dalloc<double>(ns);
-      lo[t] = dalloc<double>(ns);
-      rp[t] = dalloc<double>(ns);
-      rm[t] = dalloc<double>(ns);
-    }
-    slots = n;
-  }
-  // launch profiling: when prof is set, every launch is bracketed by events
-  struct ProfRec { int kind; cudaEvent_t a, b; };
-  std::vector<ProfRec> *prof = nullptr;
-  void mark_begin(int kind) {
-    if (!prof) return;
-    ProfRec r{kind, nullptr, nullptr};
-    CK(cudaEventCreate(&r.a));
-    CK(cudaEventCreate(&r.b));
-    CK(cudaEventRecord(r.a, stream));
-    prof->push_back(r);
-  }
-  void mark_end() {
-    if (!prof) return;
-    CK(cudaEventRecord(prof->back().b, stream));
-  }
+// (ld, ncol) column-major host doubles -> device columns of stride S, type R
+template <typename R>
+R *upload_cols(EngineImpl &P, const double *h, int ld, int ncol, int nvalid) {
+  std::vector<R> st((size_t)ncol * P.S, R(0));
+  for (int c = 0; c < ncol; c++)
+    for (int k = 0; k < nvalid; k++) st[(size_t)c * P.S + k] = (R)h[(size_t)c * ld + k];
+  return P.upload(st);
+}
+template <typename R>
+R *upload_conv(EngineImpl &P, const std::vector<double> &h) {
+  std::vector<R> st(h.size());
+  for (size_t i = 0; i < h.size(); i++) st[i] = (R)h[i];
+  return P.upload(st);
+}
 
-  template <typename T>
-  T *dalloc(size_t n) {
-    void *p = nullptr;
-    if (n == 0) n = 1;
-    CK(cudaMalloc(&p, n * sizeof(T)));
-    CK(cudaMemsetAsync(p, 0, n * sizeof(T), stream));
-    allocs.push_back(p);
-    bytes += n * sizeof(T);
-    return (T *)p;
-  }
-  void dfree(void *p) {
-    if (!p) return;
-    auto it = std::find(allocs.begin(), allocs.end(), p);
-    if (it != allocs.end()) allocs.erase(it);
-    cudaFree(p);
-  }
-  // Every transfer is ordered on the engine's stream (which does not
-  // synchronise with the legacy default stream) and completes before the call
-  // returns, so host staging buffers may be released right after.
-  void h2d(void *d, const void *h, size_t bytes) {
-    if (!bytes) return;
-    CK(cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, stream));
-    CK(cudaStreamSynchronize(stream));
-  }
-  void d2h(void *h, const void *d, size_t bytes) {
-    if (!bytes) return;
-    CK(cudaMemcpyAsync(h, d, bytes, cudaMemcpyDeviceToHost, stream));
-    CK(cudaStreamSynchronize(stream));
-  }
-  void d2d(void *dst, const void *src, size_t bytes) {
-    if (!bytes) return;
-    CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, stream));
-    CK(cudaStreamSynchronize(stream));
-  }
-  template <typename T>
-  T *upload(const std::vector<T> &h) {
-    T *d = dalloc<T>(h.size());
-    h2d(d, h.data(), h.size() * sizeof(T));
-    return d;
-  }
-  // (ld, ncol) column-major host array -> device columns of stride S
-  double *upload_cols(const double *h, int ld, int ncol, int nvalid) {
-    std::vector<double> st((size_t)ncol * S, 0.0);
-    for (int c = 0; c < ncol; c++) std::memcpy(&st[(size_t)c * S], h + (size_t)c * ld, sizeof(double) * nvalid);
-    return upload(st);
-  }
-  void copy_cols_to(double *d, const double *h, int ld, int ncol) {
-    std::vector<double> st((size_t)ncol * S, 0.0);
-    for (int c = 0; c < ncol; c++) std::memcpy(&st[(size_t)c * S], h + (size_t)c * ld, sizeof(double) * ld);
-    h2d(d, st.data(), st.size() * sizeof(double));
-  }
-};
-
-Engine::Engine(const MeshHost &mesh) : p_(new EngineImpl) {
-  EngineImpl &P = *p_;
-  P.mesh = mesh;
-  const std::string bad = mesh.validate();
-  if (!bad.empty()) throw std::invalid_argument("mesh: " + bad);
+template <typename R>
+void build_dmesh(EngineImpl &P, DMeshT<R> &d, const std::vector<int> &slot_edge, const std::vector<int> &edge_slot) {
   const MeshHost &M = P.mesh;
   const int N = M.nod2D, T = M.elem2D, E = M.edge2D, nl = M.nl, L = nl - 1;
-  P.S = (nl + 3) / 4 * 4;
-  CK(cudaStreamCreateWithFlags(&P.stream, cudaStreamNonBlocking));
-  DMeshT<double> &d = P.dm;
   d.N = N; d.T = T; d.E = E; d.nl = nl; d.S = P.S;
-
-  // slot order: edges sorted by their smaller node id (stable in edge id)
-  std::vector<int> slot_edge(E), edge_slot(E);
-  for (int e = 0; e < E; e++) slot_edge[e] = e;
-  std::stable_sort(slot_edge.begin(), slot_edge.end(), [&](int a, int b) {
-    return std::min(M.edge_nodes[2 * a], M.edge_nodes[2 * a + 1]) <
-           std::min(M.edge_nodes[2 * b], M.edge_nodes[2 * b + 1]);
-  });
-  for (int s = 0; s < E; s++) edge_slot[slot_edge[s]] = s;
   std::vector<int2> en(E), et(E), el(E), ud(E);
   std::vector<double> ecross(4 * (size_t)E), edxdy(2 * (size_t)E), ea(E);
   for (int s = 0; s < E; s++) {
@@ -185,16 +97,16 @@ Engine::Engine(const MeshHost &mesh) : p_(new EngineImpl) {
   d.edge_tri = P.upload(et);
   d.edge_lev = P.upload(el);
   d.up_dn = P.upload(ud);
-  d.edge_cross = P.upload(ecross);
-  d.edge_dxdy = P.upload(edxdy);
-  d.edge_a = P.upload(ea);
+  d.edge_cross = upload_conv<R>(P, ecross);
+  d.edge_dxdy = upload_conv<R>(P, edxdy);
+  d.edge_a = upload_conv<R>(P, ea);
   d.nlev_elem = P.upload(M.nlev_elem);
   d.nlev_node = P.upload(M.nlev_node);
   d.nlev_node_min = P.upload(M.nlev_node_min);
   d.nbl = P.upload(M.nboundary_lay);
   d.elem_nodes = P.upload(M.elem_nodes);
-  d.grad_sca = P.upload(M.grad_sca);
-  d.elem_area = P.upload(M.elem_area);
+  d.grad_sca = upload_conv<R>(P, M.grad_sca);
+  d.elem_area = upload_conv<R>(P, M.elem_area);
   d.ring_ptr = P.upload(M.ring_ptr);
   d.ring_elem = P.upload(M.ring_elem);
   d.ne_ptr = P.upload(M.node_edge_ptr);
@@ -208,13 +120,13 @@ Engine::Engine(const MeshHost &mesh) : p_(new EngineImpl) {
       }
     d.ne4 = P.upload(ne4);
   }
-  d.zbar = P.upload(M.zbar);
-  d.Z = P.upload(M.Z);
-  d.area = P.upload_cols(M.area.data(), nl, N, nl);
-  d.areasvol = P.upload_cols(M.areasvol.data(), nl, N, nl);
-  d.hnode = P.upload_cols(M.hnode.data(), L, N, L);
-  d.hnode_new = P.upload_cols(M.hnode_new.data(), L, N, L);
-  d.helem = P.upload_cols(M.helem.data(), L, T, L);
+  d.zbar = upload_conv<R>(P, M.zbar);
+  d.Z = upload_conv<R>(P, M.Z);
+  d.area = upload_cols<R>(P, M.area.data(), nl, N, nl);
+  d.areasvol = upload_cols<R>(P, M.areasvol.data(), nl, N, nl);
+  d.hnode = upload_cols<R>(P, M.hnode.data(), L, N, L);
+  d.hnode_new = upload_cols<R>(P, M.hnode_new.data(), L, N, L);
+  d.helem = upload_cols<R>(P, M.helem.data(), L, T, L);
 
   std::vector<int> cnt(N), off, blk;
   for (int n = 0; n < N; n++) cnt[n] = M.nlev_node[n] - 1;
@@ -228,9 +140,35 @@ Engine::Engine(const MeshHost &mesh) : p_(new EngineImpl) {
   d.edge_sched.cell_off = P.upload(off);
   d.edge_sched.blk = P.upload(blk);
   d.edge_sched.nblk = (int)blk.size() - 1;
+}
 
-  P.vel = P.dalloc<double>((size_t)2 * T * P.S);
-  P.W = P.dalloc<double>((size_t)N * P.S);
+}  // namespace
+
+Engine::Engine(const MeshHost &mesh, Precision prec) : p_(new EngineImpl) {
+  EngineImpl &P = *p_;
+  P.mesh = mesh;
+  P.prec = prec;
+  P.r_bytes = prec == Precision::FP64 ? 8 : 4;
+  P.ts_bytes = prec == Precision::FP64 ? 8 : (prec == Precision::FP32 ? 4 : 2);
+  const std::string bad = mesh.validate();
+  if (!bad.empty()) throw std::invalid_argument("mesh: " + bad);
+  const MeshHost &M = P.mesh;
+  const int E = M.edge2D;
+  // level stride: 32-byte aligned columns for FP64, 16-byte aligned ones (or
+  // better) for the 4- and 2-byte types
+  P.S = prec == Precision::FP64 ? (M.nl + 3) / 4 * 4 : (M.nl + 7) / 8 * 8;
+  CK(cudaStreamCreateWithFlags(&P.stream, cudaStreamNonBlocking));
+  // slot order: edges sorted by their smaller node id (stable in edge id)
+  std::vector<int> slot_edge(E), edge_slot(E);
+  for (int e = 0; e < E; e++) slot_edge[e] = e;
+  std::stable_sort(slot_edge.begin(), slot_edge.end(), [&](int a, int b) {
+    return std::min(M.edge_nodes[2 * a], M.edge_nodes[2 * a + 1]) < std::min(M.edge_nodes[2 * b], M.edge_nodes[2 * b + 1]);
+  });
+  for (int s = 0; s < E; s++) edge_slot[slot_edge[s]] = s;
+  if (prec == Precision::FP64) build_dmesh<double>(P, P.dm64, slot_edge, edge_slot);
+  else build_dmesh<float>(P, P.dm32, slot_edge, edge_slot);
+  P.vel = P.dalloc_bytes((size_t)2 * M.elem2D * P.S * P.r_bytes);
+  P.W = P.dalloc_bytes((size_t)M.nod2D * P.S * P.r_bytes);
   CK(cudaStreamSynchronize(P.stream));
 }
 
@@ -244,6 +182,7 @@ Engine::~Engine() {
 
 const MeshHost &Engine::mesh() const { return p_->mesh; }
 int Engine::level_stride() const { return p_->S; }
+Precision Engine::precision() const { return p_->prec; }
 void *Engine::stream() const { return (void *)p_->stream; }
 void Engine::synchronize() const { CK(cudaStreamSynchronize(p_->stream)); }
 size_t Engine::device_bytes() const { return p_->bytes; }
@@ -253,20 +192,27 @@ void Engine::set_velocity(const double *uv, const double *w) {
   EngineImpl &P = *p_;
   const MeshHost &M = P.mesh;
   const int L = M.nl - 1, T = M.elem2D, N = M.nod2D;
-  std::vector<double> st((size_t)2 * T * P.S, 0.0);
+  std::vector<double> st((size_t)2 * T * P.S, 0.0), wst((size_t)N * P.S, 0.0);
   for (int e = 0; e < T; e++)
     for (int k = 0; k < L; k++) {
       st[2 * ((size_t)e * P.S + k)] = uv[2 * ((size_t)e * L + k)];
       st[2 * ((size_t)e * P.S + k) + 1] = uv[2 * ((size_t)e * L + k) + 1];
     }
-  P.h2d(P.vel, st.data(), st.size() * sizeof(double));
-  P.copy_cols_to(P.W, w, M.nl, N);
+  for (int n = 0; n < N; n++) std::memcpy(&wst[(size_t)n * P.S], w + (size_t)n * M.nl, sizeof(double) * M.nl);
+  if (P.prec == Precision::FP64) {
+    P.h2d(P.vel, st.data(), st.size() * sizeof(double));
+    P.h2d(P.W, wst.data(), wst.size() * sizeof(double));
+  } else {
+    std::vector<float> f(st.begin(), st.end()), fw(wst.begin(), wst.end());
+    P.h2d(P.vel, f.data(), f.size() * sizeof(float));
+    P.h2d(P.W, fw.data(), fw.size() * sizeof(float));
+  }
 }
 
 void Engine::set_velocity_zero() {
   EngineImpl &P = *p_;
-  CK(cudaMemsetAsync(P.vel, 0, sizeof(double) * 2 * P.mesh.elem2D * P.S, P.stream));
-  CK(cudaMemsetAsync(P.W, 0, sizeof(double) * P.mesh.nod2D * P.S, P.stream));
+  CK(cudaMemsetAsync(P.vel, 0, P.r_bytes * 2 * P.mesh.elem2D * P.S, P.stream));
+  CK(cudaMemsetAsync(P.W, 0, P.r_bytes * P.mesh.nod2D * P.S, P.stream));
   CK(cudaStreamSynchronize(P.stream));
 }
 
@@ -275,11 +221,11 @@ void Engine::allocate_tracers(int ntr) {
   CK(cudaStreamSynchronize(P.stream));
   for (auto &t : P.tr) { P.dfree(t.T); P.dfree(t.Tout); P.dfree(t.TAB); }
   P.tr.assign(ntr, EngineImpl::Tracer{});
-  const size_t n = (size_t)P.mesh.nod2D * P.S;
+  const size_t n = (size_t)P.mesh.nod2D * P.S * P.ts_bytes;
   for (auto &t : P.tr) {
-    t.T = P.dalloc<double>(n);
-    t.Tout = P.dalloc<double>(n);
-    t.TAB = P.dalloc<double>(n);
+    t.T = P.dalloc_bytes(n);
+    t.Tout = P.dalloc_bytes(n);
+    t.TAB = P.dalloc_bytes(n);
   }
   CK(cudaStreamSynchronize(P.stream));
 }
@@ -288,29 +234,41 @@ static void check_id(const EngineImpl &P, int id) {
   if (id < 0 || id >= (int)P.tr.size()) throw std::out_of_range("invalid tracer id " + std::to_string(id + 1));
 }
 
+// host (ld, N) doubles -> device storage columns
+static void put_tracer(EngineImpl &P, void *d, const double *v) {
+  const int L = P.mesh.nl - 1, N = P.mesh.nod2D;
+  std::vector<double> st((size_t)N * P.S, 0.0);
+  for (int n = 0; n < N; n++) std::memcpy(&st[(size_t)n * P.S], v + (size_t)n * L, sizeof(double) * L);
+  std::vector<unsigned char> buf(st.size() * P.ts_bytes);
+  to_storage(P.prec, st.data(), buf.data(), st.size());
+  P.h2d(d, buf.data(), buf.size());
+}
+
 void Engine::set_values(int id, const double *v, bool also_ab) {
   EngineImpl &P = *p_;
   check_id(P, id);
-  const int L = P.mesh.nl - 1;
   CK(cudaStreamSynchronize(P.stream));
-  P.copy_cols_to(P.tr[id].T, v, L, P.mesh.nod2D);
-  P.d2d(P.tr[id].Tout, P.tr[id].T, sizeof(double) * P.mesh.nod2D * P.S);
-  if (also_ab) P.d2d(P.tr[id].TAB, P.tr[id].T, sizeof(double) * P.mesh.nod2D * P.S);
+  put_tracer(P, P.tr[id].T, v);
+  const size_t n = (size_t)P.mesh.nod2D * P.S * P.ts_bytes;
+  P.d2d(P.tr[id].Tout, P.tr[id].T, n);
+  if (also_ab) P.d2d(P.tr[id].TAB, P.tr[id].T, n);
 }
 
 void Engine::set_values_ab(int id, const double *v) {
   EngineImpl &P = *p_;
   check_id(P, id);
   CK(cudaStreamSynchronize(P.stream));
-  P.copy_cols_to(P.tr[id].TAB, v, P.mesh.nl - 1, P.mesh.nod2D);
+  put_tracer(P, P.tr[id].TAB, v);
 }
 
 void Engine::get_values(int id, double *out) const {
   EngineImpl &P = *p_;
   check_id(P, id);
   const int L = P.mesh.nl - 1, N = P.mesh.nod2D;
+  std::vector<unsigned char> buf((size_t)N * P.S * P.ts_bytes);
+  P.d2h(buf.data(), P.tr[id].T, buf.size());
   std::vector<double> st((size_t)N * P.S);
-  P.d2h(st.data(), P.tr[id].T, st.size() * sizeof(double));
+  from_storage(P.prec, buf.data(), st.data(), st.size());
   for (int n = 0; n < N; n++) std::memcpy(out + (size_t)n * L, &st[(size_t)n * P.S], sizeof(double) * L);
 }
 
@@ -325,109 +283,46 @@ TracerScheme Engine::scheme(int id) const {
   return p_->tr[id].sch;
 }
 
-namespace {
-
-enum { KK_EDGE = 0, KK_COL1, KK_COL2, KK_COL3, KK_COUNT };
-const char *const kKindNames[KK_COUNT] = {"k_edge", "k_col1", "k_col2", "k_col3"};
-
-// Raise the dynamic shared-memory limit of a kernel once (per kernel
-// function; all kernels share one C++ function-pointer type).
-template <typename K>
-void set_smem(K kernel, size_t bytes) {
-  static std::mutex mu;
-  static std::unordered_map<const void *, size_t> done;
-  std::lock_guard<std::mutex> lock(mu);
-  auto it = done.find((const void *)kernel);
-  if (it != done.end() && it->second >= bytes) return;
-  CK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
-  done[(const void *)kernel] = bytes;
-}
-
-template <int NT, int HOR, int LIM>
-void launch_edge(EngineImpl &P, const FusedArgs<double> &a) {
-  const DSched &s = P.dm.edge_sched;
-  if (s.nblk <= 0) return;
-  const size_t sm = smem_edge<double>();
-  P.mark_begin(KK_EDGE);
-  k_edge<double, NT, HOR, LIM><<<s.nblk, kThreads, sm, P.stream>>>(P.dm, a);
-  P.mark_end();
-}
-
-template <int NT, int VER, int LIM>
-void launch_col1(EngineImpl &P, const FusedArgs<double> &a) {
-  const DSched &s = P.dm.node_sched;
-  const size_t sm = smem_col<double>(NT, 4);
-  set_smem(k_col1<double, NT, VER, LIM>, sm);
-  P.mark_begin(KK_COL1);
-  k_col1<double, NT, VER, LIM><<<s.nblk, kThreads, sm, P.stream>>>(P.dm, a);
-  P.mark_end();
-}
-
-template <int NT, int LIM>
-void run_group(EngineImpl &P, const TracerScheme &sc, const FusedArgs<double> &a) {
-  switch (sc.hor) {
-    case 1: launch_edge<NT, HOR_MUSCL, LIM>(P, a); break;
-    case 2: launch_edge<NT, HOR_MFCT, LIM>(P, a); break;
-    default: launch_edge<NT, HOR_UPW1, LIM>(P, a); break;
+static void ensure_slots(EngineImpl &P, int n) {
+  if (n <= P.slots) return;
+  const size_t ns = (size_t)P.mesh.nod2D * P.S * P.r_bytes, es = (size_t)P.mesh.edge2D * P.S * P.r_bytes;
+  if (!P.vflux) P.vflux = P.dalloc_bytes(es);
+  for (int t = P.slots; t < n; t++) {
+    P.adfh[t] = P.dalloc_bytes(es);
+    P.adfv[t] = P.dalloc_bytes(ns);
+    P.lo[t] = P.dalloc_bytes(ns);
+    P.rp[t] = P.dalloc_bytes(ns);
+    P.rm[t] = P.dalloc_bytes(ns);
   }
-  switch (sc.ver) {
-    case 1: launch_col1<NT, VER_PPM, LIM>(P, a); break;
-    case 2: launch_col1<NT, VER_QR4C, LIM>(P, a); break;
-    case 3: launch_col1<NT, VER_CDIFF, LIM>(P, a); break;
-    default: launch_col1<NT, VER_UPW1, LIM>(P, a); break;
-  }
-  const DSched &s = P.dm.node_sched;
-  if (LIM == LIM_FCT) {
-    const size_t sm2 = smem_col<double>(NT, 2);
-    set_smem(k_col2<double, NT>, sm2);
-    P.mark_begin(KK_COL2);
-    k_col2<double, NT><<<s.nblk, kThreads, sm2, P.stream>>>(P.dm, a);
-    P.mark_end();
-  }
-  const size_t sm3 = smem_col<double>(NT, 0);
-  P.mark_begin(KK_COL3);
-  k_col3<double, NT, LIM><<<s.nblk, kThreads, sm3, P.stream>>>(P.dm, a);
-  P.mark_end();
+  P.slots = n;
 }
 
-template <int NT>
-void run_group_nt(EngineImpl &P, const TracerScheme &sc, const FusedArgs<double> &a) {
-  if (sc.lim == 1) run_group<NT, LIM_FCT>(P, sc, a);
-  else run_group<NT, LIM_NONE>(P, sc, a);
+static void dispatch(EngineImpl &P, const TracerScheme &sc, int nt, const BatchPtrs &b, double dt) {
+  if (P.mesh.nod2D <= 0) return;
+  if (P.prec == Precision::FP64) launch_batch_f64(P, sc, nt, b, dt);
+  else launch_batch_f32(P, sc, nt, b, dt);
+  CK(cudaGetLastError());
 }
 
-}  // namespace
-
-// Tracers are advanced in batches of up to NTMAX consecutive tracers with
+// Tracers are advanced in batches of up to kBatchMax consecutive tracers with
 // the same scheme; a batch shares the edge volume fluxes, the geometry loads
 // and every geometry-only division.
 static void run_batch(EngineImpl &P, int first, int nt, double dt, bool refresh_ab) {
-  P.ensure_slots(nt);
-  FusedArgs<double> a{};
-  const TracerScheme &sc = P.tr[first].sch;
+  ensure_slots(P, nt);
+  BatchPtrs b;
   for (int t = 0; t < nt; t++) {
     auto &tr = P.tr[first + t];
-    a.T[t] = tr.T;
-    a.TAB[t] = refresh_ab ? tr.T : tr.TAB;
-    a.T_out[t] = tr.Tout;
-    a.adf_h[t] = P.adfh[t];
-    a.adf_v[t] = P.adfv[t];
-    a.lo[t] = P.lo[t];
-    a.rp[t] = P.rp[t];
-    a.rm[t] = P.rm[t];
+    b.T[t] = tr.T;
+    b.TAB[t] = refresh_ab ? tr.T : tr.TAB;
+    b.T_out[t] = tr.Tout;
+    b.adf_h[t] = P.adfh[t];
+    b.adf_v[t] = P.adfv[t];
+    b.lo[t] = P.lo[t];
+    b.rp[t] = P.rp[t];
+    b.rm[t] = P.rm[t];
   }
-  a.vflux = P.vflux;
-  a.vel = P.vel;
-  a.W = P.W;
-  a.dt = dt;
-  a.ph = sc.ph;
-  a.pv = sc.pv;
-  if (P.mesh.nod2D > 0) {
-    if (nt == 4) run_group_nt<4>(P, sc, a);
-    else if (nt == 2) run_group_nt<2>(P, sc, a);
-    else run_group_nt<1>(P, sc, a);
-    CK(cudaGetLastError());
-  }
+  b.vflux = P.vflux;
+  dispatch(P, P.tr[first].sch, nt, b, dt);
   for (int t = 0; t < nt; t++) std::swap(P.tr[first + t].T, P.tr[first + t].Tout);
 }
 
@@ -438,7 +333,7 @@ static bool same_scheme(const TracerScheme &a, const TracerScheme &b) {
 // batch sizes the engine launches: 4, 2 or 1 tracers
 static int batch_size(const EngineImpl &P, int first) {
   int run = 1;
-  while (first + run < (int)P.tr.size() && run < NTMAX && same_scheme(P.tr[first].sch, P.tr[first + run].sch)) run++;
+  while (first + run < (int)P.tr.size() && run < kBatchMax && same_scheme(P.tr[first].sch, P.tr[first + run].sch)) run++;
   return run >= 4 ? 4 : (run >= 2 ? 2 : 1);
 }
 
@@ -458,43 +353,6 @@ void Engine::step_tracer(int id, double dt, bool refresh_ab) {
   run_batch(*p_, id, 1, dt, refresh_ab);
 }
 
-size_t Engine::step_scratch_doubles() const {
-  const EngineImpl &P = *p_;
-  auto up = [](size_t n) { return (n + 31) / 32 * 32; };  // 256-byte pieces
-  const size_t es = up((size_t)P.mesh.edge2D * P.S), ns = up((size_t)P.mesh.nod2D * P.S);
-  return 2 * es + 4 * ns;
-}
-
-void Engine::step_with_scratch(int id, const double *T, const double *TAB, double *T_out, double dt,
-                               double *scratch, size_t scratch_doubles) {
-  EngineImpl &P = *p_;
-  check_id(P, id);
-  if (scratch_doubles < step_scratch_doubles()) throw std::length_error("scratch too small for this mesh");
-  auto up = [](size_t n) { return (n + 31) / 32 * 32; };
-  const size_t es = up((size_t)P.mesh.edge2D * P.S), ns = up((size_t)P.mesh.nod2D * P.S);
-  const TracerScheme &sc = P.tr[id].sch;
-  FusedArgs<double> a{};
-  a.T[0] = T;
-  a.TAB[0] = TAB;
-  a.T_out[0] = T_out;
-  a.vflux = scratch;
-  a.adf_h[0] = scratch + es;
-  a.adf_v[0] = scratch + 2 * es;
-  a.lo[0] = scratch + 2 * es + ns;
-  a.rp[0] = scratch + 2 * es + 2 * ns;
-  a.rm[0] = scratch + 2 * es + 3 * ns;
-  a.vel = P.vel;
-  a.W = P.W;
-  a.dt = dt;
-  a.ph = sc.ph;
-  a.pv = sc.pv;
-  if (P.mesh.nod2D > 0) {
-    run_group_nt<1>(P, sc, a);
-    CK(cudaGetLastError());
-  }
-  CK(cudaStreamSynchronize(P.stream));
-}
-
 void Engine::step(double dt, bool refresh_ab) {
   for (int i = 0; i < (int)p_->tr.size();) {
     const int nt = batch_size(*p_, i);
@@ -503,9 +361,39 @@ void Engine::step(double dt, bool refresh_ab) {
   }
 }
 
+size_t Engine::step_scratch_doubles() const {
+  const EngineImpl &P = *p_;
+  auto up = [](size_t n) { return (n + 31) / 32 * 32; };  // 256-byte pieces
+  const size_t es = up((size_t)P.mesh.edge2D * P.S), ns = up((size_t)P.mesh.nod2D * P.S);
+  return 2 * es + 4 * ns;
+}
+
+void Engine::step_with_scratch(int id, const double *T, const double *TAB, double *T_out, double dt, double *scratch,
+                               size_t scratch_doubles) {
+  EngineImpl &P = *p_;
+  check_id(P, id);
+  if (P.prec != Precision::FP64) throw std::invalid_argument("the allocation-free step runs the FP64 engine only");
+  if (scratch_doubles < step_scratch_doubles()) throw std::length_error("scratch too small for this mesh");
+  auto up = [](size_t n) { return (n + 31) / 32 * 32; };
+  const size_t es = up((size_t)P.mesh.edge2D * P.S), ns = up((size_t)P.mesh.nod2D * P.S);
+  BatchPtrs b;
+  b.T[0] = T;
+  b.TAB[0] = TAB;
+  b.T_out[0] = T_out;
+  b.vflux = scratch;
+  b.adf_h[0] = scratch + es;
+  b.adf_v[0] = scratch + 2 * es;
+  b.lo[0] = scratch + 2 * es + ns;
+  b.rp[0] = scratch + 2 * es + 2 * ns;
+  b.rm[0] = scratch + 2 * es + 3 * ns;
+  dispatch(P, P.tr[id].sch, 1, b, dt);
+  CK(cudaStreamSynchronize(P.stream));
+}
+
 const char *const *Engine::kernel_kind_names(int *n) {
+  static const char *const names[KK_COUNT] = {"k_edge", "k_col1", "k_col2", "k_col3"};
   *n = KK_COUNT;
-  return kKindNames;
+  return names;
 }
 
 int Engine::profile_steps(int nsteps, double dt, bool refresh_ab, double *ms, int nkinds) {
@@ -529,6 +417,14 @@ int Engine::profile_steps(int nsteps, double dt, bool refresh_ab, double *ms, in
     cudaEventDestroy(r.b);
   }
   return (int)recs.size();
+}
+
+void Engine::volume_sum(int id, double out[2]) const {
+  EngineImpl &P = *p_;
+  check_id(P, id);
+  CK(cudaStreamSynchronize(P.stream));
+  if (P.prec == Precision::FP64) volume_sum_f64(P, P.tr[id].T, out);
+  else volume_sum_f32(P, P.tr[id].T, out);
 }
 
 void Engine::stats(int id, double out[4]) const {

@@ -21,11 +21,21 @@ struct TracerScheme {
   double pv = 1.0;  // tra_adv_pv
 };
 
+// Arithmetic / storage modes.  FP64: the bit-exact drop-in.  FP32: FP32
+// tracers, geometry and arithmetic.  BF16 / FP16: 16-bit tracer storage with
+// FP32 arithmetic and accumulation.  In the FP32-based modes the FCT ratio
+// denominators are formed in FP64.
+enum class Precision { FP64 = 0, FP32 = 1, BF16 = 2, FP16 = 3 };
+
 struct EngineImpl;
 
 class Engine {
  public:
-  explicit Engine(const MeshHost &mesh);
+  explicit Engine(const MeshHost &mesh, Precision prec = Precision::FP64);
+  Precision precision() const;
+  // Compensated FP64 sums over the wet cells of tracer id: out[0] = Sum T,
+  // out[1] = Sum T * areasvol * hnode_new (the conserved tracer content).
+  void volume_sum(int id, double out[2]) const;
   ~Engine();
   Engine(const Engine &) = delete;
   Engine &operator=(const Engine &) = delete;

@@ -1,0 +1,134 @@
+// Engine internals shared by the host engine (engine.cu) and the
+// per-precision kernel translation units (step_f64.cu, step_f32.cu).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "dmesh.hpp"
+#include "engine.hpp"
+
+namespace fesom {
+
+#define CK(x)                                                                                          \
+  do {                                                                                                 \
+    cudaError_t e_ = (x);                                                                              \
+    if (e_ != cudaSuccess) throw std::runtime_error(std::string(#x) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+constexpr int kBatchMax = 4;  // tracers per batch (NTMAX of the kernels)
+
+// Device pointers of one batch of tracers, untyped (the element types follow
+// the engine's precision mode).
+struct BatchPtrs {
+  const void *T[kBatchMax] = {};
+  const void *TAB[kBatchMax] = {};
+  void *T_out[kBatchMax] = {};
+  void *adf_h[kBatchMax] = {};
+  void *adf_v[kBatchMax] = {};
+  void *lo[kBatchMax] = {};
+  void *rp[kBatchMax] = {};
+  void *rm[kBatchMax] = {};
+  void *vflux = nullptr;
+};
+
+struct EngineImpl {
+  MeshHost mesh;
+  int S = 0;
+  Precision prec = Precision::FP64;
+  size_t ts_bytes = 8;  // tracer storage element
+  size_t r_bytes = 8;   // compute / geometry / work element
+  cudaStream_t stream = nullptr;
+  std::vector<void *> allocs;
+  size_t bytes = 0;
+  DMeshT<double> dm64{};
+  DMeshT<float> dm32{};
+  void *vel = nullptr, *W = nullptr;
+  struct Tracer {
+    void *T = nullptr, *Tout = nullptr, *TAB = nullptr;
+    TracerScheme sch;
+  };
+  std::vector<Tracer> tr;
+  int slots = 0;
+  void *vflux = nullptr;
+  void *adfh[kBatchMax] = {}, *adfv[kBatchMax] = {}, *lo[kBatchMax] = {}, *rp[kBatchMax] = {}, *rm[kBatchMax] = {};
+
+  // launch profiling: when prof is set, every launch is bracketed by events
+  struct ProfRec {
+    int kind;
+    cudaEvent_t a, b;
+  };
+  std::vector<ProfRec> *prof = nullptr;
+  void mark_begin(int kind) {
+    if (!prof) return;
+    ProfRec r{kind, nullptr, nullptr};
+    CK(cudaEventCreate(&r.a));
+    CK(cudaEventCreate(&r.b));
+    CK(cudaEventRecord(r.a, stream));
+    prof->push_back(r);
+  }
+  void mark_end() {
+    if (!prof) return;
+    CK(cudaEventRecord(prof->back().b, stream));
+  }
+
+  void *dalloc_bytes(size_t n) {
+    void *p = nullptr;
+    if (n == 0) n = 8;
+    CK(cudaMalloc(&p, n));
+    CK(cudaMemsetAsync(p, 0, n, stream));
+    allocs.push_back(p);
+    bytes += n;
+    return p;
+  }
+  template <typename T>
+  T *dalloc(size_t n) {
+    return (T *)dalloc_bytes(n * sizeof(T));
+  }
+  void dfree(void *p) {
+    if (!p) return;
+    auto it = std::find(allocs.begin(), allocs.end(), p);
+    if (it != allocs.end()) allocs.erase(it);
+    cudaFree(p);
+  }
+  // Every transfer is ordered on the engine's stream (which does not
+  // synchronise with the legacy default stream) and completes before the call
+  // returns, so host staging buffers may be released right after.
+  void h2d(void *d, const void *h, size_t n) {
+    if (!n) return;
+    CK(cudaMemcpyAsync(d, h, n, cudaMemcpyHostToDevice, stream));
+    CK(cudaStreamSynchronize(stream));
+  }
+  void d2h(void *h, const void *d, size_t n) {
+    if (!n) return;
+    CK(cudaMemcpyAsync(h, d, n, cudaMemcpyDeviceToHost, stream));
+    CK(cudaStreamSynchronize(stream));
+  }
+  void d2d(void *dst, const void *src, size_t n) {
+    if (!n) return;
+    CK(cudaMemcpyAsync(dst, src, n, cudaMemcpyDeviceToDevice, stream));
+    CK(cudaStreamSynchronize(stream));
+  }
+  template <typename T>
+  T *upload(const std::vector<T> &h) {
+    T *d = dalloc<T>(h.size());
+    h2d(d, h.data(), h.size() * sizeof(T));
+    return d;
+  }
+};
+
+// Kernel kinds reported by profile_steps.
+enum { KK_EDGE = 0, KK_COL1, KK_COL2, KK_COL3, KK_COUNT };
+
+// Launch one batch of nt tracers (kernels in step_f64.cu / step_f32.cu).
+void launch_batch_f64(EngineImpl &P, const TracerScheme &sc, int nt, const BatchPtrs &b, double dt);
+void launch_batch_f32(EngineImpl &P, const TracerScheme &sc, int nt, const BatchPtrs &b, double dt);
+// Compensated FP64 sums of T and of T * areasvol * hnode_new over the wet
+// cells of one tracer.
+void volume_sum_f64(EngineImpl &P, const void *T, double out[2]);
+void volume_sum_f32(EngineImpl &P, const void *T, double out[2]);
+
+}  // namespace fesom

@@ -1,0 +1,174 @@
+// Templated dispatch of the step kernels for one (compute, storage) type
+// pair; included by exactly one translation unit per pair.
+#pragma once
+#include <mutex>
+#include <unordered_map>
+
+#include "advect_fused.cuh"
+#include "engine_impl.hpp"
+
+namespace fesom {
+
+template <typename R>
+const DMeshT<R> &dmesh(const EngineImpl &P);
+template <>
+inline const DMeshT<double> &dmesh<double>(const EngineImpl &P) { return P.dm64; }
+template <>
+inline const DMeshT<float> &dmesh<float>(const EngineImpl &P) { return P.dm32; }
+
+// Raise the dynamic shared-memory limit of a kernel once (per kernel
+// function; all kernels share one C++ function-pointer type).
+template <typename K>
+void set_smem(K kernel, size_t bytes) {
+  static std::mutex mu;
+  static std::unordered_map<const void *, size_t> done;
+  std::lock_guard<std::mutex> lock(mu);
+  auto it = done.find((const void *)kernel);
+  if (it != done.end() && it->second >= bytes) return;
+  CK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+  done[(const void *)kernel] = bytes;
+}
+
+template <typename R, typename TS, int NT, int HOR, int LIM>
+void launch_edge(EngineImpl &P, const FusedArgs<R, TS> &a) {
+  const DMeshT<R> &m = dmesh<R>(P);
+  if (m.edge_sched.nblk <= 0) return;
+  P.mark_begin(KK_EDGE);
+  k_edge<R, TS, NT, HOR, LIM><<<m.edge_sched.nblk, kThreads, smem_edge(), P.stream>>>(m, a);
+  P.mark_end();
+}
+
+template <typename R, typename TS, int NT, int VER, int LIM>
+void launch_col1(EngineImpl &P, const FusedArgs<R, TS> &a) {
+  const DMeshT<R> &m = dmesh<R>(P);
+  const size_t sm = smem_col<R>(NT, 4);
+  set_smem(k_col1<R, TS, NT, VER, LIM>, sm);
+  P.mark_begin(KK_COL1);
+  k_col1<R, TS, NT, VER, LIM><<<m.node_sched.nblk, kThreads, sm, P.stream>>>(m, a);
+  P.mark_end();
+}
+
+template <typename R, typename TS, int NT, int LIM>
+void run_group(EngineImpl &P, const TracerScheme &sc, const FusedArgs<R, TS> &a) {
+  switch (sc.hor) {
+    case 1: launch_edge<R, TS, NT, HOR_MUSCL, LIM>(P, a); break;
+    case 2: launch_edge<R, TS, NT, HOR_MFCT, LIM>(P, a); break;
+    default: launch_edge<R, TS, NT, HOR_UPW1, LIM>(P, a); break;
+  }
+  switch (sc.ver) {
+    case 1: launch_col1<R, TS, NT, VER_PPM, LIM>(P, a); break;
+    case 2: launch_col1<R, TS, NT, VER_QR4C, LIM>(P, a); break;
+    case 3: launch_col1<R, TS, NT, VER_CDIFF, LIM>(P, a); break;
+    default: launch_col1<R, TS, NT, VER_UPW1, LIM>(P, a); break;
+  }
+  const DMeshT<R> &m = dmesh<R>(P);
+  if (LIM == LIM_FCT) {
+    const size_t sm2 = smem_col<R>(NT, 2);
+    set_smem(k_col2<R, TS, NT>, sm2);
+    P.mark_begin(KK_COL2);
+    k_col2<R, TS, NT><<<m.node_sched.nblk, kThreads, sm2, P.stream>>>(m, a);
+    P.mark_end();
+  }
+  const size_t sm3 = smem_col<R>(NT, 0);
+  P.mark_begin(KK_COL3);
+  k_col3<R, TS, NT, LIM><<<m.node_sched.nblk, kThreads, sm3, P.stream>>>(m, a);
+  P.mark_end();
+}
+
+template <typename R, typename TS>
+void launch_batch_t(EngineImpl &P, const TracerScheme &sc, int nt, const BatchPtrs &b, double dt) {
+  FusedArgs<R, TS> a{};
+  for (int t = 0; t < nt; t++) {
+    a.T[t] = (const TS *)b.T[t];
+    a.TAB[t] = (const TS *)b.TAB[t];
+    a.T_out[t] = (TS *)b.T_out[t];
+    a.adf_h[t] = (R *)b.adf_h[t];
+    a.adf_v[t] = (R *)b.adf_v[t];
+    a.lo[t] = (R *)b.lo[t];
+    a.rp[t] = (R *)b.rp[t];
+    a.rm[t] = (R *)b.rm[t];
+  }
+  a.vflux = (R *)b.vflux;
+  a.vel = (const R *)P.vel;
+  a.W = (const R *)P.W;
+  a.dt = (R)dt;
+  a.ph = (R)sc.ph;
+  a.pv = (R)sc.pv;
+  const bool fct = sc.lim == 1;
+  if (nt == 4) fct ? run_group<R, TS, 4, LIM_FCT>(P, sc, a) : run_group<R, TS, 4, LIM_NONE>(P, sc, a);
+  else if (nt == 2) fct ? run_group<R, TS, 2, LIM_FCT>(P, sc, a) : run_group<R, TS, 2, LIM_NONE>(P, sc, a);
+  else fct ? run_group<R, TS, 1, LIM_FCT>(P, sc, a) : run_group<R, TS, 1, LIM_NONE>(P, sc, a);
+}
+
+// ---------------------------------------------------------------------------
+// compensated FP64 sums over the wet cells of one tracer
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void two_sum(double a, double b, double &s, double &e) {
+  s = a + b;
+  const double bb = s - a;
+  e = (a - (s - bb)) + (b - bb);
+}
+
+template <typename R, typename TS>
+__global__ void __launch_bounds__(256) k_volume_sum(DMeshT<R> m, const TS *T, double *out) {
+  // per thread: Neumaier-compensated partial sums of T and T*areasvol*hnode_new
+  double s0 = 0, c0 = 0, s1 = 0, c1 = 0;
+  for (int n = blockIdx.x * blockDim.y + threadIdx.y; n < m.N; n += gridDim.x * blockDim.y) {
+    const int L = m.nlev_node[n] - 1;
+    for (int k = threadIdx.x; k < L; k += blockDim.x) {
+      const size_t o = (size_t)n * m.S + k;
+      const double t = (double)R(T[o]);
+      const double v = t * (double)m.areasvol[o] * (double)m.hnode_new[o];
+      double s, e;
+      two_sum(s0, t, s, e); s0 = s; c0 += e;
+      two_sum(s1, v, s, e); s1 = s; c1 += e;
+    }
+  }
+  __shared__ double sh[4][256];
+  const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+  sh[0][tid] = s0; sh[1][tid] = c0; sh[2][tid] = s1; sh[3][tid] = c1;
+  __syncthreads();
+  for (int w = 128; w > 0; w >>= 1) {
+    if (tid < w) {
+      double s, e;
+      two_sum(sh[0][tid], sh[0][tid + w], s, e);
+      sh[0][tid] = s; sh[1][tid] += sh[1][tid + w] + e;
+      two_sum(sh[2][tid], sh[2][tid + w], s, e);
+      sh[2][tid] = s; sh[3][tid] += sh[3][tid + w] + e;
+    }
+    __syncthreads();
+  }
+  if (tid == 0) {
+    out[4 * blockIdx.x + 0] = sh[0][0];
+    out[4 * blockIdx.x + 1] = sh[1][0];
+    out[4 * blockIdx.x + 2] = sh[2][0];
+    out[4 * blockIdx.x + 3] = sh[3][0];
+  }
+}
+
+template <typename R, typename TS>
+void volume_sum_t(EngineImpl &P, const void *T, double res[2]) {
+  const int blocks = 296;
+  double *d = P.dalloc<double>(4 * blocks);
+  k_volume_sum<R, TS><<<blocks, dim3(32, 8), 0, P.stream>>>(dmesh<R>(P), (const TS *)T, d);
+  CK(cudaGetLastError());
+  std::vector<double> h(4 * blocks);
+  P.d2h(h.data(), d, h.size() * sizeof(double));
+  P.dfree(d);
+  // final compensated combination on the host, in block order
+  double s0 = 0, c0 = 0, s1 = 0, c1 = 0;
+  for (int b = 0; b < blocks; b++) {
+    for (int q = 0; q < 2; q++) {
+      double &s = q ? s1 : s0, &c = q ? c1 : c0;
+      const double x = h[4 * b + 2 * q], xc = h[4 * b + 2 * q + 1];
+      const double t = s + x;
+      c += (std::fabs(s) >= std::fabs(x)) ? (s - t) + x : (x - t) + s;
+      s = t;
+      c += xc;
+    }
+  }
+  res[0] = s0 + c0;
+  res[1] = s1 + c1;
+}
+
+}  // namespace fesom

@@ -76,7 +76,7 @@ long long MeshHost::wet_cells() const {
 }
 
 MeshHost build_analytic_mesh(int nx, int ny, int nl, double Lx, double Ly, double max_depth,
-                             bool periodic, bool full_rings, const int *node_K) {
+                             bool periodic, bool full_rings, const int *node_K, bool left_oriented) {
   if (nx < 2 || ny < 2 || nl < 3) throw std::invalid_argument("analytic mesh needs nx, ny >= 2 and nl >= 3");
   if (periodic && (nx < 4 || ny < 4)) throw std::invalid_argument("periodic analytic mesh needs nx, ny >= 4");
   MeshHost m;
@@ -137,11 +137,23 @@ MeshHost build_analytic_mesh(int nx, int ny, int nl, double Lx, double Ly, doubl
   auto push = [&](int a, int b, int t1, int t2) {
     ednx.push_back(a); ednx.push_back(b); etri.push_back(t1); etri.push_back(t2);
   };
+  // horizontal and vertical edges, optionally reversed (see left_oriented)
+  auto ab = [&](int a, int b, int &x, int &y) {
+    x = left_oriented ? b : a;
+    y = left_oriented ? a : b;
+  };
   if (periodic) {
+    int x, y;
     for (int j = 1; j <= ny - 1; j++)
-      for (int i = 1; i <= nx - 1; i++) push(g.ext(i, j), g.ext(i + 1, j), j >= 2 ? upper(i, j - 1) : upper(i, ny - 1), lower(i, j));
+      for (int i = 1; i <= nx - 1; i++) {
+        ab(g.ext(i, j), g.ext(i + 1, j), x, y);
+        push(x, y, j >= 2 ? upper(i, j - 1) : upper(i, ny - 1), lower(i, j));
+      }
     for (int j = 1; j <= ny - 1; j++)
-      for (int i = 1; i <= nx - 1; i++) push(g.ext(i, j), g.ext(i, j + 1), upper(i, j), i >= 2 ? lower(i - 1, j) : lower(nx - 1, j));
+      for (int i = 1; i <= nx - 1; i++) {
+        ab(g.ext(i, j), g.ext(i, j + 1), x, y);
+        push(x, y, upper(i, j), i >= 2 ? lower(i - 1, j) : lower(nx - 1, j));
+      }
     for (int j = 1; j <= ny - 1; j++)
       for (int i = 1; i <= nx - 1; i++) push(g.ext(i, j), g.ext(i + 1, j + 1), upper(i, j), lower(i, j));
   } else {
@@ -150,12 +162,17 @@ MeshHost build_analytic_mesh(int nx, int ny, int nl, double Lx, double Ly, doubl
       if (t1 < 0 && t2 >= 0) { t1 = t2; t2 = -1; }  // valid element first
       rn.push_back(a); rn.push_back(b); rt.push_back(t1); rt.push_back(t2);
     };
+    int x, y;
     for (int j = 1; j <= ny; j++)
-      for (int i = 1; i <= nx - 1; i++)
-        rpush(g.ext(i, j), g.ext(i + 1, j), j >= 2 ? upper(i, j - 1) : -1, j <= ny - 1 ? lower(i, j) : -1);
+      for (int i = 1; i <= nx - 1; i++) {
+        ab(g.ext(i, j), g.ext(i + 1, j), x, y);
+        rpush(x, y, j >= 2 ? upper(i, j - 1) : -1, j <= ny - 1 ? lower(i, j) : -1);
+      }
     for (int j = 1; j <= ny - 1; j++)
-      for (int i = 1; i <= nx; i++)
-        rpush(g.ext(i, j), g.ext(i, j + 1), i <= nx - 1 ? upper(i, j) : -1, i >= 2 ? lower(i - 1, j) : -1);
+      for (int i = 1; i <= nx; i++) {
+        ab(g.ext(i, j), g.ext(i, j + 1), x, y);
+        rpush(x, y, i <= nx - 1 ? upper(i, j) : -1, i >= 2 ? lower(i - 1, j) : -1);
+      }
     for (int j = 1; j <= ny - 1; j++)
       for (int i = 1; i <= nx - 1; i++) rpush(g.ext(i, j), g.ext(i + 1, j + 1), upper(i, j), lower(i, j));
     // internal edges first, boundary edges after, each in generation order

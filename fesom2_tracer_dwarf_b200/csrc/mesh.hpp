@@ -12,11 +12,34 @@
 //   * up/down-wind triangles and nboundary_lay for MUSCL
 //     (lib/oce_muscl_adv.F90:96-357).
 #pragma once
+#include <cstddef>
 #include <cstdint>
 #include <string>
 #include <vector>
 
 namespace fesom {
+
+// Zero-filled host array backed by an anonymous mapping advised as
+// transparent huge pages: first-touch faults of multi-GB inputs cost 512x
+// fewer page faults than with 4 KB pages (glibc's malloc does not advise).
+template <typename T>
+class HugeArray {
+ public:
+  HugeArray() = default;
+  explicit HugeArray(size_t n);
+  ~HugeArray();
+  HugeArray(const HugeArray &) = delete;
+  HugeArray &operator=(const HugeArray &) = delete;
+  T *data() { return p_; }
+  const T *data() const { return p_; }
+  T &operator[](size_t i) { return p_[i]; }
+  const T &operator[](size_t i) const { return p_[i]; }
+  size_t size() const { return n_; }
+
+ private:
+  T *p_ = nullptr;
+  size_t n_ = 0, bytes_ = 0;
+};
 
 constexpr double kREarth = 6367500.0;          // lib/oce_modules.F90:24
 constexpr double kPiRef = 3.14159265358979;     // lib/oce_modules.F90:19
@@ -69,15 +92,22 @@ struct MeshHost {
 // Analytic rectangular mesh of lib/analytic_mesh.F90:114-829 (doubly periodic
 // or closed wall), flat or with a per-node bottom level index node_K
 // (length nod2D, values in [3, nl]); full_rings = false keeps the reference's
-// incomplete periodic nod_in_elem2D lists.
+// incomplete periodic nod_in_elem2D lists; left_oriented = true reverses the
+// horizontal and vertical edges so that edge_tri(1) lies left of
+// edges(1)->edges(2) on every edge (the reference mesh has it on the right of
+// those two families and on the left of the diagonals).
 MeshHost build_analytic_mesh(int nx, int ny, int nl, double Lx, double Ly, double max_depth,
-                             bool periodic, bool full_rings, const int *node_K);
+                             bool periodic, bool full_rings, const int *node_K, bool left_oriented = false);
 
 // Number of 2D nodes of the analytic mesh.
 int analytic_nodes(int nx, int ny, bool periodic);
 
 // Seeded per-node bottom level index, uniform in [3, nl] (std::mt19937_64).
 std::vector<int> synth_bathymetry(int nnodes, int nl, uint64_t seed);
+// Seeded smooth bottom level index of the analytic grid's nodes: a Gaussian
+// random field (correlation length about corr_cells grid cells) mapped to a
+// uniform marginal on [3, nl].
+std::vector<int> synth_bathymetry_smooth(int nx, int ny, bool periodic, int nl, double corr_cells, uint64_t seed);
 
 // Seeded synthetic flow: element velocity u(k) = a1(k) U1 + f a2(k) U2 with
 // U1 = curl(psi1), U2 = curl(psi2) + grad(chi) smooth periodic patterns and
@@ -86,13 +116,17 @@ std::vector<int> synth_bathymetry(int nnodes, int nl, uint64_t seed);
 // zero over the column, so W, obtained from the discrete continuity of the
 // edge volume fluxes upward from W = 0 at the bottom, closes with W = 0 at the
 // surface (to round-off) whatever the orientation convention of edge_tri.
+// baro_frac != 0 adds a depth-independent part baro_frac curl(psi0), psi0
+// zeroed at nodes next to an element dry at the level and on walls: its edge
+// fluxes sum to zero around every node only on a mesh whose edges all carry
+// edge_tri(1) on their left (build_analytic_mesh(left_oriented = true)).
 // uv: (2, nl-1, elem2D); W: (nl, nod2D).
-void synth_velocity(const MeshHost &m, uint64_t seed, double umax, double mode2_frac,
-                    std::vector<double> &uv, std::vector<double> &W);
+void synth_velocity(const MeshHost &m, uint64_t seed, double umax, double mode2_frac, double baro_frac,
+                    double *uv, double *W);
 
 // Seeded tracer fields: kind 0 = temperature-like U[0,20] plus Gaussian blobs,
 // kind 1 = salinity-like 35 + N(0, 0.5).  (nl-1, nod2D); dry cells are 0.
-void synth_tracer(const MeshHost &m, uint64_t seed, int kind, std::vector<double> &T);
+void synth_tracer(const MeshHost &m, uint64_t seed, int kind, double *T);
 
 // Initial fields of the analytic driver (src/fesom_analytic.F90:251-256,306-331).
 void analytic_driver_fields(const MeshHost &m, std::vector<double> &T, std::vector<double> &S,

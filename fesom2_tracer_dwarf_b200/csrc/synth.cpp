@@ -1,13 +1,36 @@
 // Seeded synthetic inputs for the large analytic configurations: bathymetry,
 // a discretely consistent layered flow, and tracer fields.  All arithmetic is
 // host FP64; the generator is deterministic for a given seed.
+#include <sys/mman.h>
+
 #include <algorithm>
 #include <cmath>
+#include <cstring>
+#include <new>
 #include <random>
 
 #include "mesh.hpp"
 
 namespace fesom {
+
+template <typename T>
+HugeArray<T>::HugeArray(size_t n) : n_(n) {
+  if (n == 0) return;
+  const size_t huge = size_t(2) << 20;
+  bytes_ = (n * sizeof(T) + huge - 1) / huge * huge;
+  void *p = mmap(nullptr, bytes_, PROT_READ | PROT_WRITE, MAP_PRIVATE | MAP_ANONYMOUS, -1, 0);
+  if (p == MAP_FAILED) throw std::bad_alloc();
+  madvise(p, bytes_, MADV_HUGEPAGE);  // advisory: 4 KB pages if refused
+  p_ = static_cast<T *>(p);
+}
+
+template <typename T>
+HugeArray<T>::~HugeArray() {
+  if (p_) munmap(p_, bytes_);
+}
+
+template class HugeArray<double>;
+template class HugeArray<int>;
 
 namespace {
 
@@ -52,25 +75,83 @@ std::vector<int> synth_bathymetry(int nnodes, int nl, uint64_t seed) {
   return K;
 }
 
-void synth_velocity(const MeshHost &m, uint64_t seed, double umax, double mode2_frac,
-                    std::vector<double> &uv, std::vector<double> &W) {
+std::vector<int> synth_bathymetry_smooth(int nx, int ny, bool periodic, int nl, double corr_cells, uint64_t seed) {
+  // Gaussian random field from random-phase Fourier modes (integer wave
+  // numbers, so it is periodic), mapped through the normal CDF to a uniform
+  // marginal on [3, nl]
+  Rng r(seed);
+  const int nm = 48;
+  std::vector<double> kx(nm), ky(nm), ph(nm);
+  const double kmax = std::max(1.0, (double)std::max(nx, ny) / std::max(1.0, corr_cells));
+  for (int q = 0; q < nm; q++) {
+    double a, b;
+    do {
+      a = std::floor((2.0 * r.uni() - 1.0) * (kmax + 1.0));
+      b = std::floor((2.0 * r.uni() - 1.0) * (kmax + 1.0));
+    } while (a == 0.0 && b == 0.0);
+    kx[q] = a; ky[q] = b;
+    ph[q] = 2.0 * kPiRef * r.uni();
+  }
+  const int ni = periodic ? nx - 1 : nx, nj = periodic ? ny - 1 : ny;
+  std::vector<int> K((size_t)ni * nj);
+  const double norm = std::sqrt(2.0 / nm);
+  for (int j = 0; j < nj; j++)
+    for (int i = 0; i < ni; i++) {
+      const double x = (double)i / (double)(nx - 1), y = (double)j / (double)(ny - 1);
+      double g = 0.0;
+      for (int q = 0; q < nm; q++) g += std::cos(2.0 * kPiRef * (kx[q] * x + ky[q] * y) + ph[q]);
+      g *= norm;                                            // ~ N(0, 1)
+      const double u = 0.5 * std::erfc(-g / std::sqrt(2.0));  // ~ U(0, 1)
+      int k = 3 + (int)(u * (double)(nl - 2));
+      K[(size_t)j * ni + i] = std::min(nl, std::max(3, k));
+    }
+  return K;
+}
+
+void synth_velocity(const MeshHost &m, uint64_t seed, double umax, double mode2_frac, double baro_frac,
+                    double *uv, double *W) {
   const int N = m.nod2D, T = m.elem2D, E = m.edge2D, nl = m.nl, L = nl - 1;
   Rng rng(seed);
   std::vector<double> xm(N), ym(N);
   for (int n = 0; n < N; n++) { xm[n] = m.coord[2 * n] * kREarth; ym[n] = m.coord[2 * n + 1] * kREarth; }
   // two smooth horizontal patterns per element: U1 = curl(psi1),
   // U2 = curl(psi2) + grad(chi)
-  Modes p1, p2, chi;
+  Modes p1, p2, chi, p0;
   p1.draw(rng);
   p2.draw(rng);
   chi.draw(rng);
+  if (baro_frac != 0.0) p0.draw(rng);
   std::vector<double> f1(N), f2(N), f3(N);
   for (int n = 0; n < N; n++) {
     f1[n] = p1.eval(xm[n], ym[n], m.Lx, m.Ly);
     f2[n] = p2.eval(xm[n], ym[n], m.Lx, m.Ly);
     f3[n] = chi.eval(xm[n], ym[n], m.Lx, m.Ly);
   }
-  uv.assign((size_t)2 * L * T, 0.0);
+  const size_t nuv = (size_t)2 * L * T;
+  std::memset(uv, 0, nuv * sizeof(double));
+  // barotropic part curl(psi0): psi0 zeroed at nodes touching an element dry
+  // at the level and on walls, so that on a mesh whose edges all carry
+  // edge_tri(1) on their left its edge fluxes sum to zero at every node
+  if (baro_frac != 0.0) {
+    std::vector<int> shallowest(N, nl);
+    for (int e = 0; e < T; e++)
+      for (int q = 0; q < 3; q++) shallowest[m.elem_nodes[3 * e + q]] = std::min(shallowest[m.elem_nodes[3 * e + q]], m.nlev_elem[e]);
+    std::vector<char> wall(N, 0);
+    for (int e = 0; e < E; e++)
+      if (m.edge_tri[2 * e + 1] < 0) { wall[m.edge_nodes[2 * e]] = 1; wall[m.edge_nodes[2 * e + 1]] = 1; }
+    std::vector<double> f0(N);
+    for (int n = 0; n < N; n++) f0[n] = wall[n] ? 0.0 : baro_frac * p0.eval(xm[n], ym[n], m.Lx, m.Ly);
+    for (int e = 0; e < T; e++) {
+      const int *en = &m.elem_nodes[3 * e];
+      const double *gs = &m.grad_sca[6 * e];
+      for (int k = 0; k < m.nlev_elem[e] - 1; k++) {
+        double psi[3];
+        for (int q = 0; q < 3; q++) psi[q] = (k + 1) > shallowest[en[q]] - 1 ? 0.0 : f0[en[q]];
+        uv[2 * ((size_t)e * L + k)] += -(gs[3] * psi[0] + gs[4] * psi[1] + gs[5] * psi[2]);
+        uv[2 * ((size_t)e * L + k) + 1] += gs[0] * psi[0] + gs[1] * psi[1] + gs[2] * psi[2];
+      }
+    }
+  }
   for (int e = 0; e < T; e++) {
     const int *en = &m.elem_nodes[3 * e];
     const double *gs = &m.grad_sca[6 * e];
@@ -84,18 +165,18 @@ void synth_velocity(const MeshHost &m, uint64_t seed, double umax, double mode2_
     for (int k = 0; k < M; k++) {
       const double a1 = std::cos(kPiRef * ((double)k + 0.5) / (double)M);
       const double a2 = mode2_frac * std::cos(2.0 * kPiRef * ((double)k + 0.5) / (double)M);
-      uv[2 * ((size_t)e * L + k)] = a1 * u1 + a2 * u2;
-      uv[2 * ((size_t)e * L + k) + 1] = a1 * v1 + a2 * v2;
+      uv[2 * ((size_t)e * L + k)] += a1 * u1 + a2 * u2;
+      uv[2 * ((size_t)e * L + k) + 1] += a1 * v1 + a2 * v2;
     }
   }
   double vmax = 0.0;
-  for (size_t i = 0; i < uv.size() / 2; i++) vmax = std::max(vmax, std::hypot(uv[2 * i], uv[2 * i + 1]));
+  for (size_t i = 0; i < nuv / 2; i++) vmax = std::max(vmax, std::hypot(uv[2 * i], uv[2 * i + 1]));
   const double scale = vmax > 0.0 ? umax / vmax : 0.0;
-  for (double &v : uv) v *= scale;
+  for (size_t i = 0; i < nuv; i++) uv[i] *= scale;
 
   // horizontal divergence D(n,k) of the edge volume fluxes, with the same
   // segment rule the advection kernels use
-  std::vector<double> D((size_t)L * N, 0.0);
+  HugeArray<double> D((size_t)L * N);
   for (int e = 0; e < E; e++) {
     const int n1 = m.edge_nodes[2 * e], n2 = m.edge_nodes[2 * e + 1];
     const int t1 = m.edge_tri[2 * e], t2 = m.edge_tri[2 * e + 1];
@@ -111,7 +192,7 @@ void synth_velocity(const MeshHost &m, uint64_t seed, double umax, double mode2_
   }
   // W from bottom to top: W(k) A(k) = W(k+1) A(k+1) - D(k); W = 0 at the
   // bottom and at the surface
-  W.assign((size_t)nl * N, 0.0);
+  std::memset(W, 0, (size_t)nl * N * sizeof(double));
   for (int n = 0; n < N; n++) {
     const int nlev = m.nlev_node[n];
     for (int i = nlev - 1; i >= 2; i--) {  // 1-based interface i, top of layer i
@@ -123,10 +204,10 @@ void synth_velocity(const MeshHost &m, uint64_t seed, double umax, double mode2_
   }
 }
 
-void synth_tracer(const MeshHost &m, uint64_t seed, int kind, std::vector<double> &T) {
+void synth_tracer(const MeshHost &m, uint64_t seed, int kind, double *T) {
   const int N = m.nod2D, L = m.nl - 1;
   Rng r(seed);
-  T.assign((size_t)L * N, 0.0);
+  std::memset(T, 0, (size_t)L * N * sizeof(double));
   if (kind == 0) {
     double bx[8], by[8], bs[8], ba[8];
     for (int b = 0; b < 8; b++) {

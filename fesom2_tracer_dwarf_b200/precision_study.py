@@ -1,0 +1,86 @@
+"""Precision study: FP32, BF16-storage and FP16-storage runs of the tracer
+step against the FP64 path on identical seeded inputs.
+
+The FP64 path is bit-identical to the CPU oracle (tests/test_gpu_parity.py
+checks it at every size up to 1000x1000x64), so it serves as the FP64
+reference at sizes where a CPU run would take hours.  Reported per mode and
+tracer: relative L2 and max-abs error of the final field over wet cells, the
+drift of the conserved content Sum(T*areasvol*hnode_new) (compensated FP64
+sum on the device), and device time per step.
+
+    python -m fesom2_tracer_dwarf_b200.precision_study --nx 2000 --nl 48 --steps 200
+"""
+from __future__ import annotations
+
+import argparse
+import json
+
+import numpy as np
+
+from .tracer import FESOMTracerAdvection
+from .workloads import layered_flow_case
+
+
+def run_mode(api, c, mode, steps, hor="MUSCL", ver="PPM", lim="FCT"):
+    """Advance both tracers of case c (mesh already in api) steps steps in one precision mode."""
+    T, S, uv, w, dt, wet = c.T, c.S, c.uv, c.w, c.dt, c.wet
+    api.set_precision(mode)
+    api.allocate_tracers(2)
+    api.set_values(1, T)
+    api.set_values(2, S)
+    for t in (1, 2):
+        api.set_scheme(t, hor, ver, lim)
+    api.set_velocity(uv, w)
+    api.set_ab_refresh(True)
+    v0 = [api.volume_sum(t)[1] for t in (1, 2)]
+    ms = api.time_steps(steps, dt)
+    v1 = [api.volume_sum(t)[1] for t in (1, 2)]
+    out = [api.get_tracer_values(t) for t in (1, 2)]
+    return {"fields": out, "wet": wet, "v0": v0, "v1": v1, "ms_per_step": ms / steps, "cells": c.wet_cells,
+            "dt": dt}
+
+
+def compare(ref, res):
+    wet = ref["wet"]
+    rows = []
+    for t in range(2):
+        a, b = res["fields"][t][wet], ref["fields"][t][wet]
+        rows.append({
+            "tracer": t + 1,
+            "l2_rel": float(np.linalg.norm(a - b) / np.linalg.norm(b)),
+            "linf_abs": float(np.max(np.abs(a - b))),
+            "content_drift_rel": float((res["v1"][t] - res["v0"][t]) / res["v0"][t]),
+            "content_drift_rel_fp64": float((ref["v1"][t] - ref["v0"][t]) / ref["v0"][t]),
+        })
+    return rows
+
+
+def study(nx, nl, steps, modes=("fp32", "bf16", "fp16"), seed=0):
+    api = FESOMTracerAdvection()
+    api.cleanup()
+    c = layered_flow_case(api, nx, nl, seed=seed)
+    ref = run_mode(api, c, "fp64", steps)
+    out = {"config": {"nx": nx, "nl": nl, "steps": steps, "wet_cells": ref["cells"], "seed": seed,
+                      "dt_s": ref["dt"]},
+           "fp64_ms_per_step": ref["ms_per_step"], "modes": {}}
+    for m in modes:
+        res = run_mode(api, c, m, steps)
+        out["modes"][m] = {"ms_per_step": res["ms_per_step"],
+                           "cell_updates_per_s": 2 * res["cells"] / (res["ms_per_step"] / 1e3),
+                           "errors": compare(ref, res)}
+    out["fp64_cell_updates_per_s"] = 2 * ref["cells"] / (ref["ms_per_step"] / 1e3)
+    api.cleanup()
+    return out
+
+
+def main():
+    p = argparse.ArgumentParser()
+    p.add_argument("--nx", type=int, default=2000)
+    p.add_argument("--nl", type=int, default=48)
+    p.add_argument("--steps", type=int, default=200)
+    a = p.parse_args()
+    print(json.dumps(study(a.nx, a.nl, a.steps), indent=1))
+
+
+if __name__ == "__main__":
+    main()

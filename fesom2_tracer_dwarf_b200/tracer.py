@@ -69,15 +69,15 @@ class FESOMTracerAdvection:
 
     # ---- extensions ---------------------------------------------------------
     def init_analytic(self, nx, ny, nl, Lx=1.0e5, Ly=1.0e5, max_depth=1000.0, periodic=True,
-                      full_rings=True, node_K=None):
+                      full_rings=True, node_K=None, left_oriented=False):
         """Analytic mesh of the reference's generate_analytic_mesh (+ optional bathymetry)."""
         K = None
         if node_K is not None:
             K = np.ascontiguousarray(node_K, dtype=np.int32)
             if K.size != self.lib.tracer_analytic_nodes(nx, ny, int(periodic)):
                 raise ValueError("node_K must have one entry per mesh node")
-        rc = self.lib.tracer_init_analytic(nx, ny, nl, Lx, Ly, max_depth, int(periodic), int(full_rings),
-                                           _lib.ptr(K))
+        opts = int(bool(full_rings)) | (2 if left_oriented else 0)
+        rc = self.lib.tracer_init_analytic(nx, ny, nl, Lx, Ly, max_depth, int(periodic), opts, _lib.ptr(K))
         _lib.check(self.lib, rc, "tracer_init_analytic")
         self.dims = self.mesh_dims()
         return rc
@@ -115,6 +115,18 @@ class FESOMTracerAdvection:
         rc = self.lib.tracer_set_velocity_elem(_lib.ptr(u), _lib.ptr(ww), d["nl"], d["nod2D"], d["elem2D"])
         _lib.check(self.lib, rc, "tracer_set_velocity_elem")
 
+    PRECISIONS = {"fp64": 0, "fp32": 1, "bf16": 2, "fp16": 3}
+
+    def set_precision(self, mode):
+        """'fp64' (bit-exact), 'fp32', 'bf16' or 'fp16' (16-bit tracer storage, FP32 arithmetic)."""
+        _lib.check(self.lib, self.lib.tracer_set_precision(self.PRECISIONS[mode]), "tracer_set_precision")
+
+    def volume_sum(self, tracer_id=1):
+        """(Sum T, Sum T*areasvol*hnode_new) over wet cells, compensated FP64 on the device."""
+        out = np.zeros(2)
+        _lib.check(self.lib, self.lib.tracer_volume_sum(tracer_id, _lib.ptr(out)), "tracer_volume_sum")
+        return float(out[0]), float(out[1])
+
     def set_ab_refresh(self, on):
         self.lib.tracer_set_ab_refresh(int(bool(on)))
 
@@ -133,11 +145,12 @@ class FESOMTracerAdvection:
                    "tracer_analytic_fields")
         return Tt, S, uv, w
 
-    def synth_velocity(self, seed=0, umax=1.0, mode2=0.5):
+    def synth_velocity(self, seed=0, umax=1.0, mode2=0.5, baro=0.0):
+        """Seeded layered flow (see tracer_synth_velocity): uv (2, nl-1, elem2D), w (nl, nod2D)."""
         d = self.mesh_dims()
         uv = np.zeros((2, d["nl"] - 1, d["elem2D"]), order="F")
         w = np.zeros((d["nl"], d["nod2D"]), order="F")
-        _lib.check(self.lib, self.lib.tracer_synth_velocity(seed, umax, mode2, _lib.ptr(uv), _lib.ptr(w)),
+        _lib.check(self.lib, self.lib.tracer_synth_velocity(seed, umax, mode2, baro, _lib.ptr(uv), _lib.ptr(w)),
                    "tracer_synth_velocity")
         return uv, w
 
@@ -166,6 +179,15 @@ class FESOMTracerAdvection:
 
     def cleanup(self):
         return self.lib.tracer_cleanup()
+
+
+def synth_bathymetry_smooth(nx, ny, nl, periodic=True, corr_cells=40.0, seed=0):
+    """Smooth seeded bottom level index (uniform marginal on [3, nl]) per node of the analytic grid."""
+    lib = _lib.load()
+    K = np.zeros(lib.tracer_analytic_nodes(nx, ny, int(periodic)), dtype=np.int32)
+    _lib.check(lib, lib.tracer_synth_bathymetry_smooth(nx, ny, int(periodic), nl, corr_cells, seed, _lib.ptr(K)),
+               "tracer_synth_bathymetry_smooth")
+    return K
 
 
 def synth_bathymetry(nnodes, nl, seed=0):

@@ -87,10 +87,14 @@ int tracer_init_for_advection(void);
 
 /* Analytic mesh of lib/analytic_mesh.F90:114 (generate_analytic_mesh) with
  * the ALE arrays of src/fesom_analytic.F90:206-244.  node_K (nullable,
- * length nod2D) is a per-node bottom level index in [3, nl].  full_rings = 0
- * keeps the reference's incomplete periodic nod_in_elem2D lists. */
+ * length nod2D) is a per-node bottom level index in [3, nl].  options bit 0:
+ * 1 rebuilds the periodic nod_in_elem2D lists after the halo remap, 0 keeps
+ * the reference's incomplete ones.  options bit 1: reverse the horizontal and
+ * vertical edges so that edge_tri(1) lies left of edges(1)->edges(2) on every
+ * edge (the reference mesh has it on the right of those edges and on the left
+ * of the diagonals, so its fluxes across them point against the flow). */
 int tracer_init_analytic(int nx, int ny, int nl, double Lx, double Ly, double max_depth,
-                         int periodic, int full_rings, const int *node_K);
+                         int periodic, int options, const int *node_K);
 /* Number of nodes of the analytic mesh (nx, ny, periodic). */
 int tracer_analytic_nodes(int nx, int ny, int periodic);
 /* Generic mesh from arrays (1-based Fortran indices, 0 = no element):
@@ -122,6 +126,15 @@ int tracer_set_values_ab(int tracer_id, const double *values, int nl, int nod2D)
 /* 1: valuesAB := values before every step; 0 (default, as the reference
  * drivers): valuesAB stays as set. */
 int tracer_set_ab_refresh(int on);
+/* Arithmetic mode of the device state: 0 FP64 (default, bit-identical to the
+ * reference algorithm), 1 FP32, 2 BF16 tracer storage with FP32 arithmetic, 3
+ * FP16 tracer storage with FP32 arithmetic; in modes 1-3 the FCT ratio
+ * denominators are formed in FP64.  Changing it rebuilds the device state and
+ * keeps the tracer values. */
+int tracer_set_precision(int mode);
+/* Compensated FP64 sums over the wet cells of one tracer, on the device:
+ * out2[0] = Sum T, out2[1] = Sum T*areasvol*hnode_new (conserved content). */
+int tracer_volume_sum(int tracer_id, double *out2);
 /* nsteps steps of every tracer. */
 int tracer_advect_steps(int nsteps, double dt);
 /* Values / stats of tracer tracer_id (1-based). stats4 = min, max, sum, nan. */
@@ -131,10 +144,17 @@ int tracer_get_stats_id(int tracer_id, double *stats4);
  * T, S (nl-1, nod2D), uv (2, nl-1, elem2D), w (nl, nod2D); any may be NULL. */
 int tracer_analytic_fields(double *T, double *S, double *uv, double *w);
 /* Seeded synthetic inputs: bathymetry K(nnodes) in [3, nl]; a layered flow
- * for the current mesh; a tracer field (kind 0 temperature-like, 1
- * salinity-like). */
+ * for the current mesh (two zero-column-mean vertical modes, the second
+ * weighted by mode2_frac, plus baro_frac times a depth-independent
+ * non-divergent part, which needs a left-oriented mesh; w from the discrete
+ * continuity); a tracer field (kind 0 temperature-like, 1 salinity-like). */
 int tracer_synth_bathymetry(int nnodes, int nl, uint64_t seed, int *K);
-int tracer_synth_velocity(uint64_t seed, double umax, double mode2_frac, double *uv, double *w);
+int tracer_synth_velocity(uint64_t seed, double umax, double mode2_frac, double baro_frac, double *uv,
+                          double *w);
+/* Smooth seeded bathymetry of the analytic grid (tracer_analytic_nodes
+ * entries): a random field of correlation length ~corr_cells cells with a
+ * uniform marginal on [3, nl]. */
+int tracer_synth_bathymetry_smooth(int nx, int ny, int periodic, int nl, double corr_cells, uint64_t seed, int *K);
 int tracer_synth_tracer(uint64_t seed, int kind, double *values);
 /* Mesh sizes: nl, nod2D, elem2D, edge2D, wet cells (low 31 bits), level stride. */
 int tracer_mesh_dims(int *dims6);

@@ -234,12 +234,13 @@ static void build_nod_in_elem(om_mesh *m, int nnodes) {
 }
 
 om_mesh *om_mesh_analytic(int nx, int ny, int nl, double Lx, double Ly,
-                          double max_depth, int periodic, int full_rings,
+                          double max_depth, int periodic, int options,
                           const int *node_K) {
   if (nx < 2 || ny < 2 || nl < 3) return NULL;
   om_mesh *m = (om_mesh *)calloc(1, sizeof(om_mesh));
   m->nx = nx; m->ny = ny; m->nl = nl; m->periodic = periodic ? 1 : 0;
-  m->full_rings = full_rings ? 1 : 0;
+  m->full_rings = (options & OM_FULL_RINGS) ? 1 : 0;
+  const int left = (options & OM_LEFT_ORIENTED) ? 1 : 0;
   m->Lx = Lx; m->Ly = Ly; m->max_depth = max_depth;
 
   /* 1b. sizes (lib/analytic_mesh.F90:175-190) */
@@ -332,7 +333,7 @@ om_mesh *om_mesh_analytic(int nx, int ny, int nl, double Lx, double Ly,
       for (int j = 1; j <= ny - 1; j++)
         for (int i = 1; i <= nx - 1; i++) {
           c++;
-          A2(en, 1, c, 2) = PNODE(i, j); A2(en, 2, c, 2) = PNODE(i + 1, j);
+          A2(en, 1 + left, c, 2) = PNODE(i, j); A2(en, 2 - left, c, 2) = PNODE(i + 1, j);
           int e_lower = 2 * ((j - 1) * (nx - 1) + (i - 1)) + 1;
           int e_upper = (j >= 2) ? 2 * ((j - 2) * (nx - 1) + (i - 1)) + 2
                                  : 2 * ((ny - 2) * (nx - 1) + (i - 1)) + 2;
@@ -341,7 +342,7 @@ om_mesh *om_mesh_analytic(int nx, int ny, int nl, double Lx, double Ly,
       for (int j = 1; j <= ny - 1; j++)
         for (int i = 1; i <= nx - 1; i++) {
           c++;
-          A2(en, 1, c, 2) = PNODE(i, j); A2(en, 2, c, 2) = PNODE(i, j + 1);
+          A2(en, 1 + left, c, 2) = PNODE(i, j); A2(en, 2 - left, c, 2) = PNODE(i, j + 1);
           int e_upper = 2 * ((j - 1) * (nx - 1) + (i - 1)) + 2;
           int e_lower = (i >= 2) ? 2 * ((j - 1) * (nx - 1) + (i - 2)) + 1
                                  : 2 * ((j - 1) * (nx - 1) + (nx - 2)) + 1;
@@ -360,7 +361,7 @@ om_mesh *om_mesh_analytic(int nx, int ny, int nl, double Lx, double Ly,
       for (int j = 1; j <= ny; j++)
         for (int i = 1; i <= nx - 1; i++) {
           c++;
-          A2(en, 1, c, 2) = (j - 1) * nx + i; A2(en, 2, c, 2) = (j - 1) * nx + i + 1;
+          A2(en, 1 + left, c, 2) = (j - 1) * nx + i; A2(en, 2 - left, c, 2) = (j - 1) * nx + i + 1;
           int e_lower = (j <= ny - 1) ? 2 * ((j - 1) * (nx - 1) + (i - 1)) + 1 : 0;
           int e_upper = (j >= 2) ? 2 * ((j - 2) * (nx - 1) + (i - 1)) + 2 : 0;
           A2(ee, 1, c, 2) = e_upper; A2(ee, 2, c, 2) = e_lower;
@@ -368,7 +369,7 @@ om_mesh *om_mesh_analytic(int nx, int ny, int nl, double Lx, double Ly,
       for (int j = 1; j <= ny - 1; j++)
         for (int i = 1; i <= nx; i++) {
           c++;
-          A2(en, 1, c, 2) = (j - 1) * nx + i; A2(en, 2, c, 2) = j * nx + i;
+          A2(en, 1 + left, c, 2) = (j - 1) * nx + i; A2(en, 2 - left, c, 2) = j * nx + i;
           int e_upper = (i <= nx - 1) ? 2 * ((j - 1) * (nx - 1) + (i - 1)) + 2 : 0;
           int e_lower = (i >= 2) ? 2 * ((j - 1) * (nx - 1) + (i - 2)) + 1 : 0;
           A2(ee, 1, c, 2) = e_upper; A2(ee, 2, c, 2) = e_lower;

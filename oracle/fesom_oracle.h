@@ -28,13 +28,19 @@ enum { OM_VER_UPW1 = 0, OM_VER_PPM = 1, OM_VER_QR4C = 2, OM_VER_CDIFF = 3 };
 enum { OM_LIM_NONE = 0, OM_LIM_FCT = 1 };
 
 /* Build the analytic mesh of lib/analytic_mesh.F90:114 (periodic or closed).
- * full_rings = 0 keeps the reference's periodic nod_in_elem2D lists, which are
- * built before the halo remap and are therefore incomplete on the wrap rows
- * (lib/analytic_mesh.F90:674-694); full_rings = 1 rebuilds them after the remap.
+ * options bit 0 (OM_FULL_RINGS): 0 keeps the reference's periodic
+ * nod_in_elem2D lists, which are built before the halo remap and are therefore
+ * incomplete on the wrap rows (lib/analytic_mesh.F90:674-694); 1 rebuilds them
+ * after the remap.  options bit 1 (OM_LEFT_ORIENTED): reverse the node order
+ * of the horizontal and vertical edges so that edge_tri(1) lies to the left of
+ * edges(1)->edges(2) on every edge, as it does on the diagonals of the
+ * reference mesh (lib/analytic_mesh.F90:386-441 puts it on the right of the
+ * horizontal and vertical edges).
  * node_K (length nod2D, nullable) gives a per-node bottom level index in
  * [3, nl]; NULL reproduces the reference's flat bottom (nlevels = nl). */
+enum { OM_FULL_RINGS = 1, OM_LEFT_ORIENTED = 2 };
 om_mesh *om_mesh_analytic(int nx, int ny, int nl, double Lx, double Ly,
-                          double max_depth, int periodic, int full_rings,
+                          double max_depth, int periodic, int options,
                           const int *node_K);
 void om_mesh_free(om_mesh *m);
 

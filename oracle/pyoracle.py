@@ -68,10 +68,11 @@ class OracleMesh:
     """An analytic mesh built by the oracle (lib/analytic_mesh.F90 restated)."""
 
     def __init__(self, oracle: Oracle, nx, ny, nl, Lx=1.0e5, Ly=1.0e5, max_depth=1000.0, periodic=True,
-                 full_rings=True, node_K=None):
+                 full_rings=True, node_K=None, left_oriented=False):
         self.o = oracle
         K = None if node_K is None else np.ascontiguousarray(node_K, dtype=np.int32)
-        h = oracle.lib.om_mesh_analytic(nx, ny, nl, Lx, Ly, max_depth, int(periodic), int(full_rings), _p(K))
+        opts = int(bool(full_rings)) | (2 if left_oriented else 0)
+        h = oracle.lib.om_mesh_analytic(nx, ny, nl, Lx, Ly, max_depth, int(periodic), opts, _p(K))
         if not h:
             raise ValueError("oracle mesh construction failed")
         self.h = ctypes.c_void_p(h)

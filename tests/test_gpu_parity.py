@@ -190,28 +190,31 @@ def volume_sum(api, T):
 
 
 def test_c2_size_one_step_bitwise_and_conservation(api):
-    """The 1000x1000x64 periodic configuration with random bathymetry:
-    one GPU step against the OpenMP oracle bit for bit, then 5 more steps
-    conserving Sum(T*vol) to FP64 round-off."""
+    """The benchmark's 1000x1000x64 periodic case (smooth bathymetry,
+    divergence-free layered flow, two tracers): one GPU step against the
+    OpenMP oracle bit for bit, then 5 more steps conserving Sum(T*vol) to
+    FP64 round-off."""
+    from fesom2_tracer_dwarf_b200.workloads import layered_flow_case
     oracle = pyoracle.Oracle(openmp=True)
     nx = ny = 1000
     nl = 64
-    K, uv, w, T, S, dt = synth_case(api, nx, ny, nl, True, 0)
-    sch = ("MUSCL", "PPM", "FCT", 1.0, 1.0)
-    api.allocate_tracers(1)
-    api.set_values(1, T)
-    api.set_scheme(1, *sch)
-    api.set_velocity(uv, w)
+    c = layered_flow_case(api, nx, nl, seed=0)
+    api.allocate_tracers(2)
+    api.set_values(1, c.T)
+    api.set_values(2, c.S)
+    for t in (1, 2):
+        api.set_scheme(t, "MUSCL", "PPM", "FCT")
+    api.set_velocity(c.uv, c.w)
     api.set_ab_refresh(True)
-    s0, wet = volume_sum(api, T)
-    api.advect_steps(1, dt)
-    m = pyoracle.OracleMesh(oracle, nx, ny, nl, periodic=True, full_rings=True, node_K=K)
-    To = T.copy(order="F")
-    m.step(To, To.copy(order="F"), uv, w, dt, "MUSCL", "PPM", "FCT")
+    s0, wet = volume_sum(api, c.T)
+    api.advect_steps(1, c.dt)
+    m = pyoracle.OracleMesh(oracle, nx, ny, nl, periodic=True, full_rings=True, node_K=c.K, left_oriented=True)
+    for tid, F in ((1, c.T), (2, c.S)):
+        Fo = F.copy(order="F")
+        m.step(Fo, Fo.copy(order="F"), c.uv, c.w, c.dt, "MUSCL", "PPM", "FCT")
+        assert_bitwise(api.get_tracer_values(tid), Fo, f"C2 tracer {tid} step 1")
     del m
-    G = api.get_tracer_values(1)
-    assert_bitwise(G, To, "C2 step 1")
-    api.advect_steps(5, dt)
+    api.advect_steps(5, c.dt)
     G = api.get_tracer_values(1)
     assert np.all(np.isfinite(G[wet]))
     s1, _ = volume_sum(api, G)

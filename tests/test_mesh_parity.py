@@ -7,13 +7,15 @@ import pytest
 import pyoracle
 
 CASES = [
-    # nx, ny, nl, periodic, full_rings, bathymetry seed (None = flat)
-    (20, 20, 10, True, False, None),
-    (20, 20, 10, True, True, None),
-    (9, 7, 6, False, True, None),
-    (17, 13, 9, True, True, 4),
-    (11, 15, 8, False, True, 6),
-    (6, 5, 4, True, False, None),
+    # nx, ny, nl, periodic, full_rings, bathymetry seed (None = flat), left-oriented
+    (15, 12, 7, True, True, 8, True),
+    (9, 11, 5, False, True, 9, True),
+    (20, 20, 10, True, False, None, False),
+    (20, 20, 10, True, True, None, False),
+    (9, 7, 6, False, True, None, False),
+    (17, 13, 9, True, True, 4, False),
+    (11, 15, 8, False, True, 6, False),
+    (6, 5, 4, True, False, None, False),
 ]
 
 FIELDS_D = ["coord", "elem_area", "area", "areasvol", "edge_dxdy", "edge_cross_dxdy", "gradient_sca", "hnode",
@@ -22,14 +24,14 @@ FIELDS_I = ["elem2D_nodes", "edges", "edge_tri", "nlevels", "nlevels_nod2D", "nl
             "edge_up_dn_tri", "nboundary_lay"]
 
 
-@pytest.mark.parametrize("nx,ny,nl,periodic,full,seed", CASES)
-def test_mesh_bitwise(oracle, api, nx, ny, nl, periodic, full, seed):
+@pytest.mark.parametrize("nx,ny,nl,periodic,full,seed,left", CASES)
+def test_mesh_bitwise(oracle, api, nx, ny, nl, periodic, full, seed, left):
     from fesom2_tracer_dwarf_b200 import synth_bathymetry
     K = None
     if seed is not None:
         K = synth_bathymetry(api.lib.tracer_analytic_nodes(nx, ny, int(periodic)), nl, seed)
-    api.init_analytic(nx, ny, nl, periodic=periodic, full_rings=full, node_K=K)
-    m = pyoracle.OracleMesh(oracle, nx, ny, nl, periodic=periodic, full_rings=full, node_K=K)
+    api.init_analytic(nx, ny, nl, periodic=periodic, full_rings=full, node_K=K, left_oriented=left)
+    m = pyoracle.OracleMesh(oracle, nx, ny, nl, periodic=periodic, full_rings=full, node_K=K, left_oriented=left)
     d = api.mesh_dims()
     assert (d["nl"], d["nod2D"], d["elem2D"], d["edge2D"]) == (m.nl, m.nod2D, m.elem2D, m.edge2D)
     for name in FIELDS_I + FIELDS_D:
