@@ -55,6 +55,8 @@ SIGNATURES = {
     "tracer_set_values_ab": (ctypes.c_int, [ctypes.c_int, _vp, ctypes.c_int, ctypes.c_int]),
     "tracer_set_ab_refresh": (ctypes.c_int, [ctypes.c_int]),
     "tracer_set_precision": (ctypes.c_int, [ctypes.c_int]),
+    "tracer_set_rounding": (ctypes.c_int, [ctypes.c_int]),
+    "tracer_storage_offset": (ctypes.c_int, [ctypes.c_int, _vp]),
     "tracer_volume_sum": (ctypes.c_int, [ctypes.c_int, _vp]),
     "tracer_advect_steps": (ctypes.c_int, [ctypes.c_int, ctypes.c_double]),
     "tracer_get_values_id": (ctypes.c_int, [ctypes.c_int, _vp, ctypes.c_int, ctypes.c_int]),
@@ -76,6 +78,8 @@ SIGNATURES = {
     "tracer_launches_per_step": (ctypes.c_int, []),
     "tracer_device_bytes": (ctypes.c_longlong, []),
     "tracer_selftest_division": (ctypes.c_int, [ctypes.c_longlong, ctypes.c_uint64, _vp, _vp]),
+    "tracer_selftest_sround": (ctypes.c_int, [ctypes.c_int, ctypes.c_longlong, ctypes.c_int, ctypes.c_uint32,
+                                              ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_double)]),
     "tracer_advect_device_noalloc": (ctypes.c_int, [ctypes.c_int, _vp, _vp, _vp, ctypes.c_double]),
     "tracer_noalloc_scratch_bytes": (ctypes.c_longlong, []),
     "tracer_last_error": (ctypes.c_char_p, []),

@@ -83,6 +83,9 @@ struct FusedArgs {
   const R *vel;           // (2, S, elem)
   const R *W;             // (S, node) interfaces
   R dt, ph, pv;
+  R off[NTMAX];           // storage offsets (16-bit storage)
+  uint32_t seed[NTMAX];   // per-step random stream of each tracer (stochastic rounding)
+  int sround;             // 1: stochastic rounding of 16-bit stores
 };
 
 // ---------------------------------------------------------------------------
@@ -113,20 +116,22 @@ __device__ __forceinline__ CellMap map_cells(const DSched &sc, int *s_off, int *
 // k_edge
 // ---------------------------------------------------------------------------
 template <typename R, typename TS>
-__device__ __forceinline__ void trxy_n(const DMeshT<R> &m, const TS *const *tab, int NT, int elem, int k, R *gx, R *gy) {
+__device__ __forceinline__ void trxy_n(const DMeshT<R> &m, const TS *const *tab, const R *off, int NT, int elem, int k,
+                                       R *gx, R *gy) {
   const int *en = m.elem_nodes + 3 * elem;
   const int a = en[0], b = en[1], c = en[2];
   const R *gs = m.grad_sca + 6 * elem;
   const R g0 = gs[0], g1 = gs[1], g2 = gs[2], g3 = gs[3], g4 = gs[4], g5 = gs[5];
   for (int t = 0; t < NT; t++) {
-    const R t1 = R(tab[t][(size_t)a * m.S + k]), t2 = R(tab[t][(size_t)b * m.S + k]), t3 = R(tab[t][(size_t)c * m.S + k]);
+    const R t1 = ldT(tab[t], (size_t)a * m.S + k, off[t]), t2 = ldT(tab[t], (size_t)b * m.S + k, off[t]), t3 = ldT(tab[t], (size_t)c * m.S + k, off[t]);
     gx[t] = (g0 * t1 + g1 * t2) + g2 * t3;
     gy[t] = (g3 * t1 + g4 * t2) + g5 * t3;
   }
 }
 
 template <typename R, typename TS>
-__device__ __forceinline__ void ring_mean_n(const DMeshT<R> &m, const TS *const *tab, int NT, int n, int k, R *gx, R *gy) {
+__device__ __forceinline__ void ring_mean_n(const DMeshT<R> &m, const TS *const *tab, const R *off, int NT, int n, int k,
+                                            R *gx, R *gy) {
   R tvol = R(0), tx[NTMAX], ty[NTMAX];
   for (int t = 0; t < NT; t++) { tx[t] = R(0); ty[t] = R(0); }
   const int nz = k + 1;
@@ -134,7 +139,7 @@ __device__ __forceinline__ void ring_mean_n(const DMeshT<R> &m, const TS *const 
     const int el = m.ring_elem[p];
     if (m.nlev_elem[el] - 1 < nz) continue;
     R ax[NTMAX], ay[NTMAX];
-    trxy_n(m, tab, NT, el, k, ax, ay);
+    trxy_n(m, tab, off, NT, el, k, ax, ay);
     const R a = m.elem_area[el];
     tvol = tvol + a;
     for (int t = 0; t < NT; t++) {
@@ -163,8 +168,8 @@ __global__ void __launch_bounds__(kThreads, 4) k_edge(DMeshT<R> m, FusedArgs<R, 
     const size_t o1 = (size_t)c.n1 * m.S + k, o2 = (size_t)c.n2 * m.S + k;
     if (HOR == HOR_UPW1) {
       for (int t = 0; t < NT; t++) {
-        const R flo = (LIM == LIM_FCT) ? upw1_flux(vflux, R(a.T[t][o1]), R(a.T[t][o2])) : R(0);
-        a.adf_h[t][o] = upw1_flux(vflux, R(a.TAB[t][o1]), R(a.TAB[t][o2])) - flo;
+        const R flo = (LIM == LIM_FCT) ? upw1_flux(vflux, ldT(a.T[t], o1, a.off[t]), ldT(a.T[t], o2, a.off[t])) : R(0);
+        a.adf_h[t][o] = upw1_flux(vflux, ldT(a.TAB[t], o1, a.off[t]), ldT(a.TAB[t], o2, a.off[t])) - flo;
       }
       continue;
     }
@@ -174,11 +179,11 @@ __global__ void __launch_bounds__(kThreads, 4) k_edge(DMeshT<R> m, FusedArgs<R, 
     bool shared = false;
     if (ud.x >= 0 && ud.y >= 0) shared = (k + 1) <= min(m.nlev_node_min[c.n1], m.nlev_node_min[c.n2]) - 1;
     if (shared) {
-      trxy_n(m, a.TAB, NT, ud.x, k, gux, guy);
-      trxy_n(m, a.TAB, NT, ud.y, k, gdx, gdy);
+      trxy_n(m, a.TAB, a.off, NT, ud.x, k, gux, guy);
+      trxy_n(m, a.TAB, a.off, NT, ud.y, k, gdx, gdy);
     } else {
-      ring_mean_n(m, a.TAB, NT, c.n1, k, gux, guy);
-      ring_mean_n(m, a.TAB, NT, c.n2, k, gdx, gdy);
+      ring_mean_n(m, a.TAB, a.off, NT, c.n1, k, gux, guy);
+      ring_mean_n(m, a.TAB, a.off, NT, c.n2, k, gdx, gdy);
     }
     const R ex = m.edge_dxdy[2 * e], ey = m.edge_dxdy[2 * e + 1], aa = m.edge_a[e];
     R c_lo1 = R(1), c_lo2 = R(1);
@@ -187,7 +192,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_edge(DMeshT<R> m, FusedArgs<R, 
       c_lo2 = (m.nbl[c.n2] - (k + 1) >= 0) ? R(1) : R(0);
     }
     for (int t = 0; t < NT; t++) {
-      const R t1 = R(a.TAB[t][o1]), t2 = R(a.TAB[t][o2]);
+      const R t1 = ldT(a.TAB[t], o1, a.off[t]), t2 = ldT(a.TAB[t], o2, a.off[t]);
       R Tmean2, Tmean1;
       // lib/oce_adv_tra_hor.F90:454-469 (MUSCL), :743-753 (MFCT, no c_lo)
       const R x2 = R(2) * (t2 - t1) + ex * aa * gdx[t] + ey * re * gdy[t];
@@ -201,7 +206,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_edge(DMeshT<R> m, FusedArgs<R, 
       }
       const R cHO = (vflux + fabs(vflux)) * Tmean1 + (vflux - fabs(vflux)) * Tmean2;
       const R ho = -(R(0.5) * (R(1) - a.ph) * cHO) - vflux * a.ph * R(0.5) * (Tmean1 + Tmean2);
-      const R flo = (LIM == LIM_FCT) ? upw1_flux(vflux, R(a.T[t][o1]), R(a.T[t][o2])) : R(0);
+      const R flo = (LIM == LIM_FCT) ? upw1_flux(vflux, ldT(a.T[t], o1, a.off[t]), ldT(a.T[t], o2, a.off[t])) : R(0);
       a.adf_h[t][o] = ho - flo;
     }
   }
@@ -247,7 +252,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_col1(DMeshT<R> m, FusedArgs<R, 
         const R vf = a.vflux[(size_t)(q.x >> 1) * S + k];
         const size_t o1 = (size_t)(second ? q.y : n) * S + k, o2 = (size_t)(second ? n : q.y) * S + k;
         for (int t = 0; t < NT; t++) {
-          const R F = upw1_flux(vf, R(a.T[t][o1]), R(a.T[t][o2]));
+          const R F = upw1_flux(vf, ldT(a.T[t], o1, a.off[t]), ldT(a.T[t], o2, a.off[t]));
           acc[t] = second ? acc[t] - F : acc[t] + F;
         }
       }
@@ -263,7 +268,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_col1(DMeshT<R> m, FusedArgs<R, 
         const R c3 = (dzj + R(2) * dzjp1) / (dzjm1 + dzj);
         for (int t = 0; t < NT; t++) {
           const TS *Tc = a.TAB[t] + (size_t)n * S;
-          s_slope[t * kMaxCellsPerBlock + lc] = ppm_slope(R(Tc[k - 1]), R(Tc[k]), R(Tc[k + 1]), c1, c2, c3);
+          s_slope[t * kMaxCellsPerBlock + lc] = ppm_slope(ldT(Tc, k - 1, a.off[t]), ldT(Tc, k, a.off[t]), ldT(Tc, k + 1, a.off[t]), c1, c2, c3);
         }
       }
     }
@@ -278,17 +283,17 @@ __global__ void __launch_bounds__(kThreads, 4) k_col1(DMeshT<R> m, FusedArgs<R, 
       const R *HN = m.hnode_new + (size_t)n * S;
       const R *Wc = a.W + (size_t)n * S;
       if (i == 1) {
-        for (int t = 0; t < NT; t++) s_tv[t * kMaxCellsPerBlock + lc] = R(a.TAB[t][(size_t)n * S]);
+        for (int t = 0; t < NT; t++) s_tv[t * kMaxCellsPerBlock + lc] = ldT(a.TAB[t], (size_t)n * S, a.off[t]);
       } else if (i == nlev - 1) {
         const R s = sgn1(Wc[nlev - 2]);
         for (int t = 0; t < NT; t++) {
           const TS *Tc = a.TAB[t] + (size_t)n * S;
-          s_tv[t * kMaxCellsPerBlock + lc] = -R(Tc[nlev - 3]) * fmin2(s, R(0)) + R(Tc[nlev - 2]) * fmax2(s, R(0));
+          s_tv[t * kMaxCellsPerBlock + lc] = -ldT(Tc, nlev - 3, a.off[t]) * fmin2(s, R(0)) + ldT(Tc, nlev - 2, a.off[t]) * fmax2(s, R(0));
         }
       } else if (i == 2) {
         for (int t = 0; t < NT; t++) {
           const TS *Tc = a.TAB[t] + (size_t)n * S;
-          s_tv[t * kMaxCellsPerBlock + lc] = R(0.5) * (R(Tc[0]) + R(Tc[1]));
+          s_tv[t * kMaxCellsPerBlock + lc] = R(0.5) * (ldT(Tc, 0, a.off[t]) + ldT(Tc, 1, a.off[t]));
         }
       } else {
         // lib/oce_adv_tra_ver.F90:545-553 with nz = i - 1
@@ -302,7 +307,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_col1(DMeshT<R> m, FusedArgs<R, 
         const R E = dzjp1 * (dzjp1 + dzjp2) / (dzj + R(2) * dzjp1);
         for (int t = 0; t < NT; t++) {
           const TS *Tc = a.TAB[t] + (size_t)n * S;
-          const R T0 = R(Tc[nzz - 1]), T1 = R(Tc[nzz]);
+          const R T0 = ldT(Tc, nzz - 1, a.off[t]), T1 = ldT(Tc, nzz, a.off[t]);
           const R dj = s_slope[t * kMaxCellsPerBlock + lc - 1];   // layer nzz
           const R djp1 = s_slope[t * kMaxCellsPerBlock + lc];     // layer nzz + 1
           s_tv[t * kMaxCellsPerBlock + lc] = T0 + A * (T1 - T0) + B * (C * (T1 - T0) - D * djp1 + E * dj);
@@ -325,7 +330,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_col1(DMeshT<R> m, FusedArgs<R, 
       if (LIM == LIM_FCT) {
         for (int t = 0; t < NT; t++) {
           Col<R, TS> cT;
-          cT.T = a.T[t] + col; cT.W = Wc; cT.A = Ac; cT.nlev = nlev;
+          cT.T = a.T[t] + col; cT.W = Wc; cT.A = Ac; cT.nlev = nlev; cT.off = a.off[t];
           lov[t] = ver_upw1(cT, i);
         }
       }
@@ -346,9 +351,9 @@ __global__ void __launch_bounds__(kThreads, 4) k_col1(DMeshT<R> m, FusedArgs<R, 
             const R x = (w > R(0)) ? fmin2(w * a.dt / dzj, R(1)) : fmin2(-(w * a.dt / dzj), R(1));
             const R two3 = R(2.0 / 3.0);
             for (int t = 0; t < NT; t++) {
-              const R Tc = R(a.TAB[t][col + jl - 1]);
+              const R Tc = ldT(a.TAB[t], col + jl - 1, a.off[t]);
               R aL = s_tv[t * kMaxCellsPerBlock + sl];
-              R aR = (jl + 1 == nlev) ? R(a.TAB[t][col + nlev - 2]) : s_tv[t * kMaxCellsPerBlock + sl + 1];
+              R aR = (jl + 1 == nlev) ? ldT(a.TAB[t], col + nlev - 2, a.off[t]) : s_tv[t * kMaxCellsPerBlock + sl + 1];
               if ((aR - Tc) * (Tc - aL) <= R(0)) { aL = Tc; aR = Tc; }
               if ((aR - aL) * (Tc - R(0.5) * (aL + aR)) > (aR - aL) * (aR - aL) / R(6)) aL = R(3) * Tc - R(2) * aR;
               if ((aR - aL) * (Tc - R(0.5) * (aR + aL)) < -((aR - aL) * (aR - aL) / R(6))) aR = R(3) * Tc - R(2) * aL;
@@ -363,7 +368,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_col1(DMeshT<R> m, FusedArgs<R, 
       } else {
         for (int t = 0; t < NT; t++) {
           Col<R, TS> cA;
-          cA.T = a.TAB[t] + col; cA.W = Wc; cA.A = Ac; cA.nlev = nlev;
+          cA.T = a.TAB[t] + col; cA.W = Wc; cA.A = Ac; cA.nlev = nlev; cA.off = a.off[t];
           if (VER == VER_QR4C) hov[t] = ver_qr4c(cA, m.zbar, m.Z, i, a.pv, lov[t]);
           else if (VER == VER_CDIFF) hov[t] = ver_cdiff(cA, i, lov[t]);
           else hov[t] = ver_upw1(cA, i) - lov[t];
@@ -389,7 +394,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_col1(DMeshT<R> m, FusedArgs<R, 
       const R fk = s_fv[t * kMaxCellsPerBlock + lc];
       const R fk1 = (k + 2 == nlev) ? R(0) : s_fv[t * kMaxCellsPerBlock + lc + 1];
       const R acc = s_acc[t * kMaxCellsPerBlock + lc];
-      const R num = R(a.T[t][o]) * h + div_rcp((acc + (fk - fk1)) * a.dt, asv, yasv);
+      const R num = ldT(a.T[t], o, a.off[t]) * h + div_rcp((acc + (fk - fk1)) * a.dt, asv, yasv);
       a.lo[t][o] = div_rcp(num, hn, yhn);
     }
   }
@@ -425,7 +430,7 @@ __global__ void __launch_bounds__(kThreads) k_col2(DMeshT<R> m, FusedArgs<R, TS>
         if (wet) {
           const size_t o0 = (size_t)e0 * S + k, o1 = (size_t)e1 * S + k, o2 = (size_t)e2 * S + k;
           const R l0 = a.lo[t][o0], l1 = a.lo[t][o1], l2 = a.lo[t][o2];
-          const R t0 = R(a.T[t][o0]), t1 = R(a.T[t][o1]), t2 = R(a.T[t][o2]);
+          const R t0 = ldT(a.T[t], o0, a.off[t]), t1 = ldT(a.T[t], o1, a.off[t]), t2 = ldT(a.T[t], o2, a.off[t]);
           amx = fmax3(fmax2(l0, t0), fmax2(l1, t1), fmax2(l2, t2));
           amn = fmin3(fmin2(l0, t0), fmin2(l1, t1), fmin2(l2, t2));
         } else {
@@ -538,7 +543,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_col3(DMeshT<R> m, FusedArgs<R, 
       const R *av = a.adf_v[t] + col;
       dv[t] = R(0);
       if (LIM == LIM_FCT) {
-        dv[t] = dv[t] - R(a.T[t][o]) * m.hnode[o] + a.lo[t][o] * hn;
+        dv[t] = dv[t] - ldT(a.T[t], o, a.off[t]) * m.hnode[o] + a.lo[t][o] * hn;
         const R fk = limit_v(av, a.rp[t] + col, a.rm[t] + col, nz, nlev);
         const R fk1 = limit_v(av, a.rp[t] + col, a.rm[t] + col, nz + 1, nlev);
         dv[t] = dv[t] + div_rcp((fk - fk1) * a.dt, asv, yasv);
@@ -571,7 +576,8 @@ __global__ void __launch_bounds__(kThreads, 4) k_col3(DMeshT<R> m, FusedArgs<R, 
     }
     for (int t = 0; t < NT; t++) {
       const R del = R(0) + dh[t] + dv[t];
-      a.T_out[t][o] = TS(R(a.T[t][o]) + div_rcp(del, hn, yhn));
+      const R tnew = ldT(a.T[t], o, a.off[t]) + div_rcp(del, hn, yhn);
+      a.T_out[t][o] = stT<R, TS>(tnew, a.off[t], a.sround != 0, a.sround ? mix32(a.seed[t] ^ mix32((uint32_t)o)) : 0u);
     }
   }
 }

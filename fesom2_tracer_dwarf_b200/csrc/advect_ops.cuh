@@ -10,6 +10,9 @@
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
+#include <cstdint>
+#include <type_traits>
+
 #include "dmesh.hpp"
 
 namespace fesom {
@@ -21,6 +24,73 @@ template <typename R> __device__ __forceinline__ R fmax3(R a, R b, R c) { return
 template <typename R> __device__ __forceinline__ R fmin3(R a, R b, R c) { return fmin2(fmin2(a, b), c); }
 __device__ __forceinline__ double sgn1(double w) { return copysign(1.0, w); }
 __device__ __forceinline__ float sgn1(float w) { return copysignf(1.0f, w); }
+
+// ---------------------------------------------------------------------------
+// tracer storage.  FP64 and FP32 storage hold the tracer T itself; 16-bit
+// storage holds the anomaly T - off on wet cells, with off a per-tracer FP32
+// constant near the field's mean, so that the storage ulp follows the
+// anomaly's magnitude.  Arithmetic is always in R.
+// ---------------------------------------------------------------------------
+template <typename R, typename TS>
+__device__ __forceinline__ R ldT(const TS *p, size_t i, R off) {
+  if constexpr (std::is_same<R, TS>::value) {
+    (void)off;
+    return p[i];
+  } else {
+    return R(p[i]) + off;
+  }
+}
+
+// 32-bit integer hash (Wellons' "lowbias32" finalizer, a published
+// xorshift-multiply mix); used as a counter-based random stream.
+__device__ __forceinline__ uint32_t mix32(uint32_t x) {
+  x ^= x >> 16;
+  x *= 0x7feb352du;
+  x ^= x >> 15;
+  x *= 0x846ca68bu;
+  x ^= x >> 16;
+  return x;
+}
+
+// Stochastic rounding of an FP32 value to BF16: add 16 random bits below the
+// kept mantissa and truncate, so the value rounds up with probability equal
+// to its distance from the lower neighbour over the spacing (Connolly, Higham
+// & Mary 2021).  Inf and NaN pass through unchanged.
+__device__ __forceinline__ __nv_bfloat16 bf16_sround(float x, uint32_t r) {
+  uint32_t u = __float_as_uint(x);
+  if ((u & 0x7f800000u) != 0x7f800000u) u += (r & 0xffffu);
+  return __ushort_as_bfloat16((unsigned short)(u >> 16));
+}
+
+// Stochastic rounding of an FP32 value to FP16: round toward zero, then step
+// one FP16 ulp away from zero with probability (remainder / spacing).
+__device__ __forceinline__ __half f16_sround(float x, uint32_t r) {
+  const __half lo = __float2half_rz(x);
+  const float flo = __half2float(lo);
+  const float rem = fabsf(x - flo);                 // exact: x - (x cut to 11 bits)
+  if (!(rem > 0.0f)) return (x == x) ? lo : __float2half_rn(x);
+  const __half hi = __ushort_as_half((unsigned short)(__half_as_ushort(lo) + 1));  // next magnitude
+  const float gap = fabsf(__half2float(hi) - flo);  // a power of two (or inf past the range)
+  const float u = (float)(r >> 8) * 0x1p-24f;       // [0, 1)
+  return (u * gap < rem) ? hi : lo;
+}
+
+// Store of a new tracer value: identity for FP64/FP32 storage; for 16-bit
+// storage the anomaly v - off rounded to nearest or stochastically with the
+// random word r.
+template <typename R, typename TS>
+__device__ __forceinline__ TS stT(R v, R off, bool sround, uint32_t r) {
+  if constexpr (std::is_same<R, TS>::value) {
+    (void)off; (void)sround; (void)r;
+    return v;
+  } else if constexpr (std::is_same<TS, __nv_bfloat16>::value) {
+    const float x = float(v - off);
+    return sround ? bf16_sround(x, r) : __float2bfloat16_rn(x);
+  } else {
+    const float x = float(v - off);
+    return sround ? f16_sround(x, r) : __float2half_rn(x);
+  }
+}
 
 enum HorScheme { HOR_UPW1 = 0, HOR_MUSCL = 1, HOR_MFCT = 2 };
 enum VerScheme { VER_UPW1 = 0, VER_PPM = 1, VER_QR4C = 2, VER_CDIFF = 3 };
@@ -89,22 +159,23 @@ struct Col {
   const R *HN;  // hnode_new column
   const R *H;   // hnode column
   int nlev;
+  R off;        // storage offset (16-bit storage only)
 };
 
 // adv_tra_ver_upw1 (lib/oce_adv_tra_ver.F90:300-327)
 template <typename R, typename TS>
 __device__ __forceinline__ R ver_upw1(const Col<R, TS> &c, int i) {
-  if (i == 1) return -(c.W[0] * R(c.T[0]) * c.A[0]);
+  if (i == 1) return -(c.W[0] * ldT(c.T, 0, c.off) * c.A[0]);
   if (i == c.nlev) return R(0);
   const R w = c.W[i - 1];
-  return -(R(0.5) * (R(c.T[i - 1]) * (w + fabs(w)) + R(c.T[i - 2]) * (w - fabs(w))) * c.A[i - 1]);
+  return -(R(0.5) * (ldT(c.T, i - 1, c.off) * (w + fabs(w)) + ldT(c.T, i - 2, c.off) * (w - fabs(w))) * c.A[i - 1]);
 }
 
 // QR4C (lib/oce_adv_tra_ver.F90:397-436): the reference's assignments replayed
 // in order for interface i, starting from the previous flux value v.
 template <typename R, typename TS>
 __device__ __forceinline__ R ver_qr4c(const Col<R, TS> &c, const R *zbar, const R *Z, int i, R num_ord, R v) {
-  auto T = [&](int q) { return R(c.T[q - 1]); };  // 1-based views
+  auto T = [&](int q) { return ldT(c.T, q - 1, c.off); };  // 1-based views
   const R *W = c.W - 1;
   const R *A = c.A - 1;
   const int nzmin = 1, nzmax = c.nlev;
@@ -131,8 +202,8 @@ __device__ __forceinline__ R ver_qr4c(const Col<R, TS> &c, const R *zbar, const 
 template <typename R, typename TS>
 __device__ __forceinline__ R ver_cdiff(const Col<R, TS> &c, int i, R v) {
   if (i == c.nlev) return v;
-  if (i == 1) return -(c.W[0] * R(c.T[0]) * c.A[0]) - v;
-  const R tv = R(0.5) * (R(c.T[i - 2]) + R(c.T[i - 1]));
+  if (i == 1) return -(c.W[0] * ldT(c.T, 0, c.off) * c.A[0]) - v;
+  const R tv = R(0.5) * (ldT(c.T, i - 2, c.off) + ldT(c.T, i - 1, c.off));
   return -(tv * c.W[i - 1] * c.A[i - 1]) - v;
 }
 

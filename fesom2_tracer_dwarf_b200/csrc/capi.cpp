@@ -33,6 +33,7 @@ struct State {
   std::vector<double> pend_uv, pend_w;  // uv in (2, nl-1, elem2D)
   bool pend_vel = false;
   Precision prec = Precision::FP64;
+  int sround = 0;  // rounding of 16-bit stores (tracer_set_rounding)
 };
 State g;
 
@@ -58,6 +59,7 @@ void ensure_engine() {
   if (g.eng) return;
   if (!g.mesh) throw std::runtime_error("no mesh connectivity: use tracer_init_analytic or tracer_set_mesh_arrays");
   g.eng.reset(new Engine(*g.mesh, g.prec));
+  g.eng->set_rounding(g.sround);
   if (g.ntr > 0) {
     g.eng->allocate_tracers(g.ntr);
     for (int i = 0; i < g.ntr; i++) {
@@ -394,6 +396,24 @@ int tracer_set_precision(int mode) {
   }
   g.prec = p;
   return 0;
+}
+
+int tracer_set_rounding(int mode) {
+  if (mode < 0 || mode > 1) return fail("rounding mode must be 0 (nearest) or 1 (stochastic)");
+  g.sround = mode;
+  if (g.eng) g.eng->set_rounding(mode);
+  return 0;
+}
+
+int tracer_storage_offset(int tracer_id, double *off) {
+  return guarded([&] {
+    if (check_ready()) return -1;
+    if (tracer_id < 1 || tracer_id > g.ntr) return fail("invalid tracer_id " + std::to_string(tracer_id));
+    if (!off) return fail("null output");
+    ensure_engine();
+    *off = g.eng->storage_offset(tracer_id - 1);
+    return 0;
+  });
 }
 
 int tracer_volume_sum(int tracer_id, double *out2) {

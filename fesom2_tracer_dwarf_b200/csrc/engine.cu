@@ -4,6 +4,7 @@
 #include <cuda_fp16.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <stdexcept>
 #include <string>
@@ -234,21 +235,61 @@ static void check_id(const EngineImpl &P, int id) {
   if (id < 0 || id >= (int)P.tr.size()) throw std::out_of_range("invalid tracer id " + std::to_string(id + 1));
 }
 
-// host (ld, N) doubles -> device storage columns
-static void put_tracer(EngineImpl &P, void *d, const double *v) {
+static bool storage16(const EngineImpl &P) { return P.prec == Precision::BF16 || P.prec == Precision::FP16; }
+
+// 16-bit storage offset for a field: its mean over wet cells, rounded to
+// FP32 (the kernels add it in FP32); 0 for FP64 and FP32 storage
+static double storage_offset_for(const EngineImpl &P, const double *v) {
+  if (!storage16(P)) return 0.0;
+  const int L = P.mesh.nl - 1, N = P.mesh.nod2D;
+  double s = 0.0;
+  long long c = 0;
+  for (int n = 0; n < N; n++)
+    for (int k = 0; k < P.mesh.nlev_node[n] - 1; k++) { s += v[(size_t)n * L + k]; c++; }
+  const double off = c ? (double)(float)(s / (double)c) : 0.0;
+  return std::isfinite(off) ? off : 0.0;
+}
+
+// host (ld, N) doubles -> device storage columns (wet cells minus off)
+static void put_tracer(EngineImpl &P, void *d, const double *v, double off) {
   const int L = P.mesh.nl - 1, N = P.mesh.nod2D;
   std::vector<double> st((size_t)N * P.S, 0.0);
   for (int n = 0; n < N; n++) std::memcpy(&st[(size_t)n * P.S], v + (size_t)n * L, sizeof(double) * L);
+  if (off != 0.0)
+    for (int n = 0; n < N; n++)
+      for (int k = 0; k < P.mesh.nlev_node[n] - 1; k++) st[(size_t)n * P.S + k] -= off;
   std::vector<unsigned char> buf(st.size() * P.ts_bytes);
   to_storage(P.prec, st.data(), buf.data(), st.size());
   P.h2d(d, buf.data(), buf.size());
+}
+
+// device storage columns -> host (ld, N) doubles (wet cells plus off)
+static void get_tracer(EngineImpl &P, const void *d, double off, double *out) {
+  const int L = P.mesh.nl - 1, N = P.mesh.nod2D;
+  std::vector<unsigned char> buf((size_t)N * P.S * P.ts_bytes);
+  P.d2h(buf.data(), d, buf.size());
+  std::vector<double> st((size_t)N * P.S);
+  from_storage(P.prec, buf.data(), st.data(), st.size());
+  if (off != 0.0)
+    for (int n = 0; n < N; n++)
+      for (int k = 0; k < P.mesh.nlev_node[n] - 1; k++) st[(size_t)n * P.S + k] += off;
+  for (int n = 0; n < N; n++) std::memcpy(out + (size_t)n * L, &st[(size_t)n * P.S], sizeof(double) * L);
 }
 
 void Engine::set_values(int id, const double *v, bool also_ab) {
   EngineImpl &P = *p_;
   check_id(P, id);
   CK(cudaStreamSynchronize(P.stream));
-  put_tracer(P, P.tr[id].T, v);
+  auto &tr = P.tr[id];
+  const double off = storage_offset_for(P, v);
+  if (!also_ab && off != tr.off) {
+    // valuesAB stays: re-encode it under the new offset
+    std::vector<double> ab((size_t)(P.mesh.nl - 1) * P.mesh.nod2D);
+    get_tracer(P, tr.TAB, tr.off, ab.data());
+    put_tracer(P, tr.TAB, ab.data(), off);
+  }
+  tr.off = off;
+  put_tracer(P, tr.T, v, off);
   const size_t n = (size_t)P.mesh.nod2D * P.S * P.ts_bytes;
   P.d2d(P.tr[id].Tout, P.tr[id].T, n);
   if (also_ab) P.d2d(P.tr[id].TAB, P.tr[id].T, n);
@@ -258,18 +299,33 @@ void Engine::set_values_ab(int id, const double *v) {
   EngineImpl &P = *p_;
   check_id(P, id);
   CK(cudaStreamSynchronize(P.stream));
-  put_tracer(P, P.tr[id].TAB, v);
+  put_tracer(P, P.tr[id].TAB, v, P.tr[id].off);
 }
 
 void Engine::get_values(int id, double *out) const {
   EngineImpl &P = *p_;
   check_id(P, id);
-  const int L = P.mesh.nl - 1, N = P.mesh.nod2D;
-  std::vector<unsigned char> buf((size_t)N * P.S * P.ts_bytes);
-  P.d2h(buf.data(), P.tr[id].T, buf.size());
-  std::vector<double> st((size_t)N * P.S);
-  from_storage(P.prec, buf.data(), st.data(), st.size());
-  for (int n = 0; n < N; n++) std::memcpy(out + (size_t)n * L, &st[(size_t)n * P.S], sizeof(double) * L);
+  get_tracer(P, P.tr[id].T, P.tr[id].off, out);
+}
+
+void Engine::set_rounding(int mode) {
+  if (mode < 0 || mode > 1) throw std::invalid_argument("rounding mode must be 0 (nearest) or 1 (stochastic)");
+  p_->sround = mode;
+}
+int Engine::rounding() const { return p_->sround; }
+double Engine::storage_offset(int id) const {
+  check_id(*p_, id);
+  return p_->tr[id].off;
+}
+
+// host copy of the kernels' mix32 (lowbias32)
+static uint32_t mix32_host(uint32_t x) {
+  x ^= x >> 16;
+  x *= 0x7feb352du;
+  x ^= x >> 15;
+  x *= 0x846ca68bu;
+  x ^= x >> 16;
+  return x;
 }
 
 void Engine::set_scheme(int id, const TracerScheme &s) {
@@ -320,7 +376,11 @@ static void run_batch(EngineImpl &P, int first, int nt, double dt, bool refresh_
     b.lo[t] = P.lo[t];
     b.rp[t] = P.rp[t];
     b.rm[t] = P.rm[t];
+    b.off[t] = tr.off;
+    b.seed[t] = mix32_host(P.sround_seed ^ mix32_host((uint32_t)(first + t) * 0x9e3779b9u + tr.nstep));
+    tr.nstep++;
   }
+  b.sround = storage16(P) ? P.sround : 0;
   b.vflux = P.vflux;
   dispatch(P, P.tr[first].sch, nt, b, dt);
   for (int t = 0; t < nt; t++) std::swap(P.tr[first + t].T, P.tr[first + t].Tout);
@@ -424,7 +484,7 @@ void Engine::volume_sum(int id, double out[2]) const {
   check_id(P, id);
   CK(cudaStreamSynchronize(P.stream));
   if (P.prec == Precision::FP64) volume_sum_f64(P, P.tr[id].T, out);
-  else volume_sum_f32(P, P.tr[id].T, out);
+  else volume_sum_f32(P, P.tr[id].T, P.tr[id].off, out);
 }
 
 void Engine::stats(int id, double out[4]) const {

@@ -36,6 +36,12 @@ class Engine {
   // Compensated FP64 sums over the wet cells of tracer id: out[0] = Sum T,
   // out[1] = Sum T * areasvol * hnode_new (the conserved tracer content).
   void volume_sum(int id, double out[2]) const;
+  // 16-bit storage: 0 rounds new values to nearest, 1 rounds them
+  // stochastically (a reproducible per-step, per-tracer, per-cell stream)
+  void set_rounding(int mode);
+  int rounding() const;
+  // offset subtracted from a tracer's wet cells in 16-bit storage (0 otherwise)
+  double storage_offset(int id) const;
   ~Engine();
   Engine(const Engine &) = delete;
   Engine &operator=(const Engine &) = delete;

@@ -33,6 +33,9 @@ struct BatchPtrs {
   void *rp[kBatchMax] = {};
   void *rm[kBatchMax] = {};
   void *vflux = nullptr;
+  double off[kBatchMax] = {};     // storage offsets (16-bit storage)
+  uint32_t seed[kBatchMax] = {};  // stochastic-rounding streams
+  int sround = 0;
 };
 
 struct EngineImpl {
@@ -50,7 +53,11 @@ struct EngineImpl {
   struct Tracer {
     void *T = nullptr, *Tout = nullptr, *TAB = nullptr;
     TracerScheme sch;
+    double off = 0.0;    // 16-bit storage holds T - off on wet cells
+    uint32_t nstep = 0;  // steps taken (stochastic-rounding stream)
   };
+  int sround = 0;        // 1: stochastic rounding of 16-bit stores
+  uint32_t sround_seed = 0x2545f491u;
   std::vector<Tracer> tr;
   int slots = 0;
   void *vflux = nullptr;
@@ -129,6 +136,6 @@ void launch_batch_f32(EngineImpl &P, const TracerScheme &sc, int nt, const Batch
 // Compensated FP64 sums of T and of T * areasvol * hnode_new over the wet
 // cells of one tracer.
 void volume_sum_f64(EngineImpl &P, const void *T, double out[2]);
-void volume_sum_f32(EngineImpl &P, const void *T, double out[2]);
+void volume_sum_f32(EngineImpl &P, const void *T, double off, double out[2]);
 
 }  // namespace fesom

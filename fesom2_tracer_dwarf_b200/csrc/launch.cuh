@@ -94,6 +94,11 @@ void launch_batch_t(EngineImpl &P, const TracerScheme &sc, int nt, const BatchPt
   a.dt = (R)dt;
   a.ph = (R)sc.ph;
   a.pv = (R)sc.pv;
+  for (int t = 0; t < nt; t++) {
+    a.off[t] = (R)b.off[t];
+    a.seed[t] = b.seed[t];
+  }
+  a.sround = b.sround;
   const bool fct = sc.lim == 1;
   if (nt == 4) fct ? run_group<R, TS, 4, LIM_FCT>(P, sc, a) : run_group<R, TS, 4, LIM_NONE>(P, sc, a);
   else if (nt == 2) fct ? run_group<R, TS, 2, LIM_FCT>(P, sc, a) : run_group<R, TS, 2, LIM_NONE>(P, sc, a);
@@ -110,14 +115,14 @@ __device__ __forceinline__ void two_sum(double a, double b, double &s, double &e
 }
 
 template <typename R, typename TS>
-__global__ void __launch_bounds__(256) k_volume_sum(DMeshT<R> m, const TS *T, double *out) {
+__global__ void __launch_bounds__(256) k_volume_sum(DMeshT<R> m, const TS *T, double off, double *out) {
   // per thread: Neumaier-compensated partial sums of T and T*areasvol*hnode_new
   double s0 = 0, c0 = 0, s1 = 0, c1 = 0;
   for (int n = blockIdx.x * blockDim.y + threadIdx.y; n < m.N; n += gridDim.x * blockDim.y) {
     const int L = m.nlev_node[n] - 1;
     for (int k = threadIdx.x; k < L; k += blockDim.x) {
       const size_t o = (size_t)n * m.S + k;
-      const double t = (double)R(T[o]);
+      const double t = std::is_same<R, TS>::value ? (double)R(T[o]) : (double)R(T[o]) + off;
       const double v = t * (double)m.areasvol[o] * (double)m.hnode_new[o];
       double s, e;
       two_sum(s0, t, s, e); s0 = s; c0 += e;
@@ -147,10 +152,10 @@ __global__ void __launch_bounds__(256) k_volume_sum(DMeshT<R> m, const TS *T, do
 }
 
 template <typename R, typename TS>
-void volume_sum_t(EngineImpl &P, const void *T, double res[2]) {
+void volume_sum_t(EngineImpl &P, const void *T, double off, double res[2]) {
   const int blocks = 296;
   double *d = P.dalloc<double>(4 * blocks);
-  k_volume_sum<R, TS><<<blocks, dim3(32, 8), 0, P.stream>>>(dmesh<R>(P), (const TS *)T, d);
+  k_volume_sum<R, TS><<<blocks, dim3(32, 8), 0, P.stream>>>(dmesh<R>(P), (const TS *)T, off, d);
   CK(cudaGetLastError());
   std::vector<double> h(4 * blocks);
   P.d2h(h.data(), d, h.size() * sizeof(double));

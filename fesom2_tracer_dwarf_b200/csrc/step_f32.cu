@@ -13,11 +13,11 @@ void launch_batch_f32(EngineImpl &P, const TracerScheme &sc, int nt, const Batch
   }
 }
 
-void volume_sum_f32(EngineImpl &P, const void *T, double out[2]) {
+void volume_sum_f32(EngineImpl &P, const void *T, double off, double out[2]) {
   switch (P.prec) {
-    case Precision::BF16: volume_sum_t<float, __nv_bfloat16>(P, T, out); break;
-    case Precision::FP16: volume_sum_t<float, __half>(P, T, out); break;
-    default: volume_sum_t<float, float>(P, T, out); break;
+    case Precision::BF16: volume_sum_t<float, __nv_bfloat16>(P, T, off, out); break;
+    case Precision::FP16: volume_sum_t<float, __half>(P, T, off, out); break;
+    default: volume_sum_t<float, float>(P, T, off, out); break;
   }
 }
 

@@ -1,5 +1,6 @@
 """Precision study: FP32, BF16-storage and FP16-storage runs of the tracer
-step against the FP64 path on identical seeded inputs.
+step (16-bit stores rounded to nearest or stochastically) against the FP64
+path on identical seeded inputs.
 
 The FP64 path is bit-identical to the CPU oracle (tests/test_gpu_parity.py
 checks it at every size up to 1000x1000x64), so it serves as the FP64
@@ -22,9 +23,13 @@ from .workloads import layered_flow_case
 
 
 def run_mode(api, c, mode, steps, hor="MUSCL", ver="PPM", lim="FCT"):
-    """Advance both tracers of case c (mesh already in api) steps steps in one precision mode."""
+    """Advance both tracers of case c (mesh already in api) steps steps in one
+    mode: 'fp64', 'fp32', 'bf16', 'fp16', or a 16-bit mode with '+sr'
+    (stochastic rounding of the stores)."""
     T, S, uv, w, dt, wet = c.T, c.S, c.uv, c.w, c.dt, c.wet
-    api.set_precision(mode)
+    prec, _, sr = mode.partition("+")
+    api.set_precision(prec)
+    api.set_rounding("stochastic" if sr == "sr" else "nearest")
     api.allocate_tracers(2)
     api.set_values(1, T)
     api.set_values(2, S)
@@ -36,8 +41,10 @@ def run_mode(api, c, mode, steps, hor="MUSCL", ver="PPM", lim="FCT"):
     ms = api.time_steps(steps, dt)
     v1 = [api.volume_sum(t)[1] for t in (1, 2)]
     out = [api.get_tracer_values(t) for t in (1, 2)]
+    offsets = [api.storage_offset(t) for t in (1, 2)]
+    api.set_rounding("nearest")
     return {"fields": out, "wet": wet, "v0": v0, "v1": v1, "ms_per_step": ms / steps, "cells": c.wet_cells,
-            "dt": dt}
+            "dt": dt, "offsets": offsets}
 
 
 def compare(ref, res):
@@ -55,7 +62,7 @@ def compare(ref, res):
     return rows
 
 
-def study(nx, nl, steps, modes=("fp32", "bf16", "fp16"), seed=0):
+def study(nx, nl, steps, modes=("fp32", "bf16", "bf16+sr", "fp16", "fp16+sr"), seed=0):
     api = FESOMTracerAdvection()
     api.cleanup()
     c = layered_flow_case(api, nx, nl, seed=seed)
@@ -65,7 +72,7 @@ def study(nx, nl, steps, modes=("fp32", "bf16", "fp16"), seed=0):
            "fp64_ms_per_step": ref["ms_per_step"], "modes": {}}
     for m in modes:
         res = run_mode(api, c, m, steps)
-        out["modes"][m] = {"ms_per_step": res["ms_per_step"],
+        out["modes"][m] = {"ms_per_step": res["ms_per_step"], "storage_offsets": res["offsets"],
                            "cell_updates_per_s": 2 * res["cells"] / (res["ms_per_step"] / 1e3),
                            "errors": compare(ref, res)}
     out["fp64_cell_updates_per_s"] = 2 * ref["cells"] / (ref["ms_per_step"] / 1e3)

@@ -121,6 +121,18 @@ class FESOMTracerAdvection:
         """'fp64' (bit-exact), 'fp32', 'bf16' or 'fp16' (16-bit tracer storage, FP32 arithmetic)."""
         _lib.check(self.lib, self.lib.tracer_set_precision(self.PRECISIONS[mode]), "tracer_set_precision")
 
+    ROUNDING = {"nearest": 0, "stochastic": 1}
+
+    def set_rounding(self, mode):
+        """Rounding of new values into 16-bit storage: 'nearest' or 'stochastic'."""
+        _lib.check(self.lib, self.lib.tracer_set_rounding(self.ROUNDING[mode]), "tracer_set_rounding")
+
+    def storage_offset(self, tracer_id=1):
+        """Offset subtracted from the tracer's wet cells in 16-bit storage (0 otherwise)."""
+        out = np.zeros(1)
+        _lib.check(self.lib, self.lib.tracer_storage_offset(tracer_id, _lib.ptr(out)), "tracer_storage_offset")
+        return float(out[0])
+
     def volume_sum(self, tracer_id=1):
         """(Sum T, Sum T*areasvol*hnode_new) over wet cells, compensated FP64 on the device."""
         out = np.zeros(2)

@@ -132,6 +132,15 @@ int tracer_set_ab_refresh(int on);
  * denominators are formed in FP64.  Changing it rebuilds the device state and
  * keeps the tracer values. */
 int tracer_set_precision(int mode);
+/* Rounding of new tracer values into 16-bit storage (modes 2, 3):
+ * 0 = to nearest (default), 1 = stochastic (round up with probability equal
+ * to the distance from the lower neighbour over the spacing; a reproducible
+ * counter-based stream per tracer, step and cell).  16-bit storage holds
+ * T - off on wet cells, off = the FP32-rounded wet-cell mean of the tracer's
+ * latest full upload (tracer_set_values); tracer_storage_offset returns it
+ * (0 in modes 0, 1). */
+int tracer_set_rounding(int mode);
+int tracer_storage_offset(int tracer_id, double *off);
 /* Compensated FP64 sums over the wet cells of one tracer, on the device:
  * out2[0] = Sum T, out2[1] = Sum T*areasvol*hnode_new (conserved content). */
 int tracer_volume_sum(int tracer_id, double *out2);
@@ -184,6 +193,11 @@ long long tracer_device_bytes(void);
  * *mismatches = number of differing results, example4 = (a, b, got,
  * expected) of the first one. */
 int tracer_selftest_division(long long n, uint64_t seed, long long *mismatches, double *example4);
+/* Checks on the GPU the stochastic rounding of 16-bit stores (fmt 0 BF16,
+ * 1 FP16) on n random inputs with `draws` roundings each: *outside = results
+ * that are not one of the input's two storage neighbours; *z = standardized
+ * total of (rounded-up count - expected count), ~N(0, 1) when unbiased. */
+int tracer_selftest_sround(int fmt, long long n, int draws, uint32_t seed, long long *outside, double *z);
 /* No counterpart in the reference.  One step of tracer tracer_id (its scheme,
  * the loaded mesh and flow) on caller-owned DEVICE buffers, allocating no
  * device memory: for callers whose runtime has reserved the GPU's memory for
