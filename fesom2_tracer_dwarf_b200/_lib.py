@@ -56,6 +56,8 @@ SIGNATURES = {
     "tracer_set_ab_refresh": (ctypes.c_int, [ctypes.c_int]),
     "tracer_set_precision": (ctypes.c_int, [ctypes.c_int]),
     "tracer_set_rounding": (ctypes.c_int, [ctypes.c_int]),
+    "tracer_host_register": (ctypes.c_int, [_vp, ctypes.c_longlong]),
+    "tracer_host_unregister": (ctypes.c_int, [_vp]),
     "tracer_storage_offset": (ctypes.c_int, [ctypes.c_int, _vp]),
     "tracer_volume_sum": (ctypes.c_int, [ctypes.c_int, _vp]),
     "tracer_advect_steps": (ctypes.c_int, [ctypes.c_int, ctypes.c_double]),

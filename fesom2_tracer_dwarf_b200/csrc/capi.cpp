@@ -197,7 +197,10 @@ int tracer_allocate_tracers(int num_tracers, int nl, int nod2D, int AB_order) {
     g.pend_ab.assign(num_tracers, std::vector<double>());
     if (g.eng) {
       g.eng->allocate_tracers(num_tracers);
-      for (int i = 0; i < num_tracers; i++) g.eng->set_values(i, g.pend_values[i].data(), true);
+      for (int i = 0; i < num_tracers; i++) {
+        g.eng->set_values(i, g.pend_values[i].data(), true);
+        std::vector<double>().swap(g.pend_values[i]);
+      }
     }
     return 0;
   });
@@ -209,9 +212,14 @@ int tracer_set_values(int tracer_id, const double *values, int nl, int nod2D) {
       return fail("invalid tracer_id " + std::to_string(tracer_id) + ", num_tracers=" + std::to_string(g.ntr));
     if (!values) return fail("null values");
     if (nl != g.nl || nod2D != g.nod2D) return fail("tracer_set_values: dimensions do not match");
-    g.pend_values[tracer_id - 1].assign(values, values + (size_t)(nl - 1) * nod2D);
     g.pend_ab[tracer_id - 1].clear();
-    if (g.eng) g.eng->set_values(tracer_id - 1, values, true);
+    if (g.eng) {
+      // the engine holds the values; host copies are only kept until it exists
+      std::vector<double>().swap(g.pend_values[tracer_id - 1]);
+      g.eng->set_values(tracer_id - 1, values, true);
+    } else {
+      g.pend_values[tracer_id - 1].assign(values, values + (size_t)(nl - 1) * nod2D);
+    }
     return 0;
   });
 }
@@ -221,8 +229,12 @@ int tracer_set_values_ab(int tracer_id, const double *values, int nl, int nod2D)
     if (tracer_id < 1 || tracer_id > g.ntr) return fail("invalid tracer_id " + std::to_string(tracer_id));
     if (!values) return fail("null values");
     if (nl != g.nl || nod2D != g.nod2D) return fail("tracer_set_values_ab: dimensions do not match");
-    g.pend_ab[tracer_id - 1].assign(values, values + (size_t)(nl - 1) * nod2D);
-    if (g.eng) g.eng->set_values_ab(tracer_id - 1, values);
+    if (g.eng) {
+      std::vector<double>().swap(g.pend_ab[tracer_id - 1]);
+      g.eng->set_values_ab(tracer_id - 1, values);
+    } else {
+      g.pend_ab[tracer_id - 1].assign(values, values + (size_t)(nl - 1) * nod2D);
+    }
     return 0;
   });
 }
@@ -398,6 +410,17 @@ int tracer_set_precision(int mode) {
   return 0;
 }
 
+int tracer_host_register(void *ptr, long long bytes) {
+  if (!ptr || bytes <= 0) return fail("tracer_host_register: null pointer or empty range");
+  if (host_register(ptr, (size_t)bytes) != 0) return fail("tracer_host_register: cudaHostRegister failed");
+  return 0;
+}
+
+int tracer_host_unregister(void *ptr) {
+  if (host_unregister(ptr) != 0) return fail("tracer_host_unregister: range was not registered");
+  return 0;
+}
+
 int tracer_set_rounding(int mode) {
   if (mode < 0 || mode > 1) return fail("rounding mode must be 0 (nearest) or 1 (stochastic)");
   g.sround = mode;
@@ -453,6 +476,7 @@ int tracer_get_values_id(int tracer_id, double *values, int nz, int nn) {
     if (!values) return fail("null values");
     if (nz != g.nl - 1 || nn != g.nod2D) return fail("tracer_get_values: expected (" + std::to_string(g.nl - 1) + ", " + std::to_string(g.nod2D) + ")");
     if (g.eng) g.eng->get_values(tracer_id - 1, values);
+    else if (g.pend_values[tracer_id - 1].empty()) std::memset(values, 0, sizeof(double) * (size_t)nz * nn);
     else std::memcpy(values, g.pend_values[tracer_id - 1].data(), sizeof(double) * (size_t)nz * nn);
     return 0;
   });
@@ -468,7 +492,7 @@ int tracer_get_stats_id(int tracer_id, double *s4) {
       g.eng->stats(tracer_id - 1, s4);
     } else {
       const std::vector<double> &v = g.pend_values[tracer_id - 1];
-      double mn = v[0], mx = v[0], sm = 0.0, nan = 0.0;
+      double mn = v.empty() ? 0.0 : v[0], mx = mn, sm = 0.0, nan = 0.0;
       for (double x : v) { mn = x < mn ? x : mn; mx = x > mx ? x : mx; sm += x; nan += (x != x); }
       s4[0] = mn; s4[1] = mx; s4[2] = sm; s4[3] = nan;
     }

@@ -44,24 +44,6 @@ void build_sched(const std::vector<int> &counts, std::vector<int> &off, std::vec
       throw std::runtime_error("schedule block exceeds the per-block cell capacity");
 }
 
-// host conversions between double and the tracer storage type
-void to_storage(Precision p, const double *src, void *dst, size_t n) {
-  switch (p) {
-    case Precision::FP64: std::memcpy(dst, src, n * sizeof(double)); break;
-    case Precision::FP32: for (size_t i = 0; i < n; i++) ((float *)dst)[i] = (float)src[i]; break;
-    case Precision::BF16: for (size_t i = 0; i < n; i++) ((__nv_bfloat16 *)dst)[i] = __float2bfloat16((float)src[i]); break;
-    case Precision::FP16: for (size_t i = 0; i < n; i++) ((__half *)dst)[i] = __float2half((float)src[i]); break;
-  }
-}
-void from_storage(Precision p, const void *src, double *dst, size_t n) {
-  switch (p) {
-    case Precision::FP64: std::memcpy(dst, src, n * sizeof(double)); break;
-    case Precision::FP32: for (size_t i = 0; i < n; i++) dst[i] = ((const float *)src)[i]; break;
-    case Precision::BF16: for (size_t i = 0; i < n; i++) dst[i] = __bfloat162float(((const __nv_bfloat16 *)src)[i]); break;
-    case Precision::FP16: for (size_t i = 0; i < n; i++) dst[i] = __half2float(((const __half *)src)[i]); break;
-  }
-}
-
 // (ld, ncol) column-major host doubles -> device columns of stride S, type R
 template <typename R>
 R *upload_cols(EngineImpl &P, const double *h, int ld, int ncol, int nvalid) {
@@ -176,6 +158,7 @@ Engine::Engine(const MeshHost &mesh, Precision prec) : p_(new EngineImpl) {
 Engine::~Engine() {
   if (!p_) return;
   cudaStreamSynchronize(p_->stream);
+  release_ring(*p_);
   for (void *a : p_->allocs) cudaFree(a);
   cudaStreamDestroy(p_->stream);
   delete p_;
@@ -237,75 +220,39 @@ static void check_id(const EngineImpl &P, int id) {
 
 static bool storage16(const EngineImpl &P) { return P.prec == Precision::BF16 || P.prec == Precision::FP16; }
 
-// 16-bit storage offset for a field: its mean over wet cells, rounded to
-// FP32 (the kernels add it in FP32); 0 for FP64 and FP32 storage
-static double storage_offset_for(const EngineImpl &P, const double *v) {
-  if (!storage16(P)) return 0.0;
-  const int L = P.mesh.nl - 1, N = P.mesh.nod2D;
-  double s = 0.0;
-  long long c = 0;
-  for (int n = 0; n < N; n++)
-    for (int k = 0; k < P.mesh.nlev_node[n] - 1; k++) { s += v[(size_t)n * L + k]; c++; }
-  const double off = c ? (double)(float)(s / (double)c) : 0.0;
-  return std::isfinite(off) ? off : 0.0;
-}
-
-// host (ld, N) doubles -> device storage columns (wet cells minus off)
-static void put_tracer(EngineImpl &P, void *d, const double *v, double off) {
-  const int L = P.mesh.nl - 1, N = P.mesh.nod2D;
-  std::vector<double> st((size_t)N * P.S, 0.0);
-  for (int n = 0; n < N; n++) std::memcpy(&st[(size_t)n * P.S], v + (size_t)n * L, sizeof(double) * L);
-  if (off != 0.0)
-    for (int n = 0; n < N; n++)
-      for (int k = 0; k < P.mesh.nlev_node[n] - 1; k++) st[(size_t)n * P.S + k] -= off;
-  std::vector<unsigned char> buf(st.size() * P.ts_bytes);
-  to_storage(P.prec, st.data(), buf.data(), st.size());
-  P.h2d(d, buf.data(), buf.size());
-}
-
-// device storage columns -> host (ld, N) doubles (wet cells plus off)
-static void get_tracer(EngineImpl &P, const void *d, double off, double *out) {
-  const int L = P.mesh.nl - 1, N = P.mesh.nod2D;
-  std::vector<unsigned char> buf((size_t)N * P.S * P.ts_bytes);
-  P.d2h(buf.data(), d, buf.size());
-  std::vector<double> st((size_t)N * P.S);
-  from_storage(P.prec, buf.data(), st.data(), st.size());
-  if (off != 0.0)
-    for (int n = 0; n < N; n++)
-      for (int k = 0; k < P.mesh.nlev_node[n] - 1; k++) st[(size_t)n * P.S + k] += off;
-  for (int n = 0; n < N; n++) std::memcpy(out + (size_t)n * L, &st[(size_t)n * P.S], sizeof(double) * L);
-}
-
 void Engine::set_values(int id, const double *v, bool also_ab) {
   EngineImpl &P = *p_;
   check_id(P, id);
   CK(cudaStreamSynchronize(P.stream));
   auto &tr = P.tr[id];
-  const double off = storage_offset_for(P, v);
-  if (!also_ab && off != tr.off) {
-    // valuesAB stays: re-encode it under the new offset
-    std::vector<double> ab((size_t)(P.mesh.nl - 1) * P.mesh.nod2D);
-    get_tracer(P, tr.TAB, tr.off, ab.data());
-    put_tracer(P, tr.TAB, ab.data(), off);
+  stage_upload(P, v);
+  // 16-bit storage offset: the wet-cell mean of this upload, rounded to FP32
+  double off = 0.0;
+  if (storage16(P)) {
+    off = (double)(float)stage_wet_mean(P);
+    if (!std::isfinite(off)) off = 0.0;
   }
+  if (!also_ab && off != tr.off) storage_reoffset(P, tr.TAB, tr.off, off);  // valuesAB stays
   tr.off = off;
-  put_tracer(P, tr.T, v, off);
-  const size_t n = (size_t)P.mesh.nod2D * P.S * P.ts_bytes;
-  P.d2d(P.tr[id].Tout, P.tr[id].T, n);
-  if (also_ab) P.d2d(P.tr[id].TAB, P.tr[id].T, n);
+  stage_pack(P, off, tr.T, also_ab ? tr.TAB : nullptr, tr.Tout);
+  CK(cudaStreamSynchronize(P.stream));
 }
 
 void Engine::set_values_ab(int id, const double *v) {
   EngineImpl &P = *p_;
   check_id(P, id);
   CK(cudaStreamSynchronize(P.stream));
-  put_tracer(P, P.tr[id].TAB, v, P.tr[id].off);
+  stage_upload(P, v);
+  stage_pack(P, P.tr[id].off, P.tr[id].TAB, nullptr, nullptr);
+  CK(cudaStreamSynchronize(P.stream));
 }
 
 void Engine::get_values(int id, double *out) const {
   EngineImpl &P = *p_;
   check_id(P, id);
-  get_tracer(P, P.tr[id].T, P.tr[id].off, out);
+  CK(cudaStreamSynchronize(P.stream));
+  stage_unpack(P, P.tr[id].T, P.tr[id].off);
+  stage_download(P, out);
 }
 
 void Engine::set_rounding(int mode) {

@@ -29,6 +29,11 @@ enum class Precision { FP64 = 0, FP32 = 1, BF16 = 2, FP16 = 3 };
 
 struct EngineImpl;
 
+// Page-lock a host range for single-DMA tracer transfers (transfer.cu);
+// 0 on success.
+int host_register(void *p, size_t bytes);
+int host_unregister(void *p);
+
 class Engine {
  public:
   explicit Engine(const MeshHost &mesh, Precision prec = Precision::FP64);

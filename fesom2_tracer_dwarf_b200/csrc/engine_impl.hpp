@@ -58,6 +58,12 @@ struct EngineImpl {
   };
   int sround = 0;        // 1: stochastic rounding of 16-bit stores
   uint32_t sround_seed = 0x2545f491u;
+  // transfers (transfer.cu): device staging of one tracer in the user's
+  // (nl-1, nod2D) FP64 layout, and a ring of pinned host slots
+  static constexpr int kRing = 4;
+  double *stage_d = nullptr;
+  void *ring[kRing] = {};
+  cudaEvent_t ring_ev[kRing] = {};
   std::vector<Tracer> tr;
   int slots = 0;
   void *vflux = nullptr;
@@ -137,5 +143,18 @@ void launch_batch_f32(EngineImpl &P, const TracerScheme &sc, int nt, const Batch
 // cells of one tracer.
 void volume_sum_f64(EngineImpl &P, const void *T, double out[2]);
 void volume_sum_f32(EngineImpl &P, const void *T, double off, double out[2]);
+
+// Transfers of one tracer field (transfer.cu).  stage_upload / stage_download
+// move a host (nl-1, nod2D) FP64 array to / from the device staging array
+// (one DMA for ranges registered with host_register, a pinned ring
+// otherwise); stage_pack converts the staging array into up to three storage
+// arrays (wet cells minus off), stage_unpack the reverse (plus off).
+void stage_upload(EngineImpl &P, const double *host);
+void stage_download(EngineImpl &P, double *host);
+double stage_wet_mean(EngineImpl &P);
+void stage_pack(EngineImpl &P, double off, void *d0, void *d1, void *d2);
+void stage_unpack(EngineImpl &P, const void *s, double off);
+void storage_reoffset(EngineImpl &P, void *s, double off_old, double off_new);
+void release_ring(EngineImpl &P);
 
 }  // namespace fesom

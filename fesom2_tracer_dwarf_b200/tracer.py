@@ -121,6 +121,16 @@ class FESOMTracerAdvection:
         """'fp64' (bit-exact), 'fp32', 'bf16' or 'fp16' (16-bit tracer storage, FP32 arithmetic)."""
         _lib.check(self.lib, self.lib.tracer_set_precision(self.PRECISIONS[mode]), "tracer_set_precision")
 
+    def pin(self, array):
+        """Page-lock a contiguous numpy array so its transfers take one DMA (tracer_host_register)."""
+        if not (array.flags["F_CONTIGUOUS"] or array.flags["C_CONTIGUOUS"]):
+            raise ValueError("pin needs a contiguous array")
+        _lib.check(self.lib, self.lib.tracer_host_register(_lib.ptr(array), array.nbytes), "tracer_host_register")
+        return array
+
+    def unpin(self, array):
+        _lib.check(self.lib, self.lib.tracer_host_unregister(_lib.ptr(array)), "tracer_host_unregister")
+
     ROUNDING = {"nearest": 0, "stochastic": 1}
 
     def set_rounding(self, mode):

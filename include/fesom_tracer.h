@@ -140,6 +140,14 @@ int tracer_set_precision(int mode);
  * latest full upload (tracer_set_values); tracer_storage_offset returns it
  * (0 in modes 0, 1). */
 int tracer_set_rounding(int mode);
+/* Page-lock a host range (cudaHostRegister) so that tracer_set_values*,
+ * tracer_get_values* and tracer_advect_* transfers from / to arrays inside it
+ * take one DMA each way instead of going through the library's pinned
+ * staging ring.  Register once, before the time loop; unregister before
+ * freeing the memory.  No counterpart in the reference (whose host arrays are
+ * Fortran-owned and never cross a PCIe bus). */
+int tracer_host_register(void *ptr, long long bytes);
+int tracer_host_unregister(void *ptr);
 int tracer_storage_offset(int tracer_id, double *off);
 /* Compensated FP64 sums over the wet cells of one tracer, on the device:
  * out2[0] = Sum T, out2[1] = Sum T*areasvol*hnode_new (conserved content). */
