@@ -80,6 +80,7 @@ struct FusedArgs {
   R *lo[NTMAX];           // (S, node)
   R *rp[NTMAX], *rm[NTMAX];
   R *vflux;               // (S, edge), shared by the tracers
+  R *gradn[NTMAX];        // (2, S, node): ring-mean gradient (gx, gy) of valuesAB
   const R *vel;           // (2, S, elem)
   const R *W;             // (S, node) interfaces
   R dt, ph, pv;
@@ -110,6 +111,42 @@ __device__ __forceinline__ CellMap map_cells(const DSched &sc, int *s_off, int *
   }
   __syncthreads();
   return cm;
+}
+
+// ---------------------------------------------------------------------------
+// k_grad: ring-mean gradients of valuesAB (lib/oce_muscl_adv.F90:400-450:
+// the mean of tr_xy over the node's ring, weighted by element area), for the
+// node-levels where some incident edge lacks a shared up/down pair
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void ld_pair(const double *p, double &x, double &y) {
+  const double2 v = *reinterpret_cast<const double2 *>(p);
+  x = v.x;
+  y = v.y;
+}
+__device__ __forceinline__ void ld_pair(const float *p, float &x, float &y) {
+  const float2 v = *reinterpret_cast<const float2 *>(p);
+  x = v.x;
+  y = v.y;
+}
+__device__ __forceinline__ void st_pair(double *p, double x, double y) {
+  *reinterpret_cast<double2 *>(p) = make_double2(x, y);
+}
+__device__ __forceinline__ void st_pair(float *p, float x, float y) {
+  *reinterpret_cast<float2 *>(p) = make_float2(x, y);
+}
+
+template <typename R, typename TS, int NT>
+__global__ void __launch_bounds__(kThreads) k_grad(DMeshT<R> m, FusedArgs<R, TS> a) {
+  extern __shared__ int smem[];
+  int *s_off = smem, *s_item = smem + kMaxItemsPerBlock + 1;
+  const CellMap cm = map_cells(m.grad_sched, s_off, s_item);
+  for (int lc = threadIdx.x; lc < cm.nc; lc += blockDim.x) {
+    const int j = s_item[lc], n = cm.i0 + j, k = m.grad_lev0[n] + lc - (s_off[j] - cm.c0);
+    R gx[NTMAX], gy[NTMAX];
+    ring_mean_n(m, a.TAB, a.off, NT, n, k, gx, gy);
+    const size_t o = (size_t)n * m.S + k;
+    for (int t = 0; t < NT; t++) st_pair(a.gradn[t] + 2 * o, gx[t], gy[t]);
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -182,8 +219,11 @@ __global__ void __launch_bounds__(kThreads, 4) k_edge(DMeshT<R> m, FusedArgs<R, 
       trxy_n(m, a.TAB, a.off, NT, ud.x, k, gux, guy);
       trxy_n(m, a.TAB, a.off, NT, ud.y, k, gdx, gdy);
     } else {
-      ring_mean_n(m, a.TAB, a.off, NT, c.n1, k, gux, guy);
-      ring_mean_n(m, a.TAB, a.off, NT, c.n2, k, gdx, gdy);
+      // node ring means, computed once per node-level by k_grad
+      for (int t = 0; t < NT; t++) {
+        ld_pair(a.gradn[t] + 2 * o1, gux[t], guy[t]);
+        ld_pair(a.gradn[t] + 2 * o2, gdx[t], gdy[t]);
+      }
     }
     const R ex = m.edge_dxdy[2 * e], ey = m.edge_dxdy[2 * e + 1], aa = m.edge_a[e];
     R c_lo1 = R(1), c_lo2 = R(1);
@@ -417,6 +457,39 @@ __global__ void __launch_bounds__(kThreads) k_col2(DMeshT<R> m, FusedArgs<R, TS>
   for (int lc = threadIdx.x; lc < cm.nc; lc += blockDim.x) {
     const int j = s_item[lc], n = cm.i0 + j, k = lc - (s_off[j] - cm.c0), nz = k + 1;
     R tmx[NTMAX], tmn[NTMAX];
+    if (m.ring_full[n]) {
+      // With a complete ring, the nodes of the ring elements wet at this level
+      // are the node itself and the far ends of its edges wet at this level
+      // (each such edge has a wet triangle holding both ends); max and min
+      // are exact, so the bounds equal the per-element ones below.
+      const size_t on = (size_t)n * S + k;
+      for (int t = 0; t < NT; t++) {
+        const R l = a.lo[t][on], tt = ldT(a.T[t], on, a.off[t]);
+        tmx[t] = fmax2(l, tt);
+        tmn[t] = fmin2(l, tt);
+      }
+      for (int p = m.ne_ptr[n]; p < m.ne_ptr[n + 1]; p++) {
+        const int4 q = m.ne4[p];
+        if (nz > q.z) continue;
+        const size_t o = (size_t)q.y * S + k;
+        for (int t = 0; t < NT; t++) {
+          const R l = a.lo[t][o], tt = ldT(a.T[t], o, a.off[t]);
+          tmx[t] = fmax2(tmx[t], fmax2(l, tt));
+          tmn[t] = fmin2(tmn[t], fmin2(l, tt));
+        }
+      }
+      if (nz > m.nlev_node_min[n] - 1) {  // a ring element is dry here: +-big enter the bounds
+        for (int t = 0; t < NT; t++) {
+          tmx[t] = fmax2(tmx[t], -big);
+          tmn[t] = fmin2(tmn[t], big);
+        }
+      }
+      for (int t = 0; t < NT; t++) {
+        s_mx[t * kMaxCellsPerBlock + lc] = tmx[t];
+        s_mn[t * kMaxCellsPerBlock + lc] = tmn[t];
+      }
+      continue;
+    }
     for (int p = m.ring_ptr[n]; p < m.ring_ptr[n + 1]; p++) {
       const int el = m.ring_elem[p];
       const bool wet = nz <= m.nlev_elem[el] - 1;

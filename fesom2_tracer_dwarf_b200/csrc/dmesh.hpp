@@ -49,6 +49,7 @@ struct DMeshT {
   const R *elem_area;       // (T)
   const int *ring_ptr;      // (N+1)
   const int *ring_elem;
+  const unsigned char *ring_full;  // (N) 1: the ring holds every element of the node
   const int *ne_ptr;        // (N+1)
   const int4 *ne4;          // per incidence, in ascending edge id:
                             // (slot << 1 | node is the edge's 2nd node, other node, edge levels, 0)
@@ -62,6 +63,10 @@ struct DMeshT {
   const R *helem;           // element
   DSched node_sched;        // items = nodes, levels = nlev_node - 1
   DSched edge_sched;        // items = edges, levels = edge levels
+  // node-levels whose MUSCL gradient is the ring mean for some incident edge
+  // (levels grad_lev0[n] .. nlev_node[n]-2 of node n)
+  const int *grad_lev0;
+  DSched grad_sched;        // items = nodes, levels = nlev_node - 1 - grad_lev0
 };
 
 }  // namespace fesom

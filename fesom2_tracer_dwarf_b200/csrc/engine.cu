@@ -92,6 +92,16 @@ void build_dmesh(EngineImpl &P, DMeshT<R> &d, const std::vector<int> &slot_edge,
   d.elem_area = upload_conv<R>(P, M.elem_area);
   d.ring_ptr = P.upload(M.ring_ptr);
   d.ring_elem = P.upload(M.ring_elem);
+  {
+    // complete rings: every element holding the node is listed (the
+    // reference's periodic compat lists are not, on the wrap rows)
+    std::vector<int> holds(N, 0);
+    for (int e = 0; e < T; e++)
+      for (int q = 0; q < 3; q++) holds[M.elem_nodes[3 * e + q]]++;
+    std::vector<unsigned char> full(N);
+    for (int n = 0; n < N; n++) full[n] = (M.ring_ptr[n + 1] - M.ring_ptr[n]) == holds[n];
+    d.ring_full = P.upload(full);
+  }
   d.ne_ptr = P.upload(M.node_edge_ptr);
   {
     std::vector<int4> ne4(M.node_edge.size());
@@ -123,6 +133,26 @@ void build_dmesh(EngineImpl &P, DMeshT<R> &d, const std::vector<int> &slot_edge,
   d.edge_sched.cell_off = P.upload(off);
   d.edge_sched.blk = P.upload(blk);
   d.edge_sched.nblk = (int)blk.size() - 1;
+
+  // ring-mean gradient levels: an edge uses the node ring means from level
+  // k = min(nlevels_nod2D_min(n1), nlevels_nod2D_min(n2)) - 1 down (from the
+  // surface when it lacks an up or down triangle)
+  std::vector<int> lev0(N);
+  for (int n = 0; n < N; n++) lev0[n] = std::max(0, M.nlev_node[n] - 1);
+  for (int e = 0; e < E; e++) {
+    const int n1 = M.edge_nodes[2 * e], n2 = M.edge_nodes[2 * e + 1];
+    const bool pair = M.up_dn_tri[2 * e] >= 0 && M.up_dn_tri[2 * e + 1] >= 0;
+    const int thr = pair ? std::max(0, std::min(M.nlev_node_min[n1], M.nlev_node_min[n2]) - 1) : 0;
+    lev0[n1] = std::min(lev0[n1], thr);
+    lev0[n2] = std::min(lev0[n2], thr);
+  }
+  d.grad_lev0 = P.upload(lev0);
+  for (int n = 0; n < N; n++) cnt[n] = std::max(0, M.nlev_node[n] - 1 - lev0[n]);
+  cnt.resize(N);
+  build_sched(cnt, off, blk, d.grad_sched.max_items);
+  d.grad_sched.cell_off = P.upload(off);
+  d.grad_sched.blk = P.upload(blk);
+  d.grad_sched.nblk = (int)blk.size() - 1;
 }
 
 }  // namespace
@@ -296,6 +326,7 @@ static void ensure_slots(EngineImpl &P, int n) {
     P.lo[t] = P.dalloc_bytes(ns);
     P.rp[t] = P.dalloc_bytes(ns);
     P.rm[t] = P.dalloc_bytes(ns);
+    P.gradn[t] = P.dalloc_bytes(2 * ns);
   }
   P.slots = n;
 }
@@ -323,6 +354,7 @@ static void run_batch(EngineImpl &P, int first, int nt, double dt, bool refresh_
     b.lo[t] = P.lo[t];
     b.rp[t] = P.rp[t];
     b.rm[t] = P.rm[t];
+    b.gradn[t] = P.gradn[t];
     b.off[t] = tr.off;
     b.seed[t] = mix32_host(P.sround_seed ^ mix32_host((uint32_t)(first + t) * 0x9e3779b9u + tr.nstep));
     tr.nstep++;
@@ -349,7 +381,7 @@ int Engine::launches_per_step() const {
   int n = 0;
   for (int i = 0; i < (int)P.tr.size();) {
     const int nt = batch_size(P, i);
-    n += P.tr[i].sch.lim == 1 ? 4 : 3;
+    n += (P.tr[i].sch.lim == 1 ? 4 : 3) + (P.tr[i].sch.hor != 0 ? 1 : 0);
     i += nt;
   }
   return n;
@@ -372,7 +404,7 @@ size_t Engine::step_scratch_doubles() const {
   const EngineImpl &P = *p_;
   auto up = [](size_t n) { return (n + 31) / 32 * 32; };  // 256-byte pieces
   const size_t es = up((size_t)P.mesh.edge2D * P.S), ns = up((size_t)P.mesh.nod2D * P.S);
-  return 2 * es + 4 * ns;
+  return 2 * es + 6 * ns;
 }
 
 void Engine::step_with_scratch(int id, const double *T, const double *TAB, double *T_out, double dt, double *scratch,
@@ -393,12 +425,13 @@ void Engine::step_with_scratch(int id, const double *T, const double *TAB, doubl
   b.lo[0] = scratch + 2 * es + ns;
   b.rp[0] = scratch + 2 * es + 2 * ns;
   b.rm[0] = scratch + 2 * es + 3 * ns;
+  b.gradn[0] = scratch + 2 * es + 4 * ns;
   dispatch(P, P.tr[id].sch, 1, b, dt);
   CK(cudaStreamSynchronize(P.stream));
 }
 
 const char *const *Engine::kernel_kind_names(int *n) {
-  static const char *const names[KK_COUNT] = {"k_edge", "k_col1", "k_col2", "k_col3"};
+  static const char *const names[KK_COUNT] = {"k_edge", "k_col1", "k_col2", "k_col3", "k_grad"};
   *n = KK_COUNT;
   return names;
 }

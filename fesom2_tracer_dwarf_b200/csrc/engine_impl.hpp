@@ -33,6 +33,7 @@ struct BatchPtrs {
   void *rp[kBatchMax] = {};
   void *rm[kBatchMax] = {};
   void *vflux = nullptr;
+  void *gradn[kBatchMax] = {};
   double off[kBatchMax] = {};     // storage offsets (16-bit storage)
   uint32_t seed[kBatchMax] = {};  // stochastic-rounding streams
   int sround = 0;
@@ -68,6 +69,7 @@ struct EngineImpl {
   int slots = 0;
   void *vflux = nullptr;
   void *adfh[kBatchMax] = {}, *adfv[kBatchMax] = {}, *lo[kBatchMax] = {}, *rp[kBatchMax] = {}, *rm[kBatchMax] = {};
+  void *gradn[kBatchMax] = {};
 
   // launch profiling: when prof is set, every launch is bracketed by events
   struct ProfRec {
@@ -134,7 +136,7 @@ struct EngineImpl {
 };
 
 // Kernel kinds reported by profile_steps.
-enum { KK_EDGE = 0, KK_COL1, KK_COL2, KK_COL3, KK_COUNT };
+enum { KK_EDGE = 0, KK_COL1, KK_COL2, KK_COL3, KK_GRAD, KK_COUNT };
 
 // Launch one batch of nt tracers (kernels in step_f64.cu / step_f32.cu).
 void launch_batch_f64(EngineImpl &P, const TracerScheme &sc, int nt, const BatchPtrs &b, double dt);

@@ -48,8 +48,18 @@ void launch_col1(EngineImpl &P, const FusedArgs<R, TS> &a) {
   P.mark_end();
 }
 
+template <typename R, typename TS, int NT>
+void launch_grad(EngineImpl &P, const FusedArgs<R, TS> &a) {
+  const DMeshT<R> &m = dmesh<R>(P);
+  if (m.grad_sched.nblk <= 0) return;
+  P.mark_begin(KK_GRAD);
+  k_grad<R, TS, NT><<<m.grad_sched.nblk, kThreads, smem_edge(), P.stream>>>(m, a);
+  P.mark_end();
+}
+
 template <typename R, typename TS, int NT, int LIM>
 void run_group(EngineImpl &P, const TracerScheme &sc, const FusedArgs<R, TS> &a) {
+  if (sc.hor != 0) launch_grad<R, TS, NT>(P, a);
   switch (sc.hor) {
     case 1: launch_edge<R, TS, NT, HOR_MUSCL, LIM>(P, a); break;
     case 2: launch_edge<R, TS, NT, HOR_MFCT, LIM>(P, a); break;
@@ -87,6 +97,7 @@ void launch_batch_t(EngineImpl &P, const TracerScheme &sc, int nt, const BatchPt
     a.lo[t] = (R *)b.lo[t];
     a.rp[t] = (R *)b.rp[t];
     a.rm[t] = (R *)b.rm[t];
+    a.gradn[t] = (R *)b.gradn[t];
   }
   a.vflux = (R *)b.vflux;
   a.vel = (const R *)P.vel;
