@@ -82,6 +82,26 @@ SIGNATURES = {
     "tracer_selftest_division": (ctypes.c_int, [ctypes.c_longlong, ctypes.c_uint64, _vp, _vp]),
     "tracer_selftest_sround": (ctypes.c_int, [ctypes.c_int, ctypes.c_longlong, ctypes.c_int, ctypes.c_uint32,
                                               ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_double)]),
+    "tracer_batch_create": (ctypes.c_int, []),
+    "tracer_batch_destroy": (ctypes.c_int, []),
+    "tracer_batch_add_member": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                               ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_int, _vp,
+                                               ctypes.c_int]),
+    "tracer_batch_member_dims": (ctypes.c_int, [ctypes.c_int, _vp]),
+    "tracer_batch_set_velocity": (ctypes.c_int, [ctypes.c_int, _vp, _vp]),
+    "tracer_batch_set_values": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _vp]),
+    "tracer_batch_get_values": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _vp]),
+    "tracer_batch_configure": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_double,
+                                              ctypes.c_double, _vp, ctypes.c_int]),
+    "tracer_batch_set_tile": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
+    "tracer_batch_get_tile": (ctypes.c_int, [_vp]),
+    "tracer_batch_autotune": (ctypes.c_int, [ctypes.c_int, ctypes.c_char_p, ctypes.c_int]),
+    "tracer_batch_steps": (ctypes.c_int, [ctypes.c_int, ctypes.c_int]),
+    "tracer_batch_time_steps": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),
+    "tracer_batch_steps_separate": (ctypes.c_int, [ctypes.c_int]),
+    "tracer_batch_time_separate": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),
+    "tracer_batch_info": (ctypes.c_int, [_vp]),
+    "tracer_selftest_barrier_timeout": (ctypes.c_int, [ctypes.c_longlong]),
     "tracer_advect_device_noalloc": (ctypes.c_int, [ctypes.c_int, _vp, _vp, _vp, ctypes.c_double]),
     "tracer_noalloc_scratch_bytes": (ctypes.c_longlong, []),
     "tracer_last_error": (ctypes.c_char_p, []),

@@ -97,10 +97,10 @@ struct CellMap {
   int i0, ni, c0, nc;
 };
 
-__device__ __forceinline__ CellMap map_cells(const DSched &sc, int *s_off, int *s_item) {
+__device__ __forceinline__ CellMap map_cells(const DSched &sc, int blk, int *s_off, int *s_item) {
   CellMap cm;
-  cm.i0 = sc.blk[blockIdx.x];
-  cm.ni = sc.blk[blockIdx.x + 1] - cm.i0;
+  cm.i0 = sc.blk[blk];
+  cm.ni = sc.blk[blk + 1] - cm.i0;
   for (int t = threadIdx.x; t <= cm.ni; t += blockDim.x) s_off[t] = sc.cell_off[cm.i0 + t];
   __syncthreads();
   cm.c0 = s_off[0];
@@ -136,10 +136,9 @@ __device__ __forceinline__ void st_pair(float *p, float x, float y) {
 }
 
 template <typename R, typename TS, int NT>
-__global__ void __launch_bounds__(kThreads) k_grad(DMeshT<R> m, FusedArgs<R, TS> a) {
-  extern __shared__ int smem[];
+__device__ __forceinline__ void grad_block(const DMeshT<R> &m, const FusedArgs<R, TS> &a, int blk, int *smem) {
   int *s_off = smem, *s_item = smem + kMaxItemsPerBlock + 1;
-  const CellMap cm = map_cells(m.grad_sched, s_off, s_item);
+  const CellMap cm = map_cells(m.grad_sched, blk, s_off, s_item);
   for (int lc = threadIdx.x; lc < cm.nc; lc += blockDim.x) {
     const int j = s_item[lc], n = cm.i0 + j, k = m.grad_lev0[n] + lc - (s_off[j] - cm.c0);
     R gx[NTMAX], gy[NTMAX];
@@ -147,6 +146,12 @@ __global__ void __launch_bounds__(kThreads) k_grad(DMeshT<R> m, FusedArgs<R, TS>
     const size_t o = (size_t)n * m.S + k;
     for (int t = 0; t < NT; t++) st_pair(a.gradn[t] + 2 * o, gx[t], gy[t]);
   }
+}
+
+template <typename R, typename TS, int NT>
+__global__ void __launch_bounds__(kThreads) k_grad(DMeshT<R> m, FusedArgs<R, TS> a) {
+  extern __shared__ int smem[];
+  grad_block<R, TS, NT>(m, a, blockIdx.x, smem);
 }
 
 // ---------------------------------------------------------------------------
@@ -191,10 +196,9 @@ __device__ __forceinline__ void ring_mean_n(const DMeshT<R> &m, const TS *const 
 }
 
 template <typename R, typename TS, int NT, int HOR, int LIM>
-__global__ void __launch_bounds__(kThreads, 4) k_edge(DMeshT<R> m, FusedArgs<R, TS> a) {
-  extern __shared__ int smem[];
+__device__ __forceinline__ void edge_block(const DMeshT<R> &m, const FusedArgs<R, TS> &a, int blk, int *smem) {
   int *s_off = smem, *s_item = smem + kMaxItemsPerBlock + 1;
-  const CellMap cm = map_cells(m.edge_sched, s_off, s_item);
+  const CellMap cm = map_cells(m.edge_sched, blk, s_off, s_item);
   const R re = R(kREarthD), sixth = R(1.0 / 6.0);
   for (int lc = threadIdx.x; lc < cm.nc; lc += blockDim.x) {
     const int j = s_item[lc], e = cm.i0 + j, k = lc - (s_off[j] - cm.c0);
@@ -252,6 +256,12 @@ __global__ void __launch_bounds__(kThreads, 4) k_edge(DMeshT<R> m, FusedArgs<R, 
   }
 }
 
+template <typename R, typename TS, int NT, int HOR, int LIM>
+__global__ void __launch_bounds__(kThreads, 4) k_edge(DMeshT<R> m, FusedArgs<R, TS> a) {
+  extern __shared__ int smem[];
+  edge_block<R, TS, NT, HOR, LIM>(m, a, blockIdx.x, smem);
+}
+
 // ---------------------------------------------------------------------------
 // k_col1: LO solution and vertical fluxes
 // ---------------------------------------------------------------------------
@@ -268,15 +278,14 @@ __device__ __forceinline__ R ppm_slope(R Tm1, R T0, R Tp1, R c1, R c2, R c3) {
 }
 
 template <typename R, typename TS, int NT, int VER, int LIM>
-__global__ void __launch_bounds__(kThreads, 4) k_col1(DMeshT<R> m, FusedArgs<R, TS> a) {
-  extern __shared__ int smem[];
+__device__ __forceinline__ void col1_block(const DMeshT<R> &m, const FusedArgs<R, TS> &a, int blk, int *smem) {
   int *s_off = smem, *s_item = smem + kMaxItemsPerBlock + 1;
   R *s_acc = (R *)(smem + kMaxItemsPerBlock + 1 + kMaxCellsPerBlock + 1);  // 8-byte aligned below
   s_acc = (R *)(((uintptr_t)s_acc + 15) & ~(uintptr_t)15);
   R *s_slope = s_acc + NT * kMaxCellsPerBlock;
   R *s_tv = s_slope + NT * kMaxCellsPerBlock;
   R *s_fv = s_tv + NT * kMaxCellsPerBlock;
-  const CellMap cm = map_cells(m.node_sched, s_off, s_item);
+  const CellMap cm = map_cells(m.node_sched, blk, s_off, s_item);
   const int S = m.S;
 
   // stage A: horizontal LO gather and PPM slopes
@@ -440,17 +449,22 @@ __global__ void __launch_bounds__(kThreads, 4) k_col1(DMeshT<R> m, FusedArgs<R, 
   }
 }
 
+template <typename R, typename TS, int NT, int VER, int LIM>
+__global__ void __launch_bounds__(kThreads, 4) k_col1(DMeshT<R> m, FusedArgs<R, TS> a) {
+  extern __shared__ int smem[];
+  col1_block<R, TS, NT, VER, LIM>(m, a, blockIdx.x, smem);
+}
+
 // ---------------------------------------------------------------------------
 // k_col2: bounds, in/out sums, ratios (lib/oce_adv_tra_fct.F90:105-374)
 // ---------------------------------------------------------------------------
 template <typename R, typename TS, int NT>
-__global__ void __launch_bounds__(kThreads) k_col2(DMeshT<R> m, FusedArgs<R, TS> a) {
-  extern __shared__ int smem[];
+__device__ __forceinline__ void col2_block(const DMeshT<R> &m, const FusedArgs<R, TS> &a, int blk, int *smem) {
   int *s_off = smem, *s_item = smem + kMaxItemsPerBlock + 1;
   R *s_mx = (R *)(smem + kMaxItemsPerBlock + 1 + kMaxCellsPerBlock + 1);
   s_mx = (R *)(((uintptr_t)s_mx + 15) & ~(uintptr_t)15);
   R *s_mn = s_mx + NT * kMaxCellsPerBlock;
-  const CellMap cm = map_cells(m.node_sched, s_off, s_item);
+  const CellMap cm = map_cells(m.node_sched, blk, s_off, s_item);
   const int S = m.S;
   const R big = R(1e3);
 
@@ -578,6 +592,12 @@ __global__ void __launch_bounds__(kThreads) k_col2(DMeshT<R> m, FusedArgs<R, TS>
   }
 }
 
+template <typename R, typename TS, int NT>
+__global__ void __launch_bounds__(kThreads) k_col2(DMeshT<R> m, FusedArgs<R, TS> a) {
+  extern __shared__ int smem[];
+  col2_block<R, TS, NT>(m, a, blockIdx.x, smem);
+}
+
 // limited vertical flux at interface i (lib/oce_adv_tra_fct.F90:396-427)
 template <typename R>
 __device__ __forceinline__ R limit_v(const R *av, const R *rp, const R *rm, int i, int nlev) {
@@ -600,10 +620,9 @@ __device__ __forceinline__ R limit_v(const R *av, const R *rp, const R *rm, int 
 // k_col3: limiting + flux2dtracer + update
 // ---------------------------------------------------------------------------
 template <typename R, typename TS, int NT, int LIM>
-__global__ void __launch_bounds__(kThreads, 4) k_col3(DMeshT<R> m, FusedArgs<R, TS> a) {
-  extern __shared__ int smem[];
+__device__ __forceinline__ void col3_block(const DMeshT<R> &m, const FusedArgs<R, TS> &a, int blk, int *smem) {
   int *s_off = smem, *s_item = smem + kMaxItemsPerBlock + 1;
-  const CellMap cm = map_cells(m.node_sched, s_off, s_item);
+  const CellMap cm = map_cells(m.node_sched, blk, s_off, s_item);
   const int S = m.S;
   for (int lc = threadIdx.x; lc < cm.nc; lc += blockDim.x) {
     const int j = s_item[lc], n = cm.i0 + j, k = lc - (s_off[j] - cm.c0), nz = k + 1;
@@ -653,6 +672,12 @@ __global__ void __launch_bounds__(kThreads, 4) k_col3(DMeshT<R> m, FusedArgs<R, 
       a.T_out[t][o] = stT<R, TS>(tnew, a.off[t], a.sround != 0, a.sround ? mix32(a.seed[t] ^ mix32((uint32_t)o)) : 0u);
     }
   }
+}
+
+template <typename R, typename TS, int NT, int LIM>
+__global__ void __launch_bounds__(kThreads, 4) k_col3(DMeshT<R> m, FusedArgs<R, TS> a) {
+  extern __shared__ int smem[];
+  col3_block<R, TS, NT, LIM>(m, a, blockIdx.x, smem);
 }
 
 // dynamic shared memory of each kernel

@@ -1,0 +1,73 @@
+// Multi-member batched stepping (many tracers of many ensemble members on
+// meshes of different sizes, advanced together).
+//
+// Every member is an FP32 Engine that owns its mesh, velocity and tracers.
+// One step of the whole batch is ONE persistent cooperative kernel launch:
+// the launch walks a work list of (member, 4-tracer batch, block of wet
+// cells) items phase by phase -- ring-mean gradients, edge fluxes, vertical
+// fluxes and low-order solution, FCT bounds and ratios, limiting and update --
+// with a grid-wide barrier between phases.  Tracer batches run in waves of a
+// bounded number per member so the work arrays stay small.  The kernel swaps
+// the new and old tracer buffers in its device-side task table at the end, so
+// the same launch, captured once in a CUDA graph, advances the batch step
+// after step.  An autotuner picks the tile (wet cells per block, i.e. nodes
+// per block x levels), the threads per block, the persistent grid size and
+// the number of tracer batches in flight.
+#pragma once
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "engine.hpp"
+
+namespace fesom {
+
+struct BatchTile {
+  int cells_per_block = 512;  // schedule tile (wet cells per block)
+  int threads = 256;          // threads per block
+  int blocks_per_sm = 2;      // persistent grid = SMs x this
+  int wave = 3;               // 4-tracer batches in flight per member
+};
+
+struct BatchImpl;
+
+class Batch {
+ public:
+  Batch();
+  ~Batch();
+  Batch(const Batch &) = delete;
+  Batch &operator=(const Batch &) = delete;
+
+  // Members: FP32 engines on their own meshes; ntracers must be a multiple of 4.
+  int add_member(const MeshHost &mesh, int ntracers);
+  int num_members() const;
+  Engine &member(int i);
+
+  // Scheme (one for every tracer), per-member time steps and valuesAB
+  // refresh; then device work arrays and the task table for a tile.
+  void configure(const TracerScheme &sch, const std::vector<double> &dt, bool refresh_ab);
+  void set_tile(const BatchTile &tile);
+  BatchTile tile() const;
+
+  // nsteps persistent launches (replayed from a CUDA graph when use_graph).
+  void step(int nsteps, bool use_graph);
+  // Device time of nsteps (CUDA events on the batch stream), milliseconds.
+  double time_steps(int nsteps, bool use_graph);
+  // The same steps as separate per-member, per-batch kernel launches.
+  void step_separate(int nsteps);
+  double time_separate(int nsteps);
+
+  // Times candidate tiles (steps_per_candidate steps each, from copies of the
+  // current tracer state, which is restored afterwards) and keeps the
+  // fastest.  Returns a description of every candidate and its time.
+  std::string autotune(int steps_per_candidate);
+
+  bool graph_captured() const;
+  long long work_bytes() const;
+  long long wet_cells() const;  // sum over members of wet cells x tracers
+
+ private:
+  BatchImpl *p_;
+};
+
+}  // namespace fesom

@@ -11,6 +11,7 @@
 #include <vector>
 
 #include "../../include/fesom_tracer.h"
+#include "batch.hpp"
 #include "engine.hpp"
 
 using namespace fesom;
@@ -703,3 +704,175 @@ long long tracer_device_bytes(void) { return g.eng ? (long long)g.eng->device_by
 const char *tracer_last_error(void) { return last_error(); }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// multi-member batch (batch.hpp)
+// ---------------------------------------------------------------------------
+namespace fesom {
+int batch_selftest_barrier_timeout(long long limit);
+}
+
+namespace {
+std::unique_ptr<Batch> g_batch;
+
+Batch &batch() {
+  if (!g_batch) throw std::runtime_error("no batch: call tracer_batch_create");
+  return *g_batch;
+}
+Engine &batch_member(int m) { return batch().member(m); }
+}  // namespace
+
+int tracer_batch_create(void) {
+  return guarded([&] {
+    g_batch.reset();
+    g_batch.reset(new Batch());
+    return 0;
+  });
+}
+
+int tracer_batch_destroy(void) {
+  return guarded([&] {
+    g_batch.reset();
+    return 0;
+  });
+}
+
+int tracer_batch_add_member(int nx, int ny, int nl, double Lx, double Ly, double max_depth, int periodic,
+                            int options, const int *node_K, int ntracers) {
+  return guarded([&] {
+    if (node_K) {
+      const int nn = analytic_nodes(nx, ny, periodic != 0);
+      for (int i = 0; i < nn; i++)
+        if (node_K[i] < 3 || node_K[i] > nl) return fail("node_K outside [3, nl]");
+    }
+    MeshHost m = build_analytic_mesh(nx, ny, nl, Lx, Ly, max_depth, periodic != 0, (options & 1) != 0, node_K,
+                                     (options & 2) != 0);
+    return batch().add_member(m, ntracers);
+  });
+}
+
+int tracer_batch_member_dims(int member, int *dims4) {
+  return guarded([&] {
+    const MeshHost &m = batch_member(member).mesh();
+    dims4[0] = m.nl; dims4[1] = m.nod2D; dims4[2] = m.elem2D; dims4[3] = m.edge2D;
+    return 0;
+  });
+}
+
+int tracer_batch_set_velocity(int member, const double *uv, const double *w) {
+  return guarded([&] {
+    if (!uv || !w) return fail("null velocity");
+    batch_member(member).set_velocity(uv, w);
+    return 0;
+  });
+}
+
+int tracer_batch_set_values(int member, int tracer_id, const double *values) {
+  return guarded([&] {
+    if (!values) return fail("null values");
+    Engine &e = batch_member(member);
+    if (tracer_id < 1 || tracer_id > e.num_tracers()) return fail("invalid tracer_id " + std::to_string(tracer_id));
+    e.set_values(tracer_id - 1, values, true);
+    return 0;
+  });
+}
+
+int tracer_batch_get_values(int member, int tracer_id, double *values) {
+  return guarded([&] {
+    if (!values) return fail("null values");
+    Engine &e = batch_member(member);
+    if (tracer_id < 1 || tracer_id > e.num_tracers()) return fail("invalid tracer_id " + std::to_string(tracer_id));
+    e.get_values(tracer_id - 1, values);
+    return 0;
+  });
+}
+
+int tracer_batch_configure(const char *hor, const char *ver, const char *lim, double ph, double pv, const double *dt,
+                           int refresh_ab) {
+  return guarded([&] {
+    if (!dt) return fail("null dt");
+    Batch &b = batch();
+    std::vector<double> d(dt, dt + b.num_members());
+    b.configure(parse_scheme(hor, ver, lim, ph, pv), d, refresh_ab != 0);
+    return 0;
+  });
+}
+
+int tracer_batch_set_tile(int cells_per_block, int threads, int blocks_per_sm, int wave) {
+  return guarded([&] {
+    BatchTile t;
+    t.cells_per_block = cells_per_block;
+    t.threads = threads;
+    t.blocks_per_sm = blocks_per_sm;
+    t.wave = wave;
+    batch().set_tile(t);
+    return 0;
+  });
+}
+
+int tracer_batch_get_tile(int *tile4) {
+  return guarded([&] {
+    const BatchTile t = batch().tile();
+    tile4[0] = t.cells_per_block; tile4[1] = t.threads; tile4[2] = t.blocks_per_sm; tile4[3] = t.wave;
+    return 0;
+  });
+}
+
+int tracer_batch_steps(int nsteps, int use_graph) {
+  return guarded([&] {
+    if (nsteps < 0) return fail("nsteps < 0");
+    batch().step(nsteps, use_graph != 0);
+    return 0;
+  });
+}
+
+int tracer_batch_time_steps(int nsteps, int use_graph, double *ms) {
+  return guarded([&] {
+    if (nsteps < 1 || !ms) return fail("nsteps < 1 or null output");
+    *ms = batch().time_steps(nsteps, use_graph != 0);
+    return 0;
+  });
+}
+
+int tracer_batch_steps_separate(int nsteps) {
+  return guarded([&] {
+    batch().step_separate(nsteps);
+    return 0;
+  });
+}
+
+int tracer_batch_time_separate(int nsteps, double *ms) {
+  return guarded([&] {
+    if (nsteps < 1 || !ms) return fail("nsteps < 1 or null output");
+    *ms = batch().time_separate(nsteps);
+    return 0;
+  });
+}
+
+int tracer_batch_autotune(int steps_per_candidate, char *log, int log_capacity) {
+  return guarded([&] {
+    const std::string s = batch().autotune(std::max(1, steps_per_candidate));
+    if (log && log_capacity > 0) {
+      const size_t n = std::min(s.size(), (size_t)log_capacity - 1);
+      std::memcpy(log, s.data(), n);
+      log[n] = 0;
+    }
+    return 0;
+  });
+}
+
+int tracer_batch_info(long long *info4) {
+  return guarded([&] {
+    Batch &b = batch();
+    info4[0] = b.num_members();
+    info4[1] = b.wet_cells();
+    info4[2] = b.work_bytes();
+    info4[3] = b.graph_captured() ? 1 : 0;
+    return 0;
+  });
+}
+
+int tracer_selftest_barrier_timeout(long long limit) {
+  return guarded([&] { return batch_selftest_barrier_timeout(limit); });
+}
+

@@ -22,26 +22,38 @@ void set_last_error(const std::string &s) { g_err = s; }
 
 namespace {
 
-void build_sched(const std::vector<int> &counts, std::vector<int> &off, std::vector<int> &blk, int &max_items) {
+void build_sched(const std::vector<int> &counts, std::vector<int> &off, std::vector<int> &blk, int &max_items,
+                 int cells_per_block) {
   const int n = (int)counts.size();
   off.assign(n + 1, 0);
   for (int i = 0; i < n; i++) off[i + 1] = off[i] + counts[i];
   blk.clear();
   blk.push_back(0);
   max_items = 1;
-  int start = 0;
+  int start = 0, cells = 0;
   for (int i = 0; i < n; i++) {
-    const int items = i + 1 - start, cells = off[i + 1] - off[start];
-    if (cells >= kCellsPerBlock || items >= kMaxItemsPerBlock || i == n - 1) {
+    // close the block before an item that would overflow its capacity
+    if (i > start && (cells + counts[i] > kMaxCellsPerBlock || i - start >= kMaxItemsPerBlock)) {
+      blk.push_back(i);
+      max_items = std::max(max_items, i - start);
+      start = i;
+      cells = 0;
+    }
+    cells += counts[i];
+    if (cells >= cells_per_block) {
       blk.push_back(i + 1);
-      max_items = std::max(max_items, items);
+      max_items = std::max(max_items, i + 1 - start);
       start = i + 1;
+      cells = 0;
     }
   }
-  if (n == 0) blk.push_back(0);
+  if (start < n || n == 0) {
+    blk.push_back(n);
+    max_items = std::max(max_items, n - start);
+  }
   for (size_t b = 0; b + 1 < blk.size(); b++)
     if (off[blk[b + 1]] - off[blk[b]] > kMaxCellsPerBlock)
-      throw std::runtime_error("schedule block exceeds the per-block cell capacity");
+      throw std::runtime_error("a column or edge has more levels than a block holds");
 }
 
 // (ld, ncol) column-major host doubles -> device columns of stride S, type R
@@ -57,6 +69,52 @@ R *upload_conv(EngineImpl &P, const std::vector<double> &h) {
   std::vector<R> st(h.size());
   for (size_t i = 0; i < h.size(); i++) st[i] = (R)h[i];
   return P.upload(st);
+}
+
+// Work schedules (node, edge and gradient cells) for a target number of wet
+// cells per block; the arrays of a previous tiling are released.
+template <typename R>
+void build_schedules(EngineImpl &P, DMeshT<R> &d, int cells_per_block) {
+  const MeshHost &M = P.mesh;
+  const int N = M.nod2D, E = M.edge2D;
+  const std::vector<int> &slot_edge = P.slot_edge;
+  for (const void *q : {(const void *)d.node_sched.cell_off, (const void *)d.node_sched.blk,
+                        (const void *)d.edge_sched.cell_off, (const void *)d.edge_sched.blk,
+                        (const void *)d.grad_sched.cell_off, (const void *)d.grad_sched.blk,
+                        (const void *)d.grad_lev0})
+    P.dfree(const_cast<void *>(q));
+  std::vector<int> cnt(N), off, blk;
+  for (int n = 0; n < N; n++) cnt[n] = M.nlev_node[n] - 1;
+  build_sched(cnt, off, blk, d.node_sched.max_items, cells_per_block);
+  d.node_sched.cell_off = P.upload(off);
+  d.node_sched.blk = P.upload(blk);
+  d.node_sched.nblk = (int)blk.size() - 1;
+  cnt.assign(E, 0);
+  for (int s = 0; s < E; s++) cnt[s] = M.edge_levels(slot_edge[s]);
+  build_sched(cnt, off, blk, d.edge_sched.max_items, cells_per_block);
+  d.edge_sched.cell_off = P.upload(off);
+  d.edge_sched.blk = P.upload(blk);
+  d.edge_sched.nblk = (int)blk.size() - 1;
+
+  // ring-mean gradient levels: an edge uses the node ring means from level
+  // k = min(nlevels_nod2D_min(n1), nlevels_nod2D_min(n2)) - 1 down (from the
+  // surface when it lacks an up or down triangle)
+  std::vector<int> lev0(N);
+  for (int n = 0; n < N; n++) lev0[n] = std::max(0, M.nlev_node[n] - 1);
+  for (int e = 0; e < E; e++) {
+    const int n1 = M.edge_nodes[2 * e], n2 = M.edge_nodes[2 * e + 1];
+    const bool pair = M.up_dn_tri[2 * e] >= 0 && M.up_dn_tri[2 * e + 1] >= 0;
+    const int thr = pair ? std::max(0, std::min(M.nlev_node_min[n1], M.nlev_node_min[n2]) - 1) : 0;
+    lev0[n1] = std::min(lev0[n1], thr);
+    lev0[n2] = std::min(lev0[n2], thr);
+  }
+  d.grad_lev0 = P.upload(lev0);
+  for (int n = 0; n < N; n++) cnt[n] = std::max(0, M.nlev_node[n] - 1 - lev0[n]);
+  cnt.resize(N);
+  build_sched(cnt, off, blk, d.grad_sched.max_items, cells_per_block);
+  d.grad_sched.cell_off = P.upload(off);
+  d.grad_sched.blk = P.upload(blk);
+  d.grad_sched.nblk = (int)blk.size() - 1;
 }
 
 template <typename R>
@@ -121,38 +179,7 @@ void build_dmesh(EngineImpl &P, DMeshT<R> &d, const std::vector<int> &slot_edge,
   d.hnode_new = upload_cols<R>(P, M.hnode_new.data(), L, N, L);
   d.helem = upload_cols<R>(P, M.helem.data(), L, T, L);
 
-  std::vector<int> cnt(N), off, blk;
-  for (int n = 0; n < N; n++) cnt[n] = M.nlev_node[n] - 1;
-  build_sched(cnt, off, blk, d.node_sched.max_items);
-  d.node_sched.cell_off = P.upload(off);
-  d.node_sched.blk = P.upload(blk);
-  d.node_sched.nblk = (int)blk.size() - 1;
-  cnt.assign(E, 0);
-  for (int s = 0; s < E; s++) cnt[s] = M.edge_levels(slot_edge[s]);
-  build_sched(cnt, off, blk, d.edge_sched.max_items);
-  d.edge_sched.cell_off = P.upload(off);
-  d.edge_sched.blk = P.upload(blk);
-  d.edge_sched.nblk = (int)blk.size() - 1;
-
-  // ring-mean gradient levels: an edge uses the node ring means from level
-  // k = min(nlevels_nod2D_min(n1), nlevels_nod2D_min(n2)) - 1 down (from the
-  // surface when it lacks an up or down triangle)
-  std::vector<int> lev0(N);
-  for (int n = 0; n < N; n++) lev0[n] = std::max(0, M.nlev_node[n] - 1);
-  for (int e = 0; e < E; e++) {
-    const int n1 = M.edge_nodes[2 * e], n2 = M.edge_nodes[2 * e + 1];
-    const bool pair = M.up_dn_tri[2 * e] >= 0 && M.up_dn_tri[2 * e + 1] >= 0;
-    const int thr = pair ? std::max(0, std::min(M.nlev_node_min[n1], M.nlev_node_min[n2]) - 1) : 0;
-    lev0[n1] = std::min(lev0[n1], thr);
-    lev0[n2] = std::min(lev0[n2], thr);
-  }
-  d.grad_lev0 = P.upload(lev0);
-  for (int n = 0; n < N; n++) cnt[n] = std::max(0, M.nlev_node[n] - 1 - lev0[n]);
-  cnt.resize(N);
-  build_sched(cnt, off, blk, d.grad_sched.max_items);
-  d.grad_sched.cell_off = P.upload(off);
-  d.grad_sched.blk = P.upload(blk);
-  d.grad_sched.nblk = (int)blk.size() - 1;
+  build_schedules(P, d, kCellsPerBlock);
 }
 
 }  // namespace
@@ -178,6 +205,7 @@ Engine::Engine(const MeshHost &mesh, Precision prec) : p_(new EngineImpl) {
     return std::min(M.edge_nodes[2 * a], M.edge_nodes[2 * a + 1]) < std::min(M.edge_nodes[2 * b], M.edge_nodes[2 * b + 1]);
   });
   for (int s = 0; s < E; s++) edge_slot[slot_edge[s]] = s;
+  P.slot_edge = slot_edge;
   if (prec == Precision::FP64) build_dmesh<double>(P, P.dm64, slot_edge, edge_slot);
   else build_dmesh<float>(P, P.dm32, slot_edge, edge_slot);
   P.vel = P.dalloc_bytes((size_t)2 * M.elem2D * P.S * P.r_bytes);
@@ -195,6 +223,18 @@ Engine::~Engine() {
 }
 
 const MeshHost &Engine::mesh() const { return p_->mesh; }
+EngineImpl *Engine::impl() { return p_; }
+
+void Engine::set_cells_per_block(int cells) {
+  EngineImpl &P = *p_;
+  if (cells < 32 || cells > kMaxCellsPerBlock) throw std::invalid_argument("cells per block must be in [32, 576]");
+  CK(cudaStreamSynchronize(P.stream));
+  if (P.prec == Precision::FP64) build_schedules(P, P.dm64, cells);
+  else build_schedules(P, P.dm32, cells);
+  P.cells_per_block = cells;
+  CK(cudaStreamSynchronize(P.stream));
+}
+int Engine::cells_per_block() const { return p_->cells_per_block; }
 int Engine::level_stride() const { return p_->S; }
 Precision Engine::precision() const { return p_->prec; }
 void *Engine::stream() const { return (void *)p_->stream; }
@@ -230,7 +270,7 @@ void Engine::set_velocity_zero() {
   CK(cudaStreamSynchronize(P.stream));
 }
 
-void Engine::allocate_tracers(int ntr) {
+void Engine::allocate_tracers(int ntr, bool with_ab) {
   EngineImpl &P = *p_;
   CK(cudaStreamSynchronize(P.stream));
   for (auto &t : P.tr) { P.dfree(t.T); P.dfree(t.Tout); P.dfree(t.TAB); }
@@ -239,9 +279,23 @@ void Engine::allocate_tracers(int ntr) {
   for (auto &t : P.tr) {
     t.T = P.dalloc_bytes(n);
     t.Tout = P.dalloc_bytes(n);
-    t.TAB = P.dalloc_bytes(n);
+    t.TAB = with_ab ? P.dalloc_bytes(n) : nullptr;
   }
   CK(cudaStreamSynchronize(P.stream));
+}
+
+void Engine::release_work() {
+  EngineImpl &P = *p_;
+  CK(cudaStreamSynchronize(P.stream));
+  for (int t = 0; t < P.slots; t++) {
+    for (void **q : {&P.adfh[t], &P.adfv[t], &P.lo[t], &P.rp[t], &P.rm[t], &P.gradn[t]}) {
+      P.dfree(*q);
+      *q = nullptr;
+    }
+  }
+  P.dfree(P.vflux);
+  P.vflux = nullptr;
+  P.slots = 0;
 }
 
 static void check_id(const EngineImpl &P, int id) {
@@ -272,6 +326,7 @@ void Engine::set_values_ab(int id, const double *v) {
   EngineImpl &P = *p_;
   check_id(P, id);
   CK(cudaStreamSynchronize(P.stream));
+  if (!P.tr[id].TAB) throw std::invalid_argument("tracer has no valuesAB array (valuesAB := values each step)");
   stage_upload(P, v);
   stage_pack(P, P.tr[id].off, P.tr[id].TAB, nullptr, nullptr);
   CK(cudaStreamSynchronize(P.stream));
@@ -347,6 +402,7 @@ static void run_batch(EngineImpl &P, int first, int nt, double dt, bool refresh_
   for (int t = 0; t < nt; t++) {
     auto &tr = P.tr[first + t];
     b.T[t] = tr.T;
+    if (!refresh_ab && !tr.TAB) throw std::invalid_argument("tracer has no valuesAB array: advance with valuesAB := values");
     b.TAB[t] = refresh_ab ? tr.T : tr.TAB;
     b.T_out[t] = tr.Tout;
     b.adf_h[t] = P.adfh[t];

@@ -53,11 +53,19 @@ class Engine {
 
   const MeshHost &mesh() const;
   int level_stride() const;
+  // Schedule tile: target wet cells per block (32..576, default 512).
+  void set_cells_per_block(int cells);
+  int cells_per_block() const;
+  // Internal state, for the multi-member batch runner (batch.cu).
+  EngineImpl *impl();
 
   void set_velocity(const double *uv, const double *w);
   void set_velocity_zero();
   // (Re)allocate ntr tracers, all zero, default scheme UPW1/UPW1/NONE.
-  void allocate_tracers(int ntr);
+  // with_ab = false: no separate valuesAB arrays (valuesAB := values only).
+  void allocate_tracers(int ntr, bool with_ab = true);
+  // Frees the per-batch work arrays (reallocated by the next step).
+  void release_work();
   int num_tracers() const;
   // values -> tracer id (0-based); valuesAB follows when also_ab.
   void set_values(int id, const double *v, bool also_ab);

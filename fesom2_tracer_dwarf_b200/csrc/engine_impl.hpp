@@ -41,6 +41,8 @@ struct BatchPtrs {
 
 struct EngineImpl {
   MeshHost mesh;
+  std::vector<int> slot_edge;  // edge stored in each slot
+  int cells_per_block = 512;   // schedule tile
   int S = 0;
   Precision prec = Precision::FP64;
   size_t ts_bytes = 8;  // tracer storage element
@@ -106,7 +108,8 @@ struct EngineImpl {
   void dfree(void *p) {
     if (!p) return;
     auto it = std::find(allocs.begin(), allocs.end(), p);
-    if (it != allocs.end()) allocs.erase(it);
+    if (it == allocs.end()) return;  // not ours
+    allocs.erase(it);
     cudaFree(p);
   }
   // Every transfer is ordered on the engine's stream (which does not

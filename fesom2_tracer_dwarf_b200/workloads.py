@@ -66,3 +66,33 @@ def layered_flow_case(api: FESOMTracerAdvection, nx: int, nl: int, ny: int | Non
     nlev = api.mesh_array("nlevels_nod2D")
     wet = np.arange(nl - 1)[:, None] < (nlev[None, :] - 1)
     return Case(nx, ny, nl, periodic, K, uv, w, T, S, cfl_dt(api, nx, ny, nl, uv, w), int(wet.sum()), wet)
+
+
+def ensemble_specs(members=8, seed=0, nx_range=(100, 800), nl_range=(20, 80)):
+    """Seeded member meshes of the batched configuration: nx = ny drawn from
+    nx_range, nl from nl_range, closed-wall and periodic alternating from a
+    seeded coin."""
+    rng = np.random.default_rng(seed)
+    specs = []
+    for m in range(members):
+        specs.append({"nx": int(rng.integers(nx_range[0], nx_range[1] + 1)),
+                      "nl": int(rng.integers(nl_range[0], nl_range[1] + 1)),
+                      "periodic": bool(rng.integers(0, 2)), "seed": int(seed * 1000 + 17 * m + 1)})
+    return specs
+
+
+def build_ensemble(batch, api: FESOMTracerAdvection, specs, ntracers=48):
+    """Adds one batch member per spec (mesh, velocity and ntracers seeded
+    tracer fields, alternately temperature- and salinity-like); the single-mesh
+    api builds each member's inputs.  Returns the per-member dt."""
+    dts = []
+    for s in specs:
+        api.cleanup()
+        c = layered_flow_case(api, s["nx"], s["nl"], periodic=s["periodic"], seed=s["seed"])
+        m = batch.add_member(s["nx"], s["nx"], s["nl"], ntracers, periodic=s["periodic"], node_K=c.K)
+        batch.set_velocity(m, c.uv, c.w)
+        for t in range(1, ntracers + 1):
+            batch.set_values(m, t, api.synth_tracer(seed=s["seed"] * 101 + t, kind=t % 2))
+        dts.append(c.dt)
+    api.cleanup()
+    return dts

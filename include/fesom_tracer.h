@@ -221,6 +221,57 @@ int tracer_advect_device_noalloc(int tracer_id, const double *T_dev, const doubl
                                  double *T_out_dev, double dt);
 /* Size in bytes of the static work array of tracer_advect_device_noalloc. */
 long long tracer_noalloc_scratch_bytes(void);
+/* ---- multi-member batch: no counterpart in the reference -----------------
+ * Many tracers of many ensemble members, each on its own analytic mesh (any
+ * sizes, periodic or closed), advanced together in FP32.  One step of the
+ * whole batch is one persistent cooperative kernel launch that walks every
+ * member's work phase by phase with grid-wide barriers (bounded waits: a
+ * timed-out barrier makes the step return -1); tracer_batch_steps with
+ * use_graph = 1 replays that launch from a CUDA graph.  Members are numbered
+ * from 0, tracers from 1.  Supported schemes: MUSCL+PPM or UPW1+UPW1, with or
+ * without FCT, one scheme for all tracers. */
+int tracer_batch_create(void);
+int tracer_batch_destroy(void);
+/* Adds a member on the analytic mesh of tracer_init_analytic's arguments with
+ * ntracers (a multiple of 4) tracers; returns its index or -1. */
+int tracer_batch_add_member(int nx, int ny, int nl, double Lx, double Ly, double max_depth, int periodic,
+                            int options, const int *node_K, int ntracers);
+/* dims4 = nl, nod2D, elem2D, edge2D of a member. */
+int tracer_batch_member_dims(int member, int *dims4);
+/* uv (2, nl-1, elem2D), w (nl, nod2D); values (nl-1, nod2D), FP64 host arrays. */
+int tracer_batch_set_velocity(int member, const double *uv, const double *w);
+int tracer_batch_set_values(int member, int tracer_id, const double *values);
+int tracer_batch_get_values(int member, int tracer_id, double *values);
+/* One scheme for every tracer, dt[num_members], refresh_ab = 1: valuesAB :=
+ * values each step.  Builds the work arrays and task table for the current
+ * tile. */
+int tracer_batch_configure(const char *hor, const char *ver, const char *lim, double ph, double pv, const double *dt,
+                           int refresh_ab);
+/* Tile: target wet cells per block (32..576), threads per block (64..256),
+ * persistent blocks per SM (capped by occupancy), 4-tracer batches in flight
+ * per member. */
+int tracer_batch_set_tile(int cells_per_block, int threads, int blocks_per_sm, int wave);
+int tracer_batch_get_tile(int *tile4);
+/* Times every candidate tile on steps_per_candidate steps (the tracer state
+ * is restored afterwards) and keeps the fastest; log receives one line per
+ * candidate (truncated to log_capacity). */
+int tracer_batch_autotune(int steps_per_candidate, char *log, int log_capacity);
+int tracer_batch_steps(int nsteps, int use_graph);
+/* Device time (CUDA events) of nsteps persistent steps, milliseconds. */
+int tracer_batch_time_steps(int nsteps, int use_graph, double *ms);
+/* The same steps as per-member launches of the four-to-five step kernels per
+ * 4-tracer batch (the path tracer_advect_step takes); the timed variant runs
+ * one untimed step first (nsteps + 1 in all) and returns the wall time of
+ * nsteps between device synchronisations. */
+int tracer_batch_steps_separate(int nsteps);
+int tracer_batch_time_separate(int nsteps, double *ms);
+/* info4 = members, wet cells x tracers, work-array bytes, graph captured. */
+int tracer_batch_info(long long *info4);
+/* Runs a grid barrier that waits for one block more than the grid holds:
+ * returns 1 when the wait ran out after `limit` polls and was reported (the
+ * expected outcome), 0 if it passed, -1 on a CUDA error. */
+int tracer_selftest_barrier_timeout(long long limit);
+
 /* Last error message of this thread ("" if none). */
 const char *tracer_last_error(void);
 

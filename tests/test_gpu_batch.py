@@ -1,0 +1,102 @@
+"""Multi-member batch (tracer_batch_*): the persistent one-launch step, with
+and without its CUDA graph, at any tile, gives the bits of the per-member
+separate launches; the bounded grid barrier reports a timeout instead of
+hanging; the autotuner keeps the tracer state."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture()
+def small_batch(api):
+    from fesom2_tracer_dwarf_b200.batch import TracerBatch
+    from fesom2_tracer_dwarf_b200.workloads import build_ensemble, ensemble_specs
+    specs = ensemble_specs(3, seed=5, nx_range=(12, 30), nl_range=(6, 14))
+    b = TracerBatch()
+    dts = build_ensemble(b, api, specs, ntracers=8)
+    b.configure(dts, "MUSCL", "PPM", "FCT")
+    init = [[b.get_values(m, t) for t in range(1, 9)] for m in range(3)]
+    yield b, specs, dts, init
+    b.close()
+
+
+def _state(b):
+    return [[b.get_values(m, t) for t in range(1, 9)] for m in range(len(b.members))]
+
+
+def _reset(b, init):
+    for m, fields in enumerate(init):
+        for t, v in enumerate(fields, start=1):
+            b.set_values(m, t, v)
+
+
+def _same(x, y):
+    return all(np.array_equal(a, c) for fa, fc in zip(x, y) for a, c in zip(fa, fc))
+
+
+def test_barrier_timeout_is_reported(lib):
+    assert lib.tracer_selftest_barrier_timeout(1 << 14) == 1
+
+
+def test_persistent_step_matches_separate_launches(small_batch):
+    b, specs, dts, init = small_batch
+    b.set_tile(cells_per_block=256, threads=128, blocks_per_sm=2, wave=1)
+    b.steps(3, graph=True)
+    graph = _state(b)
+    _reset(b, init)
+    b.steps(3, graph=False)
+    plain = _state(b)
+    _reset(b, init)
+    b.steps_separate(3)
+    sep = _state(b)
+    assert _same(graph, plain)
+    assert _same(graph, sep)
+    assert not _same(graph, init)
+    assert all(np.all(np.isfinite(v)) for f in graph for v in f)
+
+
+def test_tiles_do_not_change_results(small_batch):
+    b, specs, dts, init = small_batch
+    results = []
+    for tile in ({"cells_per_block": 128, "threads": 64, "blocks_per_sm": 1, "wave": 1},
+                 {"cells_per_block": 512, "threads": 256, "blocks_per_sm": 2, "wave": 2}):
+        _reset(b, init)
+        b.set_tile(**tile)
+        b.steps(2, graph=True)
+        results.append(_state(b))
+    assert _same(results[0], results[1])
+
+
+def test_member_matches_single_mesh_fp32_engine(small_batch, api):
+    """Member 0, tracer 1 against the single-mesh FP32 path (one tracer per
+    launch there, four here: same arithmetic per cell)."""
+    from fesom2_tracer_dwarf_b200.workloads import layered_flow_case
+    b, specs, dts, init = small_batch
+    b.steps(2, graph=True)
+    got = b.get_values(0, 1)
+    s = specs[0]
+    api.cleanup()
+    c = layered_flow_case(api, s["nx"], s["nl"], periodic=s["periodic"], seed=s["seed"])
+    api.set_precision("fp32")
+    api.allocate_tracers(1)
+    api.set_values(1, init[0][0])
+    api.set_scheme(1, "MUSCL", "PPM", "FCT")
+    api.set_velocity(c.uv, c.w)
+    api.set_ab_refresh(True)
+    api.advect_steps(2, dts[0])
+    ref = api.get_tracer_values(1)
+    scale = np.max(np.abs(ref))
+    assert np.max(np.abs(got - ref)) <= 1e-6 * scale
+
+
+def test_autotune_keeps_state_and_picks_a_tile(small_batch):
+    b, specs, dts, init = small_batch
+    before = _state(b)
+    log = b.autotune(1)
+    assert "best:" in log
+    t = b.tile()
+    assert t["cells_per_block"] in (256, 384, 512) and t["threads"] in (128, 256)
+    assert _same(_state(b), before)
+    b.steps(1, graph=True)
+    assert b.info()["graph"]

@@ -121,6 +121,20 @@ def test_closed_wall_bathymetry_bitwise(api, oracle, ph):
         assert_bitwise(api.get_tracer_values(2), So, f"S step {step + 1}")
 
 
+def test_deep_columns_bitwise(api, oracle):
+    """80 levels (the deepest batched configuration): columns and edges longer
+    than a quarter of a block's cell capacity, closed walls and bathymetry."""
+    nx, ny, nl = 15, 13, 80
+    K, uv, w, T, S, dt = synth_case(api, nx, ny, nl, False, 33)
+    sch = ("MUSCL", "PPM", "FCT", 1.0, 1.0)
+    m = setup_pair(api, oracle, nx, ny, nl, False, True, K, [T], uv, w, [sch], True)
+    To = T.copy(order="F")
+    for step in range(2):
+        api.advect_steps(1, dt)
+        m.step(To, To.copy(order="F"), uv, w, dt, "MUSCL", "PPM", "FCT")
+        assert_bitwise(api.get_tracer_values(1), To, f"step {step + 1}")
+
+
 def test_edge_cases_minimum_sizes(api, oracle):
     """Smallest meshes the generator allows (periodic 4x4, closed 2x2) with the
     thinnest columns (nl = 3: two layers, where PPM's end formulas overlap)."""

@@ -214,3 +214,11 @@ def test_smooth_bathymetry_marginal_is_uniform():
     # (mean |difference| (nl - 3) / 3 ~ 12 levels)
     G = K.reshape(199, 199)
     assert np.abs(np.diff(G, axis=1)).mean() < 5.0
+
+
+def test_ensemble_specs_are_seeded_and_in_range():
+    from fesom2_tracer_dwarf_b200.workloads import ensemble_specs
+    a, b = ensemble_specs(8, seed=0), ensemble_specs(8, seed=0)
+    assert a == b and len(a) == 8
+    assert all(100 <= s["nx"] <= 800 and 20 <= s["nl"] <= 80 for s in a)
+    assert {s["periodic"] for s in a} == {True, False}
