@@ -37,7 +37,7 @@ def study(members=8, tracers=48, seed=0, steps=10, tune_steps=2, nx_range=(100, 
     ms_sep = batch.time_separate(steps) / steps
     cells = info["cell_tracers"]
     out = {
-        "config": {"members": specs, "tracers_per_member": tracers, "scheme": "MUSCL+PPM+FCT", "precision": "fp32",
+        "config": {"nx_range": list(nx_range), "nl_range": list(nl_range), "members": specs, "tracers_per_member": tracers, "scheme": "MUSCL+PPM+FCT", "precision": "fp32",
                    "cell_tracers": cells, "work_bytes": batch.info()["work_bytes"], "build_seconds": build_s},
         "tile": tile,
         "persistent_graph": {"ms_per_step": ms_graph, "cell_updates_per_s": cells / (ms_graph / 1e3)},
@@ -56,8 +56,11 @@ def main():
     p.add_argument("--tracers", type=int, default=48)
     p.add_argument("--steps", type=int, default=10)
     p.add_argument("--seed", type=int, default=0)
+    p.add_argument("--nx-range", type=int, nargs=2, default=(100, 800))
+    p.add_argument("--nl-range", type=int, nargs=2, default=(20, 80))
     a = p.parse_args()
-    print(json.dumps(study(a.members, a.tracers, a.seed, a.steps), indent=1))
+    print(json.dumps(study(a.members, a.tracers, a.seed, a.steps, nx_range=tuple(a.nx_range),
+                           nl_range=tuple(a.nl_range)), indent=1))
 
 
 if __name__ == "__main__":

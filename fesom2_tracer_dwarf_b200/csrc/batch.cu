@@ -66,8 +66,9 @@ size_t batch_smem() { return kTaskSmem + smem_col<float>(kNT, 4); }
 
 // prefix: PH_COUNT rows of (ntasks + 1) running totals of each task's blocks;
 // wave_first: (nwaves + 1) first task of each wave (tasks are wave-major).
-template <int HOR, int VER, int LIM>
-__global__ void __launch_bounds__(256, 2)
+// MINB: resident 256-thread blocks per SM the register budget is cut for
+template <int HOR, int VER, int LIM, int MINB>
+__global__ void __launch_bounds__(256, MINB)
     k_batch_step(BatchTask *tasks, const int *prefix, int ntasks, const int *wave_first, int nwaves, GridBarrier *bar,
                  long long spin_limit, int refresh_ab) {
   extern __shared__ __align__(16) int smem[];
@@ -81,14 +82,17 @@ __global__ void __launch_bounds__(256, 2)
       if (ph == PH_COL2 && LIM != LIM_FCT) continue;
       const int *pre = prefix + ph * (ntasks + 1);
       const int base = pre[t0], total = pre[t1] - base;
-      int task = t0;
+      int task = t0, loaded = -1;
       for (int it = blockIdx.x; it < total; it += nb) {
         const int g = base + it;
         while (pre[task + 1] <= g) task++;
         __syncthreads();  // the previous item is done with shared memory
-        for (int q = threadIdx.x; q < (int)(sizeof(BatchTask) / sizeof(int)); q += blockDim.x)
-          reinterpret_cast<int *>(&st)[q] = reinterpret_cast<const int *>(&tasks[task])[q];
-        __syncthreads();
+        if (task != loaded) {
+          for (int q = threadIdx.x; q < (int)(sizeof(BatchTask) / sizeof(int)); q += blockDim.x)
+            reinterpret_cast<int *>(&st)[q] = reinterpret_cast<const int *>(&tasks[task])[q];
+          loaded = task;
+          __syncthreads();
+        }
         const int vblk = g - pre[task];
         switch (ph) {
           case PH_GRAD: grad_block<float, float, kNT>(st.m, st.a, vblk, work); break;
@@ -116,12 +120,21 @@ __global__ void __launch_bounds__(256, 2)
 
 using BatchKernel = void (*)(BatchTask *, const int *, int, const int *, int, GridBarrier *, long long, int);
 
-BatchKernel pick_kernel(const TracerScheme &s) {
-  if (s.hor == HOR_MUSCL && s.ver == VER_PPM && s.lim == LIM_FCT) return k_batch_step<HOR_MUSCL, VER_PPM, LIM_FCT>;
-  if (s.hor == HOR_MUSCL && s.ver == VER_PPM && s.lim == LIM_NONE) return k_batch_step<HOR_MUSCL, VER_PPM, LIM_NONE>;
-  if (s.hor == HOR_UPW1 && s.ver == VER_UPW1 && s.lim == LIM_FCT) return k_batch_step<HOR_UPW1, VER_UPW1, LIM_FCT>;
-  if (s.hor == HOR_UPW1 && s.ver == VER_UPW1 && s.lim == LIM_NONE) return k_batch_step<HOR_UPW1, VER_UPW1, LIM_NONE>;
+template <int MINB>
+BatchKernel pick_kernel_b(const TracerScheme &s) {
+  if (s.hor == HOR_MUSCL && s.ver == VER_PPM && s.lim == LIM_FCT) return k_batch_step<HOR_MUSCL, VER_PPM, LIM_FCT, MINB>;
+  if (s.hor == HOR_MUSCL && s.ver == VER_PPM && s.lim == LIM_NONE) return k_batch_step<HOR_MUSCL, VER_PPM, LIM_NONE, MINB>;
+  if (s.hor == HOR_UPW1 && s.ver == VER_UPW1 && s.lim == LIM_FCT) return k_batch_step<HOR_UPW1, VER_UPW1, LIM_FCT, MINB>;
+  if (s.hor == HOR_UPW1 && s.ver == VER_UPW1 && s.lim == LIM_NONE) return k_batch_step<HOR_UPW1, VER_UPW1, LIM_NONE, MINB>;
   return nullptr;
+}
+
+// the register budget follows the resident threads per SM the tile asks for
+BatchKernel pick_kernel(const TracerScheme &s, int threads = 256, int blocks_per_sm = 2) {
+  const int minb = std::max(2, std::min(4, (threads * blocks_per_sm + 255) / 256));
+  if (minb == 4) return pick_kernel_b<4>(s);
+  if (minb == 3) return pick_kernel_b<3>(s);
+  return pick_kernel_b<2>(s);
 }
 
 // test kernel: a barrier that waits for one block more than the grid has,
@@ -242,7 +255,7 @@ void Batch::set_tile(const BatchTile &tile) {
   CK(cudaStreamSynchronize(B.stream));
   B.release();
   B.tile = tile;
-  B.kernel = pick_kernel(B.sch);
+  B.kernel = pick_kernel(B.sch, tile.threads, tile.blocks_per_sm);
   const size_t smem = batch_smem();
   CK(cudaFuncSetAttribute(B.kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int occ = 0;
@@ -482,10 +495,10 @@ std::string Batch::autotune(int steps_per_candidate) {
   int max_batches = 0;
   for (int m = 0; m < num_members(); m++) max_batches = std::max(max_batches, B.ntr[m] / kNT);
   for (int cells : {256, 384, 512}) {
-    for (int wave : {1, 2, 4, 12}) {
+    for (int wave : {1, 2, 4}) {
       if (wave > max_batches && wave != 1) continue;
       for (int threads : {128, 256}) {
-        for (int bps : {1, 2, 4}) {
+        for (int bps : {2, 3, 4, 6}) {
           BatchTile t;
           t.cells_per_block = cells;
           t.wave = wave;
