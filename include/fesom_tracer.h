@@ -272,6 +272,12 @@ int tracer_batch_info(long long *info4);
  * expected outcome), 0 if it passed, -1 on a CUDA error. */
 int tracer_selftest_barrier_timeout(long long limit);
 
+/* Tensor-core self-test (tcgen05.mma, no counterpart in the reference):
+ * D[128 x N] = A[128 x K] * B[N x K]^T with A, B given as BF16 bit patterns
+ * (row-major) and D FP32 row-major; N, K multiples of 16 up to 256.  Returns
+ * 0, -1 on a CUDA error or bad arguments, -2 if the MMA did not complete. */
+int tracer_selftest_umma(int N, int K, const uint16_t *A, const uint16_t *B, float *D);
+
 /* Last error message of this thread ("" if none). */
 const char *tracer_last_error(void);
 
