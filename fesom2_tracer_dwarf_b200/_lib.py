@@ -103,6 +103,9 @@ SIGNATURES = {
     "tracer_batch_info": (ctypes.c_int, [_vp]),
     "tracer_selftest_barrier_timeout": (ctypes.c_int, [ctypes.c_longlong]),
     "tracer_selftest_umma": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _vp, _vp, _vp]),
+    "tracer_mlp_num_params": (ctypes.c_int, []),
+    "tracer_mlp_forward": (ctypes.c_int, [_vp, ctypes.c_longlong, _vp, _vp]),
+    "tracer_mlp_grads": (ctypes.c_int, [_vp, _vp, ctypes.c_longlong, _vp, _vp]),
     "tracer_advect_device_noalloc": (ctypes.c_int, [ctypes.c_int, _vp, _vp, _vp, ctypes.c_double]),
     "tracer_noalloc_scratch_bytes": (ctypes.c_longlong, []),
     "tracer_last_error": (ctypes.c_char_p, []),

@@ -4,6 +4,7 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 #include <vector>
 
@@ -73,10 +74,464 @@ __global__ void __launch_bounds__(128, 1)
   }
 }
 
+// ---------------------------------------------------------------------------
+// MLP 16 -> 64 -> 64 -> 1 (GELU).  Parameters (FP32 master copy, packed):
+// W1[64][16], b1[64], W2[64][64], b2[64], w3[64], b3 -- W1 and W2 also as
+// BF16 for the tensor cores.  One CTA of 128 threads handles 128-sample
+// tiles; thread m owns sample row m (TMEM lane m).
+// ---------------------------------------------------------------------------
+constexpr int kF = 16, kH = 64;
+constexpr int kOffW1 = 0, kOffB1 = kOffW1 + kH * kF, kOffW2 = kOffB1 + kH, kOffB2 = kOffW2 + kH * kH,
+              kOffW3 = kOffB2 + kH, kOffB3 = kOffW3 + kH, kParams = kOffB3 + 1;
+
+__device__ __forceinline__ float gelu(float z) { return 0.5f * z * (1.0f + erff(z * 0.70710678118654752f)); }
+__device__ __forceinline__ float gelu_grad(float z) {
+  return 0.5f * (1.0f + erff(z * 0.70710678118654752f)) + z * 0.39894228040143268f * expf(-0.5f * z * z);
+}
+
+struct MlpDev {
+  const __nv_bfloat16 *W1b, *W2b;  // [64][16], [64][64] BF16
+  const float *p;                  // FP32 packed parameters
+};
+
+// byte offsets of the shared-memory tiles (all 1024-aligned)
+struct FwdSmem {
+  static constexpr uint32_t W1 = 0, W2 = 2048, X = W2 + 8192, H1 = X + 4096, END = H1 + 16384;
+};
+struct TrainSmem {
+  static constexpr uint32_t W1 = 0, W2 = 2048, W2T = W2 + 8192, X = W2T + 8192, XT = X + 4096, H1 = XT + 4096,
+                            H1T = H1 + 16384, DZ2 = H1T + 16384, DZ2T = DZ2 + 16384, DZ1T = DZ2T + 32768,
+                            END = DZ1T + 32768;
+};
+
+__device__ __forceinline__ void st_bf16(unsigned char *base, uint32_t off, float v) {
+  *reinterpret_cast<__nv_bfloat16 *>(base + off) = __float2bfloat16_rn(v);
+}
+// 8 consecutive K elements of one row: one 16-byte store
+__device__ __forceinline__ void st_bf16x8(unsigned char *base, uint32_t off, const float *v) {
+  __align__(16) __nv_bfloat16 h[8];
+  for (int i = 0; i < 8; i++) h[i] = __float2bfloat16_rn(v[i]);
+  *reinterpret_cast<uint4 *>(base + off) = *reinterpret_cast<const uint4 *>(h);
+}
+
+__device__ __forceinline__ void load_weights(unsigned char *sm, const MlpDev &w, uint32_t oW1, uint32_t oW2,
+                                             uint32_t oW2T) {
+  for (int i = threadIdx.x; i < kH * kF; i += blockDim.x)
+    *reinterpret_cast<__nv_bfloat16 *>(sm + oW1 + umma::kmajor_offset(i / kF, i % kF, kF)) = w.W1b[i];
+  for (int i = threadIdx.x; i < kH * kH; i += blockDim.x) {
+    const int j = i / kH, k = i % kH;  // W2[j][k]: output j, input k
+    *reinterpret_cast<__nv_bfloat16 *>(sm + oW2 + umma::kmajor_offset(j, k, kH)) = w.W2b[i];
+    if (oW2T != 0xffffffffu)
+      *reinterpret_cast<__nv_bfloat16 *>(sm + oW2T + umma::kmajor_offset(k, j, kH)) = w.W2b[i];
+  }
+}
+
+// this thread's sample: 16 BF16 features as two 16-byte loads (zeros past S)
+__device__ __forceinline__ void load_sample(const __nv_bfloat16 *X, long long S, long long sample, uint4 &lo,
+                                            uint4 &hi) {
+  if (sample < S) {
+    const uint4 *p = reinterpret_cast<const uint4 *>(X + sample * kF);
+    lo = p[0];
+    hi = p[1];
+  } else {
+    lo = make_uint4(0, 0, 0, 0);
+    hi = lo;
+  }
+}
+
+__device__ __forceinline__ void mma_tiles(uint32_t tmem_d, uint32_t a, uint32_t b, int K, int N, bool accumulate) {
+  const uint32_t idesc = umma::idesc_bf16_f32(128, N), sbo = (uint32_t)(K / 8) * 128;
+  for (int s = 0; s < K / 16; s++)
+    umma::mma_bf16(tmem_d, umma::smem_desc(a + s * 256, 128, sbo), umma::smem_desc(b + s * 256, 128, sbo), idesc,
+                   (accumulate || s > 0) ? 1u : 0u);
+}
+
+// every thread waits; all agree on the outcome
+__device__ __forceinline__ bool wait_all(uint64_t *mbar, uint32_t &phase) {
+  const bool ok = umma::mbar_wait(mbar, phase, kWaitLimit);
+  phase ^= 1u;
+  umma::tc_fence_after();
+  return __syncthreads_and(ok ? 1 : 0) != 0;
+}
+
+__device__ __forceinline__ void smem_to_tc() {
+  umma::fence_async_smem();
+  umma::tc_fence_before();
+  __syncthreads();
+  umma::tc_fence_after();
+}
+
+__global__ void __launch_bounds__(128, 1)
+    k_mlp_fwd(const __nv_bfloat16 *X, long long S, MlpDev w, float *y, int *status) {
+  extern __shared__ __align__(1024) unsigned char sm[];
+  __shared__ __align__(8) uint64_t mbar;
+  __shared__ uint32_t tbase;
+  __shared__ float sb1[kH], sb2[kH], sw3[kH];
+  const int tid = threadIdx.x, warp = tid >> 5;
+  load_weights(sm, w, FwdSmem::W1, FwdSmem::W2, 0xffffffffu);
+  if (tid < kH) {
+    sb1[tid] = w.p[kOffB1 + tid];
+    sb2[tid] = w.p[kOffB2 + tid];
+    sw3[tid] = w.p[kOffW3 + tid];
+  }
+  const float b3 = w.p[kOffB3];
+  if (warp == 0) {
+    umma::tmem_alloc(&tbase, 128);
+    umma::tmem_relinquish();
+  }
+  if (tid == 0) {
+    umma::mbar_init(&mbar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  smem_to_tc();
+  const uint32_t tmem = tbase, lane = (uint32_t)(warp * 32) << 16;
+  const uint32_t D1 = tmem, D2 = tmem + 64;
+  const uint32_t aX = umma::smem_u32(sm + FwdSmem::X), aH1 = umma::smem_u32(sm + FwdSmem::H1);
+  const uint32_t aW1 = umma::smem_u32(sm + FwdSmem::W1), aW2 = umma::smem_u32(sm + FwdSmem::W2);
+  uint32_t phase = 0;
+  bool ok = true;
+  const long long ntiles = (S + 127) / 128;
+  for (long long t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
+    const long long sample = t * 128 + tid;
+    uint4 lo, hi;
+    load_sample(X, S, sample, lo, hi);
+    *reinterpret_cast<uint4 *>(sm + FwdSmem::X + umma::kmajor_offset(tid, 0, kF)) = lo;
+    *reinterpret_cast<uint4 *>(sm + FwdSmem::X + umma::kmajor_offset(tid, 8, kF)) = hi;
+    smem_to_tc();
+    if (tid == 0) {
+      mma_tiles(D1, aX, aW1, kF, kH, false);
+      umma::mma_commit(&mbar);
+    }
+    if (!(ok = wait_all(&mbar, phase))) break;
+    for (int c = 0; c < kH; c += 16) {
+      float v[16];
+      umma::tmem_ld16(D1 + lane + c, v);
+      for (int i = 0; i < 16; i++) v[i] = gelu(v[i] + sb1[c + i]);
+      st_bf16x8(sm + FwdSmem::H1, umma::kmajor_offset(tid, c, kH), v);
+      st_bf16x8(sm + FwdSmem::H1, umma::kmajor_offset(tid, c + 8, kH), v + 8);
+    }
+    smem_to_tc();
+    if (tid == 0) {
+      mma_tiles(D2, aH1, aW2, kH, kH, false);
+      umma::mma_commit(&mbar);
+    }
+    if (!(ok = wait_all(&mbar, phase))) break;
+    float acc = 0.f;
+    for (int c = 0; c < kH; c += 16) {
+      float v[16];
+      umma::tmem_ld16(D2 + lane + c, v);
+      for (int i = 0; i < 16; i++) acc += gelu(v[i] + sb2[c + i]) * sw3[c + i];
+    }
+    if (sample < S) y[sample] = acc + b3;
+    umma::tc_fence_before();
+    __syncthreads();
+    umma::tc_fence_after();
+  }
+  if (!ok) {
+    if (tid == 0) atomicExch(status, 2);
+    umma::mbar_wait(&mbar, phase ^ 1u, kWaitLimit);  // bounded: let the MMA in flight finish
+  }
+  umma::tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    umma::tc_fence_after();
+    umma::tmem_dealloc(tmem, 128);
+  }
+}
+
+__device__ __forceinline__ float warp_sum(float v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Gradients of sum_s dy[s] * y(x_s) with respect to every parameter, added
+// to grad (FP32, packed like the parameters).
+__global__ void __launch_bounds__(128, 1)
+    k_mlp_train(const __nv_bfloat16 *X, const float *dy, long long S, MlpDev w, float *grad, int *status) {
+  extern __shared__ __align__(1024) unsigned char sm[];
+  __shared__ __align__(8) uint64_t mbar;
+  __shared__ uint32_t tbase;
+  __shared__ float sb1[kH], sb2[kH], sw3[kH], gdb1[kH], gdb2[kH], gdw3[kH], gdb3;
+  const int tid = threadIdx.x, warp = tid >> 5, lid = tid & 31;
+  load_weights(sm, w, TrainSmem::W1, TrainSmem::W2, TrainSmem::W2T);
+  // padded rows 64..127 of the transposed gradient operands stay zero
+  for (int i = tid; i < 64 * 128 * 2 / 16; i += blockDim.x) {
+    reinterpret_cast<uint4 *>(sm + TrainSmem::DZ2T + 64 * 128 * 2)[i] = make_uint4(0, 0, 0, 0);
+    reinterpret_cast<uint4 *>(sm + TrainSmem::DZ1T + 64 * 128 * 2)[i] = make_uint4(0, 0, 0, 0);
+  }
+  if (tid < kH) {
+    sb1[tid] = w.p[kOffB1 + tid];
+    sb2[tid] = w.p[kOffB2 + tid];
+    sw3[tid] = w.p[kOffW3 + tid];
+    gdb1[tid] = gdb2[tid] = gdw3[tid] = 0.f;
+  }
+  if (tid == 0) gdb3 = 0.f;
+  if (warp == 0) {
+    umma::tmem_alloc(&tbase, 512);
+    umma::tmem_relinquish();
+  }
+  if (tid == 0) {
+    umma::mbar_init(&mbar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  smem_to_tc();
+  const uint32_t tmem = tbase, lane = (uint32_t)(warp * 32) << 16;
+  const uint32_t D1 = tmem, D2 = tmem + 64, DH1 = tmem + 128, DW2 = tmem + 192, DW1 = tmem + 256;
+  auto A = [&](uint32_t off) { return umma::smem_u32(sm + off); };
+  uint32_t phase = 0;
+  bool ok = true, first = true;
+  const long long ntiles = (S + 127) / 128;
+  for (long long t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
+    const long long sample = t * 128 + tid;
+    const float g = sample < S ? dy[sample] : 0.f;
+    uint4 lo, hi;
+    load_sample(X, S, sample, lo, hi);
+    *reinterpret_cast<uint4 *>(sm + TrainSmem::X + umma::kmajor_offset(tid, 0, kF)) = lo;
+    *reinterpret_cast<uint4 *>(sm + TrainSmem::X + umma::kmajor_offset(tid, 8, kF)) = hi;
+    {
+      const __nv_bfloat16 *xv = reinterpret_cast<const __nv_bfloat16 *>(&lo);
+      const __nv_bfloat16 *xw = reinterpret_cast<const __nv_bfloat16 *>(&hi);
+      for (int f = 0; f < 8; f++) {
+        *reinterpret_cast<__nv_bfloat16 *>(sm + TrainSmem::XT + umma::kmajor_offset(f, tid, 128)) = xv[f];
+        *reinterpret_cast<__nv_bfloat16 *>(sm + TrainSmem::XT + umma::kmajor_offset(f + 8, tid, 128)) = xw[f];
+      }
+    }
+    smem_to_tc();
+    if (tid == 0) {
+      mma_tiles(D1, A(TrainSmem::X), A(TrainSmem::W1), kF, kH, false);
+      umma::mma_commit(&mbar);
+    }
+    if (!(ok = wait_all(&mbar, phase))) break;
+    for (int c = 0; c < kH; c += 16) {
+      float v[16];
+      umma::tmem_ld16(D1 + lane + c, v);
+      for (int i = 0; i < 16; i++) {
+        v[i] = gelu(v[i] + sb1[c + i]);
+        st_bf16(sm + TrainSmem::H1T, umma::kmajor_offset(c + i, tid, 128), v[i]);
+      }
+      st_bf16x8(sm + TrainSmem::H1, umma::kmajor_offset(tid, c, kH), v);
+      st_bf16x8(sm + TrainSmem::H1, umma::kmajor_offset(tid, c + 8, kH), v + 8);
+    }
+    smem_to_tc();
+    if (tid == 0) {
+      mma_tiles(D2, A(TrainSmem::H1), A(TrainSmem::W2), kH, kH, false);
+      umma::mma_commit(&mbar);
+    }
+    if (!(ok = wait_all(&mbar, phase))) break;
+    // output layer and dZ2 = dy * w3 * gelu'(z2)
+    for (int c = 0; c < kH; c += 16) {
+      float v[16], dz[16];
+      umma::tmem_ld16(D2 + lane + c, v);
+      for (int i = 0; i < 16; i++) {
+        const float z = v[i] + sb2[c + i];
+        const float h2 = gelu(z);
+        dz[i] = g * sw3[c + i] * gelu_grad(z);
+        st_bf16(sm + TrainSmem::DZ2T, umma::kmajor_offset(c + i, tid, 128), dz[i]);
+        const float a = warp_sum(g * h2), b = warp_sum(dz[i]);
+        if (lid == 0) {
+          atomicAdd(&gdw3[c + i], a);
+          atomicAdd(&gdb2[c + i], b);
+        }
+      }
+      st_bf16x8(sm + TrainSmem::DZ2, umma::kmajor_offset(tid, c, kH), dz);
+      st_bf16x8(sm + TrainSmem::DZ2, umma::kmajor_offset(tid, c + 8, kH), dz + 8);
+    }
+    {
+      const float a = warp_sum(g);
+      if (lid == 0) atomicAdd(&gdb3, a);
+    }
+    smem_to_tc();
+    if (tid == 0) {
+      // dW2[j][i] += sum_m dZ2[m][j] H1[m][i];  dH1[m][i] = sum_j dZ2[m][j] W2[j][i]
+      mma_tiles(DW2, A(TrainSmem::DZ2T), A(TrainSmem::H1T), 128, kH, !first);
+      mma_tiles(DH1, A(TrainSmem::DZ2), A(TrainSmem::W2T), kH, kH, false);
+      umma::mma_commit(&mbar);
+    }
+    if (!(ok = wait_all(&mbar, phase))) break;
+    for (int c = 0; c < kH; c += 16) {
+      float dh[16], z1[16];
+      umma::tmem_ld16(DH1 + lane + c, dh);
+      umma::tmem_ld16(D1 + lane + c, z1);
+      for (int i = 0; i < 16; i++) {
+        const float dz = dh[i] * gelu_grad(z1[i] + sb1[c + i]);
+        st_bf16(sm + TrainSmem::DZ1T, umma::kmajor_offset(c + i, tid, 128), dz);
+        const float b = warp_sum(dz);
+        if (lid == 0) atomicAdd(&gdb1[c + i], b);
+      }
+    }
+    smem_to_tc();
+    if (tid == 0) {
+      // dW1[i][f] += sum_m dZ1[m][i] X[m][f]
+      mma_tiles(DW1, A(TrainSmem::DZ1T), A(TrainSmem::XT), 128, kF, !first);
+      umma::mma_commit(&mbar);
+    }
+    if (!(ok = wait_all(&mbar, phase))) break;
+    first = false;
+  }
+  if (!ok) {
+    if (tid == 0) atomicExch(status, 2);
+    umma::mbar_wait(&mbar, phase ^ 1u, kWaitLimit);  // bounded: let the MMA in flight finish
+  } else if (!first) {
+    // weight gradients: rows j (i) < 64 live in TMEM lanes 0..63 (warps 0, 1)
+    if (warp < 2) {
+      for (int c = 0; c < kH; c += 16) {
+        float v[16];
+        umma::tmem_ld16(DW2 + lane + c, v);
+        for (int i = 0; i < 16; i++) atomicAdd(&grad[kOffW2 + tid * kH + c + i], v[i]);
+      }
+      float v[16];
+      umma::tmem_ld16(DW1 + lane, v);
+      for (int i = 0; i < 16; i++) atomicAdd(&grad[kOffW1 + tid * kF + i], v[i]);
+    }
+  }
+  __syncthreads();
+  if (tid < kH) {
+    atomicAdd(&grad[kOffB1 + tid], gdb1[tid]);
+    atomicAdd(&grad[kOffB2 + tid], gdb2[tid]);
+    atomicAdd(&grad[kOffW3 + tid], gdw3[tid]);
+  }
+  if (tid == 0) atomicAdd(&grad[kOffB3], gdb3);
+  umma::tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    umma::tc_fence_after();
+    umma::tmem_dealloc(tmem, 512);
+  }
+}
+
+__global__ void k_params_to_bf16(const float *p, __nv_bfloat16 *W1b, __nv_bfloat16 *W2b) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < kH * kF + kH * kH; i += gridDim.x * blockDim.x) {
+    if (i < kH * kF) W1b[i] = __float2bfloat16_rn(p[kOffW1 + i]);
+    else W2b[i - kH * kF] = __float2bfloat16_rn(p[kOffW2 + i - kH * kF]);
+  }
+}
+
 }  // namespace
 }  // namespace fesom
 
 using namespace fesom;
+
+namespace fesom {
+
+// Device state of one MLP: FP32 parameters (and gradients, Adam moments),
+// BF16 copies of W1 and W2.
+struct MlpState {
+  float *p = nullptr, *grad = nullptr, *m1 = nullptr, *m2 = nullptr;
+  __nv_bfloat16 *W1b = nullptr, *W2b = nullptr;
+  int *status = nullptr;
+  int adam_t = 0;
+  int sms = 148;
+};
+
+static bool mlp_alloc(MlpState &s) {
+  if (cudaMalloc(&s.p, kParams * 4) != cudaSuccess || cudaMalloc(&s.grad, kParams * 4) != cudaSuccess ||
+      cudaMalloc(&s.m1, kParams * 4) != cudaSuccess || cudaMalloc(&s.m2, kParams * 4) != cudaSuccess ||
+      cudaMalloc(&s.W1b, kH * kF * 2) != cudaSuccess || cudaMalloc(&s.W2b, kH * kH * 2) != cudaSuccess ||
+      cudaMalloc(&s.status, 4) != cudaSuccess)
+    return false;
+  cudaMemset(s.m1, 0, kParams * 4);
+  cudaMemset(s.m2, 0, kParams * 4);
+  cudaMemset(s.status, 0, 4);
+  int dev = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&s.sms, cudaDevAttrMultiProcessorCount, dev);
+  return true;
+}
+static void mlp_free(MlpState &s) {
+  cudaFree(s.p); cudaFree(s.grad); cudaFree(s.m1); cudaFree(s.m2); cudaFree(s.W1b); cudaFree(s.W2b); cudaFree(s.status);
+  s = MlpState();
+}
+static MlpDev mlp_view(const MlpState &s) { return MlpDev{s.W1b, s.W2b, s.p}; }
+
+static void mlp_sync_bf16(const MlpState &s, cudaStream_t st) { k_params_to_bf16<<<8, 256, 0, st>>>(s.p, s.W1b, s.W2b); }
+
+static size_t fwd_smem() { return FwdSmem::END; }
+static size_t train_smem() { return TrainSmem::END; }
+
+// y[S] = MLP(X[S][16]) on the device (X BF16, 16-byte aligned rows)
+int mlp_forward_dev(const MlpState &s, const __nv_bfloat16 *X, long long S, float *y, cudaStream_t st) {
+  static bool attr = false;
+  if (!attr) {
+    if (cudaFuncSetAttribute(k_mlp_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fwd_smem()) != cudaSuccess)
+      return -1;
+    attr = true;
+  }
+  if (S <= 0) return 0;
+  const long long tiles = (S + 127) / 128;
+  const int grid = (int)std::min<long long>(tiles, (long long)s.sms * 4);
+  k_mlp_fwd<<<grid, 128, fwd_smem(), st>>>(X, S, mlp_view(s), y, s.status);
+  return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+// grad += d/dparams sum_s dy[s] y(X[s])
+int mlp_grads_dev(const MlpState &s, const __nv_bfloat16 *X, const float *dy, long long S, cudaStream_t st) {
+  static bool attr = false;
+  if (!attr) {
+    if (cudaFuncSetAttribute(k_mlp_train, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)train_smem()) !=
+        cudaSuccess)
+      return -1;
+    attr = true;
+  }
+  if (S <= 0) return 0;
+  const long long tiles = (S + 127) / 128;
+  const int grid = (int)std::min<long long>(tiles, (long long)s.sms);
+  k_mlp_train<<<grid, 128, train_smem(), st>>>(X, dy, S, mlp_view(s), s.grad, s.status);
+  return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+static int mlp_status(const MlpState &s) {
+  int h = 0;
+  if (cudaMemcpy(&h, s.status, 4, cudaMemcpyDeviceToHost) != cudaSuccess) return -1;
+  return h ? -2 : 0;
+}
+
+}  // namespace fesom
+
+extern "C" int tracer_mlp_num_params(void) { return fesom::kParams; }
+
+extern "C" int tracer_mlp_forward(const uint16_t *X, long long S, const float *params, float *y) {
+  if (!X || !params || !y || S < 0) return -1;
+  MlpState s;
+  __nv_bfloat16 *dX = nullptr;
+  float *dy = nullptr;
+  int rc = -1;
+  if (mlp_alloc(s) && cudaMalloc(&dX, std::max<long long>(S, 1) * kF * 2) == cudaSuccess &&
+      cudaMalloc(&dy, std::max<long long>(S, 1) * 4) == cudaSuccess &&
+      cudaMemcpy(s.p, params, kParams * 4, cudaMemcpyHostToDevice) == cudaSuccess &&
+      cudaMemcpy(dX, X, (size_t)S * kF * 2, cudaMemcpyHostToDevice) == cudaSuccess) {
+    mlp_sync_bf16(s, 0);
+    if (mlp_forward_dev(s, dX, S, dy, 0) == 0 && cudaDeviceSynchronize() == cudaSuccess &&
+        cudaMemcpy(y, dy, (size_t)S * 4, cudaMemcpyDeviceToHost) == cudaSuccess)
+      rc = mlp_status(s);
+  }
+  cudaFree(dX);
+  cudaFree(dy);
+  mlp_free(s);
+  return rc;
+}
+
+extern "C" int tracer_mlp_grads(const uint16_t *X, const float *dyv, long long S, const float *params, float *grads) {
+  if (!X || !dyv || !params || !grads || S < 0) return -1;
+  MlpState s;
+  __nv_bfloat16 *dX = nullptr;
+  float *ddy = nullptr;
+  int rc = -1;
+  if (mlp_alloc(s) && cudaMalloc(&dX, std::max<long long>(S, 1) * kF * 2) == cudaSuccess &&
+      cudaMalloc(&ddy, std::max<long long>(S, 1) * 4) == cudaSuccess &&
+      cudaMemcpy(s.p, params, kParams * 4, cudaMemcpyHostToDevice) == cudaSuccess &&
+      cudaMemcpy(dX, X, (size_t)S * kF * 2, cudaMemcpyHostToDevice) == cudaSuccess &&
+      cudaMemcpy(ddy, dyv, (size_t)S * 4, cudaMemcpyHostToDevice) == cudaSuccess &&
+      cudaMemset(s.grad, 0, kParams * 4) == cudaSuccess) {
+    mlp_sync_bf16(s, 0);
+    if (mlp_grads_dev(s, dX, ddy, S, 0) == 0 && cudaDeviceSynchronize() == cudaSuccess &&
+        cudaMemcpy(grads, s.grad, kParams * 4, cudaMemcpyDeviceToHost) == cudaSuccess)
+      rc = mlp_status(s);
+  }
+  cudaFree(dX);
+  cudaFree(ddy);
+  mlp_free(s);
+  return rc;
+}
 
 extern "C" int tracer_selftest_umma(int N, int K, const uint16_t *A, const uint16_t *B, float *D) {
   if (N < 16 || N > 256 || N % 16 || K < 16 || K > 256 || K % 16 || !A || !B || !D) return -1;

@@ -278,6 +278,17 @@ int tracer_selftest_barrier_timeout(long long limit);
  * 0, -1 on a CUDA error or bad arguments, -2 if the MMA did not complete. */
 int tracer_selftest_umma(int N, int K, const uint16_t *A, const uint16_t *B, float *D);
 
+/* ---- learned antidiffusive flux: no counterpart in the reference ----------
+ * Per-edge-level MLP 16 -> 64 -> 64 -> 1 with GELU, BF16 weights and
+ * activations on the tensor cores (tcgen05), FP32 accumulation.  Parameters
+ * are FP32, packed: W1[64][16], b1[64], W2[64][64], b2[64], w3[64], b3
+ * (tracer_mlp_num_params() floats).  Features X are BF16 bit patterns [S][16]. */
+int tracer_mlp_num_params(void);
+/* y[S] = MLP(X) (host arrays; device buffers are allocated per call). */
+int tracer_mlp_forward(const uint16_t *X, long long S, const float *params, float *y);
+/* grads = d/dparams sum_s dy[s] * y(X[s]) (host arrays). */
+int tracer_mlp_grads(const uint16_t *X, const float *dy, long long S, const float *params, float *grads);
+
 /* Last error message of this thread ("" if none). */
 const char *tracer_last_error(void);
 

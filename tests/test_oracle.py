@@ -222,3 +222,20 @@ def test_ensemble_specs_are_seeded_and_in_range():
     assert a == b and len(a) == 8
     assert all(100 <= s["nx"] <= 800 and 20 <= s["nl"] <= 80 for s in a)
     assert {s["periodic"] for s in a} == {True, False}
+
+
+def test_mlp_oracle_gradients_match_finite_differences():
+    """Unquantised CPU MLP: analytic gradients of sum dy*y against central
+    differences in FP64."""
+    import mlp_oracle as mo
+    rng = np.random.default_rng(3)
+    X = rng.standard_normal((40, mo.F))
+    dy = rng.standard_normal(40)
+    p = mo.init_params(1).astype(np.float64)
+    g = mo.grads(X, dy, p, quantize=False)
+    idx = rng.choice(mo.NPARAMS, 60, replace=False).tolist() + [mo.OFF["b3"], mo.OFF["b1"], mo.OFF["w3"]]
+    for i in idx:
+        e = np.zeros_like(p)
+        e[i] = 1e-6
+        fd = (dy @ mo.forward(X, p + e, False)[0] - dy @ mo.forward(X, p - e, False)[0]) / 2e-6
+        assert abs(fd - g[i]) <= 1e-6 * max(1.0, abs(g[i])), (i, fd, g[i])
