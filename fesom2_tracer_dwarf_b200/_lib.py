@@ -66,7 +66,7 @@ SIGNATURES = {
     "tracer_analytic_fields": (ctypes.c_int, [_vp] * 4),
     "tracer_synth_bathymetry": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_uint64, _vp]),
     "tracer_synth_velocity": (ctypes.c_int, [ctypes.c_uint64, ctypes.c_double, ctypes.c_double, ctypes.c_double,
-                                             _vp, _vp]),
+                                             ctypes.c_double, _vp, _vp]),
     "tracer_synth_bathymetry_smooth": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                                       ctypes.c_double, ctypes.c_uint64, _vp]),
     "tracer_synth_tracer": (ctypes.c_int, [ctypes.c_uint64, ctypes.c_int, _vp]),
@@ -106,6 +106,11 @@ SIGNATURES = {
     "tracer_mlp_num_params": (ctypes.c_int, []),
     "tracer_mlp_forward": (ctypes.c_int, [_vp, ctypes.c_longlong, _vp, _vp]),
     "tracer_mlp_grads": (ctypes.c_int, [_vp, _vp, ctypes.c_longlong, _vp, _vp]),
+    "tracer_learn_set": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "tracer_learn_get": (ctypes.c_int, [_vp]),
+    "tracer_learn_grad": (ctypes.c_int, [_vp]),
+    "tracer_learn_step": (ctypes.c_int, [_vp, _vp, ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_int,
+                                         ctypes.POINTER(ctypes.c_double)]),
     "tracer_advect_device_noalloc": (ctypes.c_int, [ctypes.c_int, _vp, _vp, _vp, ctypes.c_double]),
     "tracer_noalloc_scratch_bytes": (ctypes.c_longlong, []),
     "tracer_last_error": (ctypes.c_char_p, []),

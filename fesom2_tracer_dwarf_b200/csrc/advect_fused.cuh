@@ -84,6 +84,11 @@ struct FusedArgs {
   const R *vel;           // (2, S, elem)
   const R *W;             // (S, node) interfaces
   R dt, ph, pv;
+  // learned flux (FP32 only): when feat[t] is set the edge kernel writes 16
+  // BF16 features and the correction scale of every MUSCL edge cell (dense
+  // edge-schedule index)
+  __nv_bfloat16 *feat[NTMAX];
+  float *fscale[NTMAX];
   R off[NTMAX];           // storage offsets (16-bit storage)
   uint32_t seed[NTMAX];   // per-step random stream of each tracer (stochastic rounding)
   int sround;             // 1: stochastic rounding of 16-bit stores
@@ -252,6 +257,45 @@ __device__ __forceinline__ void edge_block(const DMeshT<R> &m, const FusedArgs<R
       const R ho = -(R(0.5) * (R(1) - a.ph) * cHO) - vflux * a.ph * R(0.5) * (Tmean1 + Tmean2);
       const R flo = (LIM == LIM_FCT) ? upw1_flux(vflux, ldT(a.T[t], o1, a.off[t]), ldT(a.T[t], o2, a.off[t])) : R(0);
       a.adf_h[t][o] = ho - flo;
+      if constexpr (sizeof(R) == 4 && HOR == HOR_MUSCL) {
+        if (a.feat[t]) {
+          // features in the flow's frame, in units of the local variation sig
+          const bool fwd = vflux >= R(0);
+          const R tu = fwd ? t1 : t2, td = fwd ? t2 : t1;
+          const R xu = fwd ? x1 : -x2, xd = fwd ? x2 : -x1;
+          const R face = R(0.5) * (Tmean1 + Tmean2);
+          const R sig = fabs(td - tu) + (fabs(xu) + fabs(xd)) * sixth + R(1e-6) * (fabs(tu) + fabs(td)) + R(1e-20);
+          const R inv = R(1) / sig;
+          const size_t ou = fwd ? o1 : o2;
+          const R cour = fmin(fabs(vflux) * a.dt / (m.areasvol[ou] * m.hnode_new[ou]), R(4));
+          const R gx = fwd ? gux[t] : gdx[t], gy = fwd ? guy[t] : gdy[t];
+          const R trans = (-ey * re * gx + ex * aa * gy) * inv;
+          float f[16];
+          f[0] = (float)((td - tu) * inv);
+          f[1] = (float)(xu * sixth * inv);
+          f[2] = (float)(xd * sixth * inv);
+          f[3] = (float)((face - tu) * inv);
+          f[4] = (float)cour;
+          f[5] = (float)(cour * cour);
+          f[6] = (float)(fwd ? c_lo1 : c_lo2);
+          f[7] = (float)(fwd ? c_lo2 : c_lo1);
+          f[8] = (float)k / (float)max(1, m.nl - 2);
+          f[9] = shared ? 1.0f : 0.0f;
+          f[10] = fabsf(f[0]);
+          f[11] = f[1] - f[2];
+          f[12] = (xu * xd > R(0)) ? 1.0f : -1.0f;
+          f[13] = fminf(fabsf(f[1]), fabsf(f[2]));
+          f[14] = fmaxf(-8.0f, fminf(8.0f, (float)trans));
+          f[15] = 1.0f;
+          const int cell = cm.c0 + lc;
+          __align__(16) __nv_bfloat16 h[16];
+          for (int q = 0; q < 16; q++) h[q] = __float2bfloat16_rn(f[q]);
+          uint4 *dst = reinterpret_cast<uint4 *>(a.feat[t] + (size_t)cell * 16);
+          dst[0] = reinterpret_cast<const uint4 *>(h)[0];
+          dst[1] = reinterpret_cast<const uint4 *>(h)[1];
+          a.fscale[t][cell] = (float)(-vflux * sig);
+        }
+      }
     }
   }
 }

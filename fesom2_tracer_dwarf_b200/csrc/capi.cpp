@@ -557,12 +557,13 @@ int tracer_synth_bathymetry_smooth(int nx, int ny, int periodic, int nl, double 
   });
 }
 
-int tracer_synth_velocity(uint64_t seed, double umax, double frac, double baro, double *uv, double *w) {
+int tracer_synth_velocity(uint64_t seed, double umax, double mode1, double frac, double baro, double *uv,
+                          double *w) {
   return guarded([&] {
     if (!g.mesh) return fail("no mesh");
     const MeshHost &m = *g.mesh;
     HugeArray<double> u(uv ? 0 : (size_t)2 * (m.nl - 1) * m.elem2D), ww(w ? 0 : (size_t)m.nl * m.nod2D);
-    synth_velocity(m, seed, umax, frac, baro, uv ? uv : u.data(), w ? w : ww.data());
+    synth_velocity(m, seed, umax, mode1, frac, baro, uv ? uv : u.data(), w ? w : ww.data());
     return 0;
   });
 }
@@ -874,5 +875,46 @@ int tracer_batch_info(long long *info4) {
 
 int tracer_selftest_barrier_timeout(long long limit) {
   return guarded([&] { return batch_selftest_barrier_timeout(limit); });
+}
+
+// ---------------------------------------------------------------------------
+// learned antidiffusive flux (Engine::set_learned / learn_step)
+// ---------------------------------------------------------------------------
+int tracer_learn_set(const float *params, int on) {
+  return guarded([&] {
+    if (check_ready()) return -1;
+    ensure_engine();
+    g.eng->set_learned(params, on != 0);
+    return 0;
+  });
+}
+
+int tracer_learn_get(float *params) {
+  return guarded([&] {
+    if (!params) return fail("null output");
+    if (!g.eng) return fail("no engine");
+    g.eng->get_learned(params);
+    return 0;
+  });
+}
+
+int tracer_learn_grad(float *grad) {
+  return guarded([&] {
+    if (!grad) return fail("null output");
+    if (!g.eng) return fail("no engine");
+    g.eng->get_learned_grad(grad);
+    return 0;
+  });
+}
+
+int tracer_learn_step(const double *T_in, const double *T_target, double dt, double lr, int update, int fct,
+                      double *loss) {
+  return guarded([&] {
+    if (!T_in || !T_target || !loss) return fail("null argument");
+    if (check_ready()) return -1;
+    ensure_engine();
+    *loss = g.eng->learn_step(T_in, T_target, dt, lr, update != 0, fct != 0);
+    return 0;
+  });
 }
 

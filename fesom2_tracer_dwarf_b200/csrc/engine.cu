@@ -217,6 +217,7 @@ Engine::~Engine() {
   if (!p_) return;
   cudaStreamSynchronize(p_->stream);
   release_ring(*p_);
+  learned_release(*p_);
   for (void *a : p_->allocs) cudaFree(a);
   cudaStreamDestroy(p_->stream);
   delete p_;
@@ -411,6 +412,7 @@ static void run_batch(EngineImpl &P, int first, int nt, double dt, bool refresh_
     b.rp[t] = P.rp[t];
     b.rm[t] = P.rm[t];
     b.gradn[t] = P.gradn[t];
+    if (learned_active(P) && tr.sch.hor == 1) learned_slot_buffers(P, t, &b.feat[t], &b.fscale[t]);
     b.off[t] = tr.off;
     b.seed[t] = mix32_host(P.sround_seed ^ mix32_host((uint32_t)(first + t) * 0x9e3779b9u + tr.nstep));
     tr.nstep++;

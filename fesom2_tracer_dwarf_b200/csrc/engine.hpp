@@ -59,6 +59,23 @@ class Engine {
   // Internal state, for the multi-member batch runner (batch.cu).
   EngineImpl *impl();
 
+  // Learned antidiffusive flux (FP32 engines, MUSCL tracers): the edge kernel
+  // writes 16 features per edge cell and the MLP's output, times a local
+  // scale, is added to the antidiffusive flux before the vertical and FCT
+  // kernels.  params (packed MLP parameters) = nullptr keeps the current ones.
+  void set_learned(const float *params, bool on);
+  bool learned() const;
+  void get_learned(float *params) const;
+  // gradient of the loss of the last updating learn_step (before its update)
+  void get_learned_grad(float *grad) const;
+  // One training step on tracer 0: values := T_in, one MUSCL+PPM step (with
+  // the FCT limiter when fct) and the learned correction, loss =
+  // volume-weighted mean squared difference to T_target; with update, one
+  // Adam step of rate lr on the MLP, the limiter's factors held at their
+  // forward values in the gradient.  Returns the loss before the update.
+  // Both arrays (nl-1, nod2D).
+  double learn_step(const double *T_in, const double *T_target, double dt, double lr, bool update, bool fct = false);
+
   void set_velocity(const double *uv, const double *w);
   void set_velocity_zero();
   // (Re)allocate ntr tracers, all zero, default scheme UPW1/UPW1/NONE.

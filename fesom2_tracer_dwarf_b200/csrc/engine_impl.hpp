@@ -34,13 +34,18 @@ struct BatchPtrs {
   void *rm[kBatchMax] = {};
   void *vflux = nullptr;
   void *gradn[kBatchMax] = {};
+  void *feat[kBatchMax] = {};     // learned flux: features (BF16 x 16) per edge cell
+  void *fscale[kBatchMax] = {};   // learned flux: correction scale per edge cell
   double off[kBatchMax] = {};     // storage offsets (16-bit storage)
   uint32_t seed[kBatchMax] = {};  // stochastic-rounding streams
   int sround = 0;
 };
 
+struct LearnedState;  // mlp.cu
+
 struct EngineImpl {
   MeshHost mesh;
+  LearnedState *learn = nullptr;  // learned antidiffusive flux (FP32 engines)
   std::vector<int> slot_edge;  // edge stored in each slot
   int cells_per_block = 512;   // schedule tile
   int S = 0;
@@ -161,5 +166,14 @@ void stage_pack(EngineImpl &P, double off, void *d0, void *d1, void *d2);
 void stage_unpack(EngineImpl &P, const void *s, double off);
 void storage_reoffset(EngineImpl &P, void *s, double off_old, double off_new);
 void release_ring(EngineImpl &P);
+
+// Learned flux (mlp.cu): after the edge kernel wrote features and scales,
+// adds scale x MLP(features) to the antidiffusive edge fluxes of nt tracers.
+template <typename R, typename TS>
+struct FusedArgs;
+void learned_correct_f32(EngineImpl &P, int nt, const FusedArgs<float, float> &a);
+void learned_release(EngineImpl &P);
+bool learned_active(const EngineImpl &P);
+void learned_slot_buffers(EngineImpl &P, int t, void **feat, void **scale);
 
 }  // namespace fesom

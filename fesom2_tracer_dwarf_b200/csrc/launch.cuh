@@ -65,6 +65,9 @@ void run_group(EngineImpl &P, const TracerScheme &sc, const FusedArgs<R, TS> &a)
     case 2: launch_edge<R, TS, NT, HOR_MFCT, LIM>(P, a); break;
     default: launch_edge<R, TS, NT, HOR_UPW1, LIM>(P, a); break;
   }
+  if constexpr (std::is_same<R, float>::value && std::is_same<TS, float>::value) {
+    if (a.feat[0] && sc.hor == 1) learned_correct_f32(P, NT, a);
+  }
   switch (sc.ver) {
     case 1: launch_col1<R, TS, NT, VER_PPM, LIM>(P, a); break;
     case 2: launch_col1<R, TS, NT, VER_QR4C, LIM>(P, a); break;
@@ -98,6 +101,8 @@ void launch_batch_t(EngineImpl &P, const TracerScheme &sc, int nt, const BatchPt
     a.rp[t] = (R *)b.rp[t];
     a.rm[t] = (R *)b.rm[t];
     a.gradn[t] = (R *)b.gradn[t];
+    a.feat[t] = (__nv_bfloat16 *)b.feat[t];
+    a.fscale[t] = (float *)b.fscale[t];
   }
   a.vflux = (R *)b.vflux;
   a.vel = (const R *)P.vel;

@@ -109,7 +109,7 @@ std::vector<int> synth_bathymetry(int nnodes, int nl, uint64_t seed);
 // uniform marginal on [3, nl].
 std::vector<int> synth_bathymetry_smooth(int nx, int ny, bool periodic, int nl, double corr_cells, uint64_t seed);
 
-// Seeded synthetic flow: element velocity u(k) = a1(k) U1 + f a2(k) U2 with
+// Seeded synthetic flow: element velocity u(k) = f1 a1(k) U1 + f2 a2(k) U2 with
 // U1 = curl(psi1), U2 = curl(psi2) + grad(chi) smooth periodic patterns and
 // a1, a2 the first two cosine modes of the element's own water column (zero
 // column mean), scaled to |u| <= umax.  Every edge flux then integrates to
@@ -121,11 +121,14 @@ std::vector<int> synth_bathymetry_smooth(int nx, int ny, bool periodic, int nl, 
 // fluxes sum to zero around every node only on a mesh whose edges all carry
 // edge_tri(1) on their left (build_analytic_mesh(left_oriented = true)).
 // uv: (2, nl-1, elem2D); W: (nl, nod2D).
-void synth_velocity(const MeshHost &m, uint64_t seed, double umax, double mode2_frac, double baro_frac,
-                    double *uv, double *W);
+void synth_velocity(const MeshHost &m, uint64_t seed, double umax, double mode1_frac, double mode2_frac,
+                    double baro_frac, double *uv, double *W);
 
 // Seeded tracer fields: kind 0 = temperature-like U[0,20] plus Gaussian blobs,
-// kind 1 = salinity-like 35 + N(0, 0.5).  (nl-1, nod2D); dry cells are 0.
+// kind 1 = salinity-like 35 + N(0, 0.5), kind 2 = smooth blobs and periodic
+// tanh fronts (a function of position only: the same field on any
+// resolution).  (nl-1, nod2D); dry cells are 0.  In synth_velocity, umax < 0
+// takes -umax as the amplitude itself instead of normalising the maximum.
 void synth_tracer(const MeshHost &m, uint64_t seed, int kind, double *T);
 
 // Initial fields of the analytic driver (src/fesom_analytic.F90:251-256,306-331).

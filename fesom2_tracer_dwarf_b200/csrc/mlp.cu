@@ -9,6 +9,8 @@
 #include <vector>
 
 #include "../../include/fesom_tracer.h"
+#include "advect_fused.cuh"
+#include "engine_impl.hpp"
 #include "umma.cuh"
 
 namespace fesom {
@@ -483,6 +485,243 @@ static int mlp_status(const MlpState &s) {
   int h = 0;
   if (cudaMemcpy(&h, s.status, 4, cudaMemcpyDeviceToHost) != cudaSuccess) return -1;
   return h ? -2 : 0;
+}
+
+}  // namespace fesom
+
+namespace fesom {
+
+// ---------------------------------------------------------------------------
+// learned flux inside the engine
+// ---------------------------------------------------------------------------
+struct LearnedState {
+  MlpState mlp;
+  bool on = false;
+  long long ncells = 0;  // edge cells of the dense edge schedule
+  __nv_bfloat16 *feat[kBatchMax] = {};
+  float *fscale[kBatchMax] = {}, *y[kBatchMax] = {};
+  float *dy = nullptr, *target = nullptr;
+  double *red = nullptr;  // per-block partial sums
+  double volume = 0.0;    // sum of areasvol * hnode_new over wet cells
+  float adam_b1 = 0.9f, adam_b2 = 0.999f;
+};
+
+namespace {
+
+__global__ void __launch_bounds__(kThreads) k_learn_apply(DMeshT<float> m, float *adf, const float *scale, const float *y) {
+  extern __shared__ int smem[];
+  int *s_off = smem, *s_item = smem + kMaxItemsPerBlock + 1;
+  const CellMap cm = map_cells(m.edge_sched, blockIdx.x, s_off, s_item);
+  for (int lc = threadIdx.x; lc < cm.nc; lc += blockDim.x) {
+    const int j = s_item[lc], e = cm.i0 + j, k = lc - (s_off[j] - cm.c0), cell = cm.c0 + lc;
+    adf[(size_t)e * m.S + k] += scale[cell] * y[cell];
+  }
+}
+
+// dL/dy for L = sum_n V_n (T_n - target_n)^2 / sum V after an unlimited step:
+// an edge flux f enters T_n1 with +dt/V and T_n2 with -dt/V, f = base + scale y
+// With the FCT limiter (adf, rp, rm set), the flux entering the update is
+// ae * f with the limiter's factor ae held at its forward value.
+__global__ void __launch_bounds__(kThreads) k_learn_dy(DMeshT<float> m, const float *T, const float *target,
+                                                      const float *scale, float c, const float *adf, const float *rp,
+                                                      const float *rm, float *dy) {
+  extern __shared__ int smem[];
+  int *s_off = smem, *s_item = smem + kMaxItemsPerBlock + 1;
+  const CellMap cm = map_cells(m.edge_sched, blockIdx.x, s_off, s_item);
+  for (int lc = threadIdx.x; lc < cm.nc; lc += blockDim.x) {
+    const int j = s_item[lc], e = cm.i0 + j, k = lc - (s_off[j] - cm.c0), cell = cm.c0 + lc;
+    const int2 nn = m.edge_nodes[e];
+    const size_t o1 = (size_t)nn.x * m.S + k, o2 = (size_t)nn.y * m.S + k;
+    float ae = 1.0f;
+    if (rp) {
+      const float f = adf[(size_t)e * m.S + k];
+      ae = f >= 0.0f ? fminf(1.0f, fminf(rp[o1], rm[o2])) : fminf(1.0f, fminf(rm[o1], rp[o2]));
+    }
+    dy[cell] = ae * scale[cell] * c * ((T[o1] - target[o1]) - (T[o2] - target[o2]));
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) k_learn_loss(DMeshT<float> m, const float *T, const float *target,
+                                                        double *part) {
+  extern __shared__ int smem[];
+  int *s_off = smem, *s_item = smem + kMaxItemsPerBlock + 1;
+  __shared__ double red[kThreads];
+  const CellMap cm = map_cells(m.node_sched, blockIdx.x, s_off, s_item);
+  double acc = 0.0;
+  for (int lc = threadIdx.x; lc < cm.nc; lc += blockDim.x) {
+    const int j = s_item[lc], n = cm.i0 + j, k = lc - (s_off[j] - cm.c0);
+    const size_t o = (size_t)n * m.S + k;
+    const double r = (double)T[o] - (double)target[o];
+    acc += (double)m.areasvol[o] * (double)m.hnode_new[o] * r * r;
+  }
+  red[threadIdx.x] = acc;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if ((int)threadIdx.x < s) red[threadIdx.x] += red[threadIdx.x + s];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) part[blockIdx.x] = red[0];
+}
+
+__global__ void k_adam(float *p, const float *g, float *m1, float *m2, int n, float lr, float b1, float b2, float bc1,
+                       float bc2) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const float gi = g[i];
+    const float a = b1 * m1[i] + (1.f - b1) * gi, b = b2 * m2[i] + (1.f - b2) * gi * gi;
+    m1[i] = a;
+    m2[i] = b;
+    p[i] -= lr * (a / bc1) / (sqrtf(b / bc2) + 1e-8f);
+  }
+}
+
+template <typename T>
+T *dmalloc(size_t n) {
+  void *p = nullptr;
+  CK(cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(T)));
+  return (T *)p;
+}
+
+}  // namespace
+
+void learned_release(EngineImpl &P) {
+  if (!P.learn) return;
+  LearnedState &L = *P.learn;
+  mlp_free(L.mlp);
+  for (int t = 0; t < kBatchMax; t++) {
+    cudaFree(L.feat[t]);
+    cudaFree(L.fscale[t]);
+    cudaFree(L.y[t]);
+  }
+  cudaFree(L.dy);
+  cudaFree(L.target);
+  cudaFree(L.red);
+  delete P.learn;
+  P.learn = nullptr;
+}
+
+void learned_correct_f32(EngineImpl &P, int nt, const FusedArgs<float, float> &a) {
+  LearnedState &L = *P.learn;
+  for (int t = 0; t < nt; t++) {
+    if (mlp_forward_dev(L.mlp, a.feat[t], L.ncells, L.y[t], P.stream) != 0)
+      throw std::runtime_error("learned flux: MLP forward launch failed");
+    if (P.dm32.edge_sched.nblk > 0)
+      k_learn_apply<<<P.dm32.edge_sched.nblk, kThreads, smem_edge(), P.stream>>>(P.dm32, a.adf_h[t], a.fscale[t],
+                                                                                  L.y[t]);
+    CK(cudaGetLastError());
+  }
+}
+
+// feature / scale buffers of the batch slots, for the run_batch of engine.cu
+void learned_slot_buffers(EngineImpl &P, int t, void **feat, void **scale) {
+  LearnedState &L = *P.learn;
+  if (!L.feat[t]) {
+    L.feat[t] = dmalloc<__nv_bfloat16>((size_t)L.ncells * kF);
+    L.fscale[t] = dmalloc<float>(L.ncells);
+    L.y[t] = dmalloc<float>(L.ncells);
+  }
+  *feat = L.feat[t];
+  *scale = L.fscale[t];
+}
+bool learned_active(const EngineImpl &P) { return P.learn && P.learn->on; }
+
+void Engine::set_learned(const float *params, bool on) {
+  EngineImpl &P = *p_;
+  if (P.prec != Precision::FP32) throw std::invalid_argument("the learned flux runs in the FP32 mode");
+  CK(cudaStreamSynchronize(P.stream));
+  if (!P.learn) {
+    P.learn = new LearnedState();
+    LearnedState &L = *P.learn;
+    if (!mlp_alloc(L.mlp)) throw std::runtime_error("learned flux: device allocation failed");
+    const MeshHost &M = P.mesh;
+    long long cells = 0;
+    for (int e = 0; e < M.edge2D; e++) cells += M.edge_levels(e);
+    L.ncells = cells;
+    double vol = 0.0;
+    const int L1 = M.nl - 1;
+    for (int n = 0; n < M.nod2D; n++)
+      for (int k = 0; k < M.nlev_node[n] - 1; k++)
+        vol += M.areasvol[(size_t)n * M.nl + k] * M.hnode_new[(size_t)n * L1 + k];
+    L.volume = vol;
+    L.dy = dmalloc<float>(L.ncells);
+    L.target = dmalloc<float>((size_t)M.nod2D * P.S);
+    CK(cudaMemset(L.target, 0, (size_t)M.nod2D * P.S * sizeof(float)));
+    L.red = dmalloc<double>(std::max(1, P.dm32.node_sched.nblk));
+  }
+  LearnedState &L = *P.learn;
+  if (params) {
+    CK(cudaMemcpy(L.mlp.p, params, kParams * sizeof(float), cudaMemcpyHostToDevice));
+    CK(cudaMemset(L.mlp.m1, 0, kParams * sizeof(float)));
+    CK(cudaMemset(L.mlp.m2, 0, kParams * sizeof(float)));
+    L.mlp.adam_t = 0;
+    mlp_sync_bf16(L.mlp, P.stream);
+    CK(cudaStreamSynchronize(P.stream));
+  }
+  L.on = on;
+}
+
+bool Engine::learned() const { return learned_active(*p_); }
+
+void Engine::get_learned_grad(float *grad) const {
+  if (!p_->learn) throw std::runtime_error("no learned flux");
+  CK(cudaMemcpy(grad, p_->learn->mlp.grad, kParams * sizeof(float), cudaMemcpyDeviceToHost));
+}
+
+void Engine::get_learned(float *params) const {
+  if (!p_->learn) throw std::runtime_error("no learned flux");
+  CK(cudaMemcpy(params, p_->learn->mlp.p, kParams * sizeof(float), cudaMemcpyDeviceToHost));
+}
+
+double Engine::learn_step(const double *T_in, const double *T_target, double dt, double lr, bool update, bool fct) {
+  EngineImpl &P = *p_;
+  if (!P.learn) throw std::runtime_error("no learned flux: call set_learned first");
+  if (P.tr.empty()) throw std::runtime_error("no tracers");
+  LearnedState &L = *P.learn;
+  const TracerScheme keep = P.tr[0].sch;
+  const bool keep_on = L.on;
+  TracerScheme sch;
+  sch.hor = 1;  // MUSCL
+  sch.ver = 1;  // PPM
+  sch.lim = fct ? 1 : 0;  // without FCT the state is linear in the correction
+  P.tr[0].sch = sch;
+  L.on = true;
+  try {
+    set_values(0, T_in, true);
+    step_tracer(0, dt, true);
+  } catch (...) {
+    P.tr[0].sch = keep;
+    L.on = keep_on;
+    throw;
+  }
+  P.tr[0].sch = keep;
+  L.on = keep_on;
+  stage_upload(P, T_target);
+  stage_pack(P, 0.0, L.target, nullptr, nullptr);
+  const DMeshT<float> &m = P.dm32;
+  const float *T = (const float *)P.tr[0].T;
+  k_learn_loss<<<m.node_sched.nblk, kThreads, smem_edge(), P.stream>>>(m, T, L.target, L.red);
+  CK(cudaGetLastError());
+  std::vector<double> part(std::max(1, m.node_sched.nblk));
+  CK(cudaMemcpyAsync(part.data(), L.red, part.size() * sizeof(double), cudaMemcpyDeviceToHost, P.stream));
+  if (update) {
+    k_learn_dy<<<m.edge_sched.nblk, kThreads, smem_edge(), P.stream>>>(
+        m, T, L.target, L.fscale[0], (float)(2.0 * dt / L.volume), (const float *)P.adfh[0],
+        fct ? (const float *)P.rp[0] : nullptr, fct ? (const float *)P.rm[0] : nullptr, L.dy);
+    CK(cudaGetLastError());
+    CK(cudaMemsetAsync(L.mlp.grad, 0, kParams * sizeof(float), P.stream));
+    if (mlp_grads_dev(L.mlp, L.feat[0], L.dy, L.ncells, P.stream) != 0)
+      throw std::runtime_error("learned flux: MLP backward launch failed");
+    L.mlp.adam_t++;
+    const float bc1 = 1.f - powf(L.adam_b1, (float)L.mlp.adam_t), bc2 = 1.f - powf(L.adam_b2, (float)L.mlp.adam_t);
+    k_adam<<<8, 256, 0, P.stream>>>(L.mlp.p, L.mlp.grad, L.mlp.m1, L.mlp.m2, kParams, (float)lr, L.adam_b1, L.adam_b2,
+                                   bc1, bc2);
+    CK(cudaGetLastError());
+    mlp_sync_bf16(L.mlp, P.stream);
+  }
+  CK(cudaStreamSynchronize(P.stream));
+  if (mlp_status(L.mlp) != 0) throw std::runtime_error("learned flux: a tensor-core wait timed out");
+  double s = 0.0;
+  for (double x : part) s += x;
+  return s / L.volume;
 }
 
 }  // namespace fesom

@@ -108,8 +108,8 @@ std::vector<int> synth_bathymetry_smooth(int nx, int ny, bool periodic, int nl, 
   return K;
 }
 
-void synth_velocity(const MeshHost &m, uint64_t seed, double umax, double mode2_frac, double baro_frac,
-                    double *uv, double *W) {
+void synth_velocity(const MeshHost &m, uint64_t seed, double umax, double mode1_frac, double mode2_frac,
+                    double baro_frac, double *uv, double *W) {
   const int N = m.nod2D, T = m.elem2D, E = m.edge2D, nl = m.nl, L = nl - 1;
   Rng rng(seed);
   std::vector<double> xm(N), ym(N);
@@ -163,7 +163,7 @@ void synth_velocity(const MeshHost &m, uint64_t seed, double umax, double mode2_
     // the column integral of every edge flux vanishes
     const int M = m.nlev_elem[e] - 1;
     for (int k = 0; k < M; k++) {
-      const double a1 = std::cos(kPiRef * ((double)k + 0.5) / (double)M);
+      const double a1 = mode1_frac * std::cos(kPiRef * ((double)k + 0.5) / (double)M);
       const double a2 = mode2_frac * std::cos(2.0 * kPiRef * ((double)k + 0.5) / (double)M);
       uv[2 * ((size_t)e * L + k)] += a1 * u1 + a2 * u2;
       uv[2 * ((size_t)e * L + k) + 1] += a1 * v1 + a2 * v2;
@@ -171,7 +171,8 @@ void synth_velocity(const MeshHost &m, uint64_t seed, double umax, double mode2_
   }
   double vmax = 0.0;
   for (size_t i = 0; i < nuv / 2; i++) vmax = std::max(vmax, std::hypot(uv[2 * i], uv[2 * i + 1]));
-  const double scale = vmax > 0.0 ? umax / vmax : 0.0;
+  // umax < 0: -umax is the amplitude itself (same flow on any resolution)
+  const double scale = umax < 0.0 ? -umax : (vmax > 0.0 ? umax / vmax : 0.0);
   for (size_t i = 0; i < nuv; i++) uv[i] *= scale;
 
   // horizontal divergence D(n,k) of the edge volume fluxes, with the same
@@ -224,9 +225,38 @@ void synth_tracer(const MeshHost &m, uint64_t seed, int kind, double *T) {
       }
       for (int k = 0; k < m.nlev_node[n] - 1; k++) T[(size_t)n * L + k] = 20.0 * r.uni() + blob;
     }
-  } else {
+  } else if (kind == 1) {
     for (int n = 0; n < N; n++)
       for (int k = 0; k < m.nlev_node[n] - 1; k++) T[(size_t)n * L + k] = 35.0 + 0.5 * r.normal();
+  } else {
+    // smooth, resolution-independent: Gaussian blobs plus periodic tanh fronts,
+    // weakly varying with depth
+    double bx[6], by[6], bs[6], ba[6], fk[3][2], fp[3], fa[3];
+    for (int b = 0; b < 6; b++) {
+      bx[b] = r.uni() * m.Lx; by[b] = r.uni() * m.Ly;
+      bs[b] = (0.04 + 0.06 * r.uni()) * m.Lx; ba[b] = (r.uni() < 0.5 ? -1.0 : 1.0) * (3.0 + 5.0 * r.uni());
+    }
+    for (int f = 0; f < 3; f++) {
+      fk[f][0] = (double)(1 + (int)(r.g() % 3)) * (r.uni() < 0.5 ? -1.0 : 1.0);
+      fk[f][1] = (double)(1 + (int)(r.g() % 3));
+      fp[f] = 2.0 * kPiRef * r.uni(); fa[f] = 1.0 + 2.0 * r.uni();
+    }
+    const double H = m.zbar[0] - m.zbar[m.nl - 1];
+    for (int n = 0; n < N; n++) {
+      const double x = m.coord[2 * n] * kREarth, y = m.coord[2 * n + 1] * kREarth;
+      double v = 15.0;
+      for (int b = 0; b < 6; b++) {
+        double dx = std::fabs(x - bx[b]), dy = std::fabs(y - by[b]);
+        if (m.periodic) { dx = std::min(dx, m.Lx - dx); dy = std::min(dy, m.Ly - dy); }
+        v += ba[b] * std::exp(-(dx * dx + dy * dy) / (bs[b] * bs[b]));
+      }
+      for (int f = 0; f < 3; f++)
+        v += fa[f] * std::tanh(4.0 * std::sin(2.0 * kPiRef * (fk[f][0] * x / m.Lx + fk[f][1] * y / m.Ly) + fp[f]));
+      for (int k = 0; k < m.nlev_node[n] - 1; k++) {
+        const double z = 0.5 * (m.zbar[k] + m.zbar[k + 1]);
+        T[(size_t)n * L + k] = v * (1.0 - 0.2 * (m.zbar[0] - z) / H);
+      }
+    }
   }
 }
 

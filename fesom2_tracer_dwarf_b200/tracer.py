@@ -167,12 +167,12 @@ class FESOMTracerAdvection:
                    "tracer_analytic_fields")
         return Tt, S, uv, w
 
-    def synth_velocity(self, seed=0, umax=1.0, mode2=0.5, baro=0.0):
+    def synth_velocity(self, seed=0, umax=1.0, mode2=0.5, baro=0.0, mode1=1.0):
         """Seeded layered flow (see tracer_synth_velocity): uv (2, nl-1, elem2D), w (nl, nod2D)."""
         d = self.mesh_dims()
         uv = np.zeros((2, d["nl"] - 1, d["elem2D"]), order="F")
         w = np.zeros((d["nl"], d["nod2D"]), order="F")
-        _lib.check(self.lib, self.lib.tracer_synth_velocity(seed, umax, mode2, baro, _lib.ptr(uv), _lib.ptr(w)),
+        _lib.check(self.lib, self.lib.tracer_synth_velocity(seed, umax, mode1, mode2, baro, _lib.ptr(uv), _lib.ptr(w)),
                    "tracer_synth_velocity")
         return uv, w
 

@@ -161,13 +161,15 @@ int tracer_get_stats_id(int tracer_id, double *stats4);
  * T, S (nl-1, nod2D), uv (2, nl-1, elem2D), w (nl, nod2D); any may be NULL. */
 int tracer_analytic_fields(double *T, double *S, double *uv, double *w);
 /* Seeded synthetic inputs: bathymetry K(nnodes) in [3, nl]; a layered flow
- * for the current mesh (two zero-column-mean vertical modes, the second
- * weighted by mode2_frac, plus baro_frac times a depth-independent
+ * for the current mesh (two zero-column-mean vertical modes weighted by
+ * mode1_frac and mode2_frac, plus baro_frac times a depth-independent
  * non-divergent part, which needs a left-oriented mesh; w from the discrete
- * continuity); a tracer field (kind 0 temperature-like, 1 salinity-like). */
+ * continuity; |u| scaled to umax, or multiplied by -umax when umax < 0); a
+ * tracer field (kind 0 temperature-like, 1 salinity-like, 2 smooth blobs and
+ * fronts that do not depend on the resolution). */
 int tracer_synth_bathymetry(int nnodes, int nl, uint64_t seed, int *K);
-int tracer_synth_velocity(uint64_t seed, double umax, double mode2_frac, double baro_frac, double *uv,
-                          double *w);
+int tracer_synth_velocity(uint64_t seed, double umax, double mode1_frac, double mode2_frac, double baro_frac,
+                          double *uv, double *w);
 /* Smooth seeded bathymetry of the analytic grid (tracer_analytic_nodes
  * entries): a random field of correlation length ~corr_cells cells with a
  * uniform marginal on [3, nl]. */
@@ -288,6 +290,22 @@ int tracer_mlp_num_params(void);
 int tracer_mlp_forward(const uint16_t *X, long long S, const float *params, float *y);
 /* grads = d/dparams sum_s dy[s] * y(X[s]) (host arrays). */
 int tracer_mlp_grads(const uint16_t *X, const float *dy, long long S, const float *params, float *grads);
+/* The learned flux inside the engine (precision mode 1, FP32; MUSCL
+ * tracers): set the parameters (NULL keeps them) and switch it on or off.  On,
+ * every MUSCL edge flux becomes HO - LO + scale * MLP(features) before the
+ * vertical fluxes and the unchanged FCT limiter.  A precision change drops it. */
+int tracer_learn_set(const float *params, int on);
+int tracer_learn_get(float *params);
+/* Gradient of the loss of the last updating tracer_learn_step, taken before
+ * that step's parameter update. */
+int tracer_learn_grad(float *grad);
+/* One training step on tracer 1 (see Engine::learn_step): values := T_in,
+ * one MUSCL+PPM step (FCT-limited when fct = 1) with the learned correction,
+ * *loss = volume-weighted mean squared difference to T_target; update = 1
+ * applies one Adam step of rate lr (the limiter's factors held at their
+ * forward values in the gradient).  T_in, T_target (nl-1, nod2D). */
+int tracer_learn_step(const double *T_in, const double *T_target, double dt, double lr, int update, int fct,
+                      double *loss);
 
 /* Last error message of this thread ("" if none). */
 const char *tracer_last_error(void);
