@@ -62,7 +62,12 @@ def parse():
     p.add_argument("--e2e-steps", type=int, default=5)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--precision", default="fp64", choices=["fp64", "fp32", "bf16", "fp16"])
-    return p.parse_args()
+    p.add_argument("--learned", action="store_true",
+                   help="FP32 with the learned antidiffusive flux (shipped parameters) ahead of FCT")
+    a = p.parse_args()
+    if a.learned:
+        a.precision = "fp32"
+    return a
 
 
 def workload_name(nx, nl):
@@ -239,6 +244,11 @@ def run_ours(args):
         api.set_scheme(t, "MUSCL", "PPM", "FCT")
     api.set_velocity(uv, w)
     api.set_ab_refresh(True)
+    if args.learned:
+        from fesom2_tracer_dwarf_b200.learned import trained_params
+        params = trained_params()
+        if api.lib.tracer_learn_set(params.ctypes.data_as(ctypes.c_void_p), 1) != 0:
+            raise RuntimeError(api.lib.tracer_last_error().decode())
     api.advect_steps(args.warmup, dt)
     launches_per_step = api.lib.tracer_launches_per_step()
     dev_bytes = api.lib.tracer_device_bytes()
@@ -322,7 +332,9 @@ def run_ours(args):
             "metric": "tracer cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": DTYPE[args.precision], "data": "synthetic",
-            "config": {"workload": workload_name(args.nx, args.nl), "wet_cells": cells, "tracers": 2,
+            "config": {"workload": workload_name(args.nx, args.nl) + (", learned antidiffusive flux (MLP on "
+                                                                       "tcgen05) ahead of FCT" if args.learned else ""),
+                       "wet_cells": cells, "tracers": 2,
                        "dt_s": dt, "parallelism": f"replicas x{world}",
                        "l2": f"inputs larger than L2 ({dev_bytes / 1e9:.1f} GB resident vs 0.13 GB L2)"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",

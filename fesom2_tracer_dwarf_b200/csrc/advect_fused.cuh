@@ -336,16 +336,22 @@ __device__ __forceinline__ void col1_block(const DMeshT<R> &m, const FusedArgs<R
   for (int lc = threadIdx.x; lc < cm.nc; lc += blockDim.x) {
     const int j = s_item[lc], n = cm.i0 + j, k = lc - (s_off[j] - cm.c0), nz = k + 1;
     if (LIM == LIM_FCT) {
-      R acc[NTMAX];
-      for (int t = 0; t < NT; t++) acc[t] = R(0);
+      R acc[NTMAX], tself[NTMAX];
+      const size_t on = (size_t)n * S + k;
+      for (int t = 0; t < NT; t++) {
+        acc[t] = R(0);
+        tself[t] = ldT(a.T[t], on, a.off[t]);
+      }
       for (int p = m.ne_ptr[n]; p < m.ne_ptr[n + 1]; p++) {
         const int4 q = m.ne4[p];
         if (nz > q.z) continue;
         const bool second = q.x & 1;
         const R vf = a.vflux[(size_t)(q.x >> 1) * S + k];
-        const size_t o1 = (size_t)(second ? q.y : n) * S + k, o2 = (size_t)(second ? n : q.y) * S + k;
+        const size_t oo = (size_t)q.y * S + k;  // the edge's other node
         for (int t = 0; t < NT; t++) {
-          const R F = upw1_flux(vf, ldT(a.T[t], o1, a.off[t]), ldT(a.T[t], o2, a.off[t]));
+          const R to = ldT(a.T[t], oo, a.off[t]);
+          // upw1_flux(vf, T(first node), T(second node))
+          const R F = second ? upw1_flux(vf, to, tself[t]) : upw1_flux(vf, tself[t], to);
           acc[t] = second ? acc[t] - F : acc[t] + F;
         }
       }
@@ -688,21 +694,31 @@ __device__ __forceinline__ void col3_block(const DMeshT<R> &m, const FusedArgs<R
       }
       dh[t] = R(0);
     }
+    R rps[NTMAX], rms[NTMAX];
+    if (LIM == LIM_FCT)
+      for (int t = 0; t < NT; t++) {
+        rps[t] = a.rp[t][o];
+        rms[t] = a.rm[t][o];
+      }
     for (int p = m.ne_ptr[n]; p < m.ne_ptr[n + 1]; p++) {
       const int4 q = m.ne4[p];
       if (nz > q.z) continue;
       const bool second = q.x & 1;
-      const size_t o1 = (size_t)(second ? q.y : n) * S + k, o2 = (size_t)(second ? n : q.y) * S + k;
+      const size_t oo = (size_t)q.y * S + k;  // the edge's other node
       for (int t = 0; t < NT; t++) {
         R f = a.adf_h[t][(size_t)(q.x >> 1) * S + k];
         if (LIM == LIM_FCT) {
+          // r+/- at the edge's first (o1) and second (o2) node
+          const R rpo = a.rp[t][oo], rmo = a.rm[t][oo];
+          const R rp1 = second ? rpo : rps[t], rm1 = second ? rmo : rms[t];
+          const R rp2 = second ? rps[t] : rpo, rm2 = second ? rms[t] : rmo;
           R ae = R(1);
           if (f >= R(0)) {
-            ae = fmin2(ae, a.rp[t][o1]);
-            ae = fmin2(ae, a.rm[t][o2]);
+            ae = fmin2(ae, rp1);
+            ae = fmin2(ae, rm2);
           } else {
-            ae = fmin2(ae, a.rm[t][o1]);
-            ae = fmin2(ae, a.rp[t][o2]);
+            ae = fmin2(ae, rm1);
+            ae = fmin2(ae, rp2);
           }
           f = ae * f;
         }
