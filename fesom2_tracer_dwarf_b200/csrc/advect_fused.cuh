@@ -342,7 +342,9 @@ __device__ __forceinline__ void col1_block(const DMeshT<R> &m, const FusedArgs<R
         acc[t] = R(0);
         tself[t] = ldT(a.T[t], on, a.off[t]);
       }
-      for (int p = m.ne_ptr[n]; p < m.ne_ptr[n + 1]; p++) {
+#pragma unroll 4
+  #pragma unroll 4
+    for (int p = m.ne_ptr[n]; p < m.ne_ptr[n + 1]; p++) {
         const int4 q = m.ne4[p];
         if (nz > q.z) continue;
         const bool second = q.x & 1;
@@ -532,7 +534,9 @@ __device__ __forceinline__ void col2_block(const DMeshT<R> &m, const FusedArgs<R
         tmx[t] = fmax2(l, tt);
         tmn[t] = fmin2(l, tt);
       }
-      for (int p = m.ne_ptr[n]; p < m.ne_ptr[n + 1]; p++) {
+#pragma unroll 4
+  #pragma unroll 4
+    for (int p = m.ne_ptr[n]; p < m.ne_ptr[n + 1]; p++) {
         const int4 q = m.ne4[p];
         if (nz > q.z) continue;
         const size_t o = (size_t)q.y * S + k;
@@ -597,6 +601,7 @@ __device__ __forceinline__ void col2_block(const DMeshT<R> &m, const FusedArgs<R
       fp[t] = R(0) + (fmax2(R(0), av[k]) + fmax2(R(0), -av[k + 1]));
       fm[t] = R(0) + (fmin2(R(0), av[k]) + fmin2(R(0), -av[k + 1]));
     }
+#pragma unroll 4
     for (int p = m.ne_ptr[n]; p < m.ne_ptr[n + 1]; p++) {
       const int4 q = m.ne4[p];
       if (nz > q.z) continue;
@@ -700,6 +705,7 @@ __device__ __forceinline__ void col3_block(const DMeshT<R> &m, const FusedArgs<R
         rps[t] = a.rp[t][o];
         rms[t] = a.rm[t][o];
       }
+#pragma unroll 4
     for (int p = m.ne_ptr[n]; p < m.ne_ptr[n + 1]; p++) {
       const int4 q = m.ne4[p];
       if (nz > q.z) continue;

@@ -1,5 +1,5 @@
 // Learned antidiffusive edge flux: a per-edge-level MLP (16 -> 64 -> 64 -> 1,
-// GELU, BF16 weights and activations, FP32 accumulation) on the fifth-
+// GELU (tanh form), BF16 weights and activations, FP32 accumulation) on the fifth-
 // generation tensor cores (tcgen05.mma, accumulators in TMEM).
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
@@ -86,9 +86,22 @@ constexpr int kF = 16, kH = 64;
 constexpr int kOffW1 = 0, kOffB1 = kOffW1 + kH * kF, kOffW2 = kOffB1 + kH, kOffB2 = kOffW2 + kH * kH,
               kOffW3 = kOffB2 + kH, kOffB3 = kOffW3 + kH, kParams = kOffB3 + 1;
 
-__device__ __forceinline__ float gelu(float z) { return 0.5f * z * (1.0f + erff(z * 0.70710678118654752f)); }
+// GELU in its tanh form (Hendrycks & Gimpel 2016),
+// g(z) = z/2 (1 + tanh(c (z + 0.044715 z^3))), c = sqrt(2/pi), with the
+// hardware tanh approximation
+__device__ __forceinline__ float tanh_fast(float x) {
+  float y;
+  asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+constexpr float kGeluC = 0.7978845608028654f, kGeluA = 0.044715f;
+__device__ __forceinline__ float gelu(float z) {
+  const float t = tanh_fast(kGeluC * (z + kGeluA * z * z * z));
+  return 0.5f * z * (1.0f + t);
+}
 __device__ __forceinline__ float gelu_grad(float z) {
-  return 0.5f * (1.0f + erff(z * 0.70710678118654752f)) + z * 0.39894228040143268f * expf(-0.5f * z * z);
+  const float t = tanh_fast(kGeluC * (z + kGeluA * z * z * z));
+  return 0.5f * (1.0f + t) + 0.5f * z * (1.0f - t * t) * kGeluC * (1.0f + 3.0f * kGeluA * z * z);
 }
 
 struct MlpDev {

@@ -18,9 +18,6 @@ OFF = {"W1": 0, "b1": H * F, "W2": H * F + H, "b2": H * F + H + H * H, "w3": H *
        "b3": H * F + 3 * H + H * H}
 NPARAMS = H * F + 3 * H + H * H + 1
 
-_erf = np.vectorize(math.erf)
-
-
 def bf16(x):
     """Round-to-nearest-even to BF16, returned as float64."""
     u = np.ascontiguousarray(np.asarray(x, dtype=np.float32)).view(np.uint32)
@@ -34,12 +31,17 @@ def bf16_bits(x):
     return ((u + r) >> 16).astype(np.uint16)
 
 
+C_GELU, A_GELU = math.sqrt(2.0 / math.pi), 0.044715
+
+
 def gelu(z):
-    return 0.5 * z * (1.0 + _erf(z / math.sqrt(2.0)))
+    """GELU, tanh form (Hendrycks & Gimpel 2016), as the kernels evaluate it."""
+    return 0.5 * z * (1.0 + np.tanh(C_GELU * (z + A_GELU * z ** 3)))
 
 
 def gelu_grad(z):
-    return 0.5 * (1.0 + _erf(z / math.sqrt(2.0))) + z * np.exp(-0.5 * z * z) / math.sqrt(2.0 * math.pi)
+    t = np.tanh(C_GELU * (z + A_GELU * z ** 3))
+    return 0.5 * (1.0 + t) + 0.5 * z * (1.0 - t * t) * C_GELU * (1.0 + 3.0 * A_GELU * z * z)
 
 
 def unpack(p):

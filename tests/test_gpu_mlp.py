@@ -46,9 +46,11 @@ def test_mlp_forward_matches_cpu(lib, S):
     y = np.zeros(S, dtype=np.float32)
     assert lib.tracer_mlp_forward(X.ctypes.data, S, p.ctypes.data, y.ctypes.data) == 0
     ref, _ = mo.forward(from_bf16_bits(X), p)
-    err = np.abs(y - ref) / (1e-3 + np.abs(ref))
-    # BF16 rounding of the hidden activation can flip on FP32-vs-FP64 ties
-    assert np.quantile(err, 0.999) < 1e-3 and err.max() < 2e-2, err.max()
+    # error relative to the output's scale: the kernels' hardware tanh
+    # (tanh.approx.f32) is good to about 2^-11, and the BF16 rounding of the
+    # hidden activation can flip on the resulting differences
+    err = np.abs(y - ref) / max(np.sqrt(np.mean(ref ** 2)), 1e-30)
+    assert np.quantile(err, 0.999) < 1e-2 and err.max() < 5e-2, (np.quantile(err, 0.999), err.max())
 
 
 @pytest.mark.parametrize("S", [128, 777, 20000])
