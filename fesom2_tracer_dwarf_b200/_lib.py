@@ -98,8 +98,8 @@ SIGNATURES = {
     "tracer_batch_autotune": (ctypes.c_int, [ctypes.c_int, ctypes.c_char_p, ctypes.c_int]),
     "tracer_batch_steps": (ctypes.c_int, [ctypes.c_int, ctypes.c_int]),
     "tracer_batch_time_steps": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),
-    "tracer_batch_steps_separate": (ctypes.c_int, [ctypes.c_int]),
-    "tracer_batch_time_separate": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),
+    "tracer_batch_steps_separate": (ctypes.c_int, [ctypes.c_int, ctypes.c_int]),
+    "tracer_batch_time_separate": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),
     "tracer_batch_info": (ctypes.c_int, [_vp]),
     "tracer_selftest_barrier_timeout": (ctypes.c_int, [ctypes.c_longlong]),
     "tracer_selftest_umma": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _vp, _vp, _vp]),

@@ -90,12 +90,13 @@ class TracerBatch:
                    "tracer_batch_time_steps")
         return ms.value
 
-    def steps_separate(self, n):
-        _lib.check(self.lib, self.lib.tracer_batch_steps_separate(n), "tracer_batch_steps_separate")
+    def steps_separate(self, n, graph=False):
+        _lib.check(self.lib, self.lib.tracer_batch_steps_separate(n, int(bool(graph))), "tracer_batch_steps_separate")
 
-    def time_separate(self, n):
+    def time_separate(self, n, graph=False):
         ms = ctypes.c_double()
-        _lib.check(self.lib, self.lib.tracer_batch_time_separate(n, ctypes.byref(ms)), "tracer_batch_time_separate")
+        _lib.check(self.lib, self.lib.tracer_batch_time_separate(n, int(bool(graph)), ctypes.byref(ms)),
+                   "tracer_batch_time_separate")
         return ms.value
 
     def info(self):

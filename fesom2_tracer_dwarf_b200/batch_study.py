@@ -33,8 +33,8 @@ def study(members=8, tracers=48, seed=0, steps=10, tune_steps=2, nx_range=(100, 
     batch.steps(2, graph=True)  # warm-up, graph capture
     ms_graph = batch.time_steps(steps, graph=True) / steps
     ms_plain = batch.time_steps(steps, graph=False) / steps
-    batch.steps_separate(1)
     ms_sep = batch.time_separate(steps) / steps
+    ms_sep_graph = batch.time_separate(steps, graph=True) / steps
     cells = info["cell_tracers"]
     out = {
         "config": {"nx_range": list(nx_range), "nl_range": list(nl_range), "members": specs, "tracers_per_member": tracers, "scheme": "MUSCL+PPM+FCT", "precision": "fp32",
@@ -43,6 +43,7 @@ def study(members=8, tracers=48, seed=0, steps=10, tune_steps=2, nx_range=(100, 
         "persistent_graph": {"ms_per_step": ms_graph, "cell_updates_per_s": cells / (ms_graph / 1e3)},
         "persistent_no_graph": {"ms_per_step": ms_plain, "cell_updates_per_s": cells / (ms_plain / 1e3)},
         "separate_launches": {"ms_per_step": ms_sep, "cell_updates_per_s": cells / (ms_sep / 1e3)},
+        "separate_launches_graph": {"ms_per_step": ms_sep_graph, "cell_updates_per_s": cells / (ms_sep_graph / 1e3)},
         "speedup_vs_separate": ms_sep / ms_graph,
         "autotune_log": log.splitlines(),
     }

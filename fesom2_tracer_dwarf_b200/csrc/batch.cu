@@ -169,8 +169,24 @@ struct BatchImpl {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t graph_exec = nullptr;
   long long spin_limit = 1ll << 24;
+  // separate per-member launches captured as one graph of two steps
+  cudaGraph_t sep_graph = nullptr;
+  cudaGraphExec_t sep_exec = nullptr;
+  std::vector<cudaEvent_t> sep_events;
 
-  ~BatchImpl() { release(); if (stream) cudaStreamDestroy(stream); }
+  ~BatchImpl() {
+    release();
+    release_sep();
+    if (stream) cudaStreamDestroy(stream);
+  }
+  void release_sep() {
+    if (sep_exec) cudaGraphExecDestroy(sep_exec);
+    if (sep_graph) cudaGraphDestroy(sep_graph);
+    sep_exec = nullptr;
+    sep_graph = nullptr;
+    for (auto e : sep_events) cudaEventDestroy(e);
+    sep_events.clear();
+  }
 
   void release_graph() {
     if (graph_exec) cudaGraphExecDestroy(graph_exec);
@@ -443,30 +459,78 @@ double Batch::time_steps(int nsteps, bool use_graph) {
 
 // The separate path uses the member engines' own work arrays; the batch's are
 // released meanwhile (device memory) and rebuilt with the task table after.
-void Batch::step_separate(int nsteps) {
+// Members launch on their own streams; with use_graph the launches of two
+// steps (so that every engine's buffer ping-pong returns to where it started)
+// are captured once as a graph forked from and joined into the batch stream.
+namespace {
+void separate_steps_direct(BatchImpl &B, int nsteps) {
+  for (int s = 0; s < nsteps; s++)
+    for (size_t m = 0; m < B.members.size(); m++) B.members[m]->step(B.dt[m], B.refresh_ab);
+}
+
+void capture_separate(BatchImpl &B) {
+  if (B.sep_exec) return;
+  const size_t M = B.members.size();
+  B.sep_events.resize(M + 1);
+  for (auto &e : B.sep_events) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  CK(cudaStreamBeginCapture(B.stream, cudaStreamCaptureModeRelaxed));
+  CK(cudaEventRecord(B.sep_events[M], B.stream));
+  for (size_t m = 0; m < M; m++) CK(cudaStreamWaitEvent((cudaStream_t)B.members[m]->stream(), B.sep_events[M], 0));
+  separate_steps_direct(B, 2);
+  for (size_t m = 0; m < M; m++) {
+    CK(cudaEventRecord(B.sep_events[m], (cudaStream_t)B.members[m]->stream()));
+    CK(cudaStreamWaitEvent(B.stream, B.sep_events[m], 0));
+  }
+  cudaGraph_t g = nullptr;
+  CK(cudaStreamEndCapture(B.stream, &g));
+  B.sep_graph = g;
+  CK(cudaGraphInstantiate(&B.sep_exec, g, 0));
+}
+
+// nsteps separate steps (graph-replayed in pairs when use_graph)
+void separate_steps(BatchImpl &B, int nsteps, bool use_graph) {
+  if (!use_graph) {
+    separate_steps_direct(B, nsteps);
+    return;
+  }
+  for (int s = 0; s + 1 < nsteps; s += 2) CK(cudaGraphLaunch(B.sep_exec, B.stream));
+  if (nsteps % 2) {
+    CK(cudaStreamSynchronize(B.stream));
+    separate_steps_direct(B, 1);
+  }
+}
+}  // namespace
+
+void Batch::step_separate(int nsteps, bool use_graph) {
   BatchImpl &B = *p_;
   CK(cudaStreamSynchronize(B.stream));
   B.release();
-  for (int s = 0; s < nsteps; s++)
-    for (int m = 0; m < num_members(); m++) B.members[m]->step(B.dt[m], B.refresh_ab);
+  // one direct step allocates the engines' work arrays and kernel attributes
+  // before any capture
+  const int first = nsteps > 0 ? 1 : 0;
+  separate_steps_direct(B, first);
+  CK(cudaDeviceSynchronize());
+  if (use_graph) capture_separate(B);
+  separate_steps(B, nsteps - first, use_graph);
+  CK(cudaDeviceSynchronize());
+  B.release_sep();
   for (auto &m : B.members) m->release_work();
   set_tile(B.tile);
 }
 
-double Batch::time_separate(int nsteps) {
+double Batch::time_separate(int nsteps, bool use_graph) {
   BatchImpl &B = *p_;
-  // every member engine launches on its own stream (members may overlap on
-  // the GPU); host time between two device-wide synchronisations
   CK(cudaStreamSynchronize(B.stream));
   B.release();
   // one untimed step allocates the engines' work arrays
-  for (int m = 0; m < num_members(); m++) B.members[m]->step(B.dt[m], B.refresh_ab);
+  separate_steps_direct(B, 1);
   CK(cudaDeviceSynchronize());
+  if (use_graph) capture_separate(B);
   const auto t0 = std::chrono::steady_clock::now();
-  for (int s = 0; s < nsteps; s++)
-    for (int m = 0; m < num_members(); m++) B.members[m]->step(B.dt[m], B.refresh_ab);
+  separate_steps(B, nsteps, use_graph);
   CK(cudaDeviceSynchronize());
   const auto t1 = std::chrono::steady_clock::now();
+  B.release_sep();
   for (auto &m : B.members) m->release_work();
   set_tile(B.tile);
   return std::chrono::duration<double, std::milli>(t1 - t0).count();

@@ -53,9 +53,12 @@ class Batch {
   void step(int nsteps, bool use_graph);
   // Device time of nsteps (CUDA events on the batch stream), milliseconds.
   double time_steps(int nsteps, bool use_graph);
-  // The same steps as separate per-member, per-batch kernel launches.
-  void step_separate(int nsteps);
-  double time_separate(int nsteps);
+  // The same steps as separate per-member, per-batch kernel launches on the
+  // members' streams; with use_graph those launches are replayed from a CUDA
+  // graph (two steps per graph).  The timed variant runs one untimed step
+  // first and returns the host time of nsteps between device syncs.
+  void step_separate(int nsteps, bool use_graph = false);
+  double time_separate(int nsteps, bool use_graph = false);
 
   // Times candidate tiles (steps_per_candidate steps each, from copies of the
   // current tracer state, which is restored afterwards) and keeps the

@@ -835,17 +835,18 @@ int tracer_batch_time_steps(int nsteps, int use_graph, double *ms) {
   });
 }
 
-int tracer_batch_steps_separate(int nsteps) {
+int tracer_batch_steps_separate(int nsteps, int use_graph) {
   return guarded([&] {
-    batch().step_separate(nsteps);
+    if (nsteps < 0) return fail("nsteps < 0");
+    batch().step_separate(nsteps, use_graph != 0);
     return 0;
   });
 }
 
-int tracer_batch_time_separate(int nsteps, double *ms) {
+int tracer_batch_time_separate(int nsteps, int use_graph, double *ms) {
   return guarded([&] {
     if (nsteps < 1 || !ms) return fail("nsteps < 1 or null output");
-    *ms = batch().time_separate(nsteps);
+    *ms = batch().time_separate(nsteps, use_graph != 0);
     return 0;
   });
 }

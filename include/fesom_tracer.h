@@ -262,11 +262,13 @@ int tracer_batch_steps(int nsteps, int use_graph);
 /* Device time (CUDA events) of nsteps persistent steps, milliseconds. */
 int tracer_batch_time_steps(int nsteps, int use_graph, double *ms);
 /* The same steps as per-member launches of the four-to-five step kernels per
- * 4-tracer batch (the path tracer_advect_step takes); the timed variant runs
- * one untimed step first (nsteps + 1 in all) and returns the wall time of
- * nsteps between device synchronisations. */
-int tracer_batch_steps_separate(int nsteps);
-int tracer_batch_time_separate(int nsteps, double *ms);
+ * 4-tracer batch (the path tracer_advect_step takes) on the members' own
+ * streams; use_graph = 1 replays them from a CUDA graph of two steps forked
+ * from and joined into the batch's stream.  The timed variant runs one
+ * untimed step first (nsteps + 1 in all) and returns the wall time of nsteps
+ * between device synchronisations. */
+int tracer_batch_steps_separate(int nsteps, int use_graph);
+int tracer_batch_time_separate(int nsteps, int use_graph, double *ms);
 /* info4 = members, wet cells x tracers, work-array bytes, graph captured. */
 int tracer_batch_info(long long *info4);
 /* Runs a grid barrier that waits for one block more than the grid holds:

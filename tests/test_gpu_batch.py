@@ -50,8 +50,12 @@ def test_persistent_step_matches_separate_launches(small_batch):
     _reset(b, init)
     b.steps_separate(3)
     sep = _state(b)
+    _reset(b, init)
+    b.steps_separate(3, graph=True)
+    sep_graph = _state(b)
     assert _same(graph, plain)
     assert _same(graph, sep)
+    assert _same(graph, sep_graph)
     assert not _same(graph, init)
     assert all(np.all(np.isfinite(v)) for f in graph for v in f)
 
