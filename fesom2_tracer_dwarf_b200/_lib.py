@@ -12,7 +12,7 @@ from pathlib import Path
 import numpy as np
 
 PKG_DIR = Path(__file__).resolve().parent
-LIB_PATH = PKG_DIR / "lib" / "libfesom_tracer.so"
+LIB_PATH = Path(os.environ.get("FESOM_TRACER_LIB", PKG_DIR / "lib" / "libfesom_tracer.so"))
 
 _c_int_p = ctypes.POINTER(ctypes.c_int)
 _c_double_p = ctypes.POINTER(ctypes.c_double)

@@ -31,6 +31,26 @@ namespace fesom {
 
 constexpr int NTMAX = 4;
 constexpr int kThreads = 256;
+// resident 256-thread blocks per SM each step kernel's register budget is
+// cut for (4 = 64 registers, 5 = 48, 6 = 40).  Measured on the FP64 plain
+// step at 1000x1000x64: more resident warps hide more gather latency than
+// the extra spills cost, up to these values (k_col1's shared memory allows
+// no more than 5 blocks anyway).  Build-time tuning knobs.
+#ifndef FESOM_MINB_EDGE
+#define FESOM_MINB_EDGE 5
+#endif
+#ifndef FESOM_MINB_COL1
+#define FESOM_MINB_COL1 5
+#endif
+#ifndef FESOM_MINB_COL2
+#define FESOM_MINB_COL2 6
+#endif
+#ifndef FESOM_MINB_COL3
+#define FESOM_MINB_COL3 6
+#endif
+#ifndef FESOM_MINB_GRAD
+#define FESOM_MINB_GRAD 5
+#endif
 constexpr int kCellsPerBlock = 512;      // schedule target: wet cells per block
 constexpr int kMaxCellsPerBlock = 576;   // upper bound (target + deepest column)
 constexpr int kMaxItemsPerBlock = 512;
@@ -154,7 +174,7 @@ __device__ __forceinline__ void grad_block(const DMeshT<R> &m, const FusedArgs<R
 }
 
 template <typename R, typename TS, int NT>
-__global__ void __launch_bounds__(kThreads) k_grad(DMeshT<R> m, FusedArgs<R, TS> a) {
+__global__ void __launch_bounds__(kThreads, FESOM_MINB_GRAD) k_grad(DMeshT<R> m, FusedArgs<R, TS> a) {
   extern __shared__ int smem[];
   grad_block<R, TS, NT>(m, a, blockIdx.x, smem);
 }
@@ -301,7 +321,7 @@ __device__ __forceinline__ void edge_block(const DMeshT<R> &m, const FusedArgs<R
 }
 
 template <typename R, typename TS, int NT, int HOR, int LIM>
-__global__ void __launch_bounds__(kThreads, 4) k_edge(DMeshT<R> m, FusedArgs<R, TS> a) {
+__global__ void __launch_bounds__(kThreads, FESOM_MINB_EDGE) k_edge(DMeshT<R> m, FusedArgs<R, TS> a) {
   extern __shared__ int smem[];
   edge_block<R, TS, NT, HOR, LIM>(m, a, blockIdx.x, smem);
 }
@@ -502,7 +522,7 @@ __device__ __forceinline__ void col1_block(const DMeshT<R> &m, const FusedArgs<R
 }
 
 template <typename R, typename TS, int NT, int VER, int LIM>
-__global__ void __launch_bounds__(kThreads, 4) k_col1(DMeshT<R> m, FusedArgs<R, TS> a) {
+__global__ void __launch_bounds__(kThreads, FESOM_MINB_COL1) k_col1(DMeshT<R> m, FusedArgs<R, TS> a) {
   extern __shared__ int smem[];
   col1_block<R, TS, NT, VER, LIM>(m, a, blockIdx.x, smem);
 }
@@ -648,7 +668,7 @@ __device__ __forceinline__ void col2_block(const DMeshT<R> &m, const FusedArgs<R
 }
 
 template <typename R, typename TS, int NT>
-__global__ void __launch_bounds__(kThreads) k_col2(DMeshT<R> m, FusedArgs<R, TS> a) {
+__global__ void __launch_bounds__(kThreads, FESOM_MINB_COL2) k_col2(DMeshT<R> m, FusedArgs<R, TS> a) {
   extern __shared__ int smem[];
   col2_block<R, TS, NT>(m, a, blockIdx.x, smem);
 }
@@ -741,7 +761,7 @@ __device__ __forceinline__ void col3_block(const DMeshT<R> &m, const FusedArgs<R
 }
 
 template <typename R, typename TS, int NT, int LIM>
-__global__ void __launch_bounds__(kThreads, 4) k_col3(DMeshT<R> m, FusedArgs<R, TS> a) {
+__global__ void __launch_bounds__(kThreads, FESOM_MINB_COL3) k_col3(DMeshT<R> m, FusedArgs<R, TS> a) {
   extern __shared__ int smem[];
   col3_block<R, TS, NT, LIM>(m, a, blockIdx.x, smem);
 }
