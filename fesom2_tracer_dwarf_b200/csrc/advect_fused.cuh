@@ -138,6 +138,42 @@ __device__ __forceinline__ CellMap map_cells(const DSched &sc, int blk, int *s_o
   return cm;
 }
 
+// A node block's incidence records (the CSR slice of its nodes) staged in
+// shared memory by one cooperative load, so that every lane's walk over its
+// node's edges starts from shared memory instead of a dependent global load.
+// Blocks with more than kNeStage records read them from global memory.
+constexpr int kNeStage = 512;
+__host__ __device__ constexpr size_t smem_stage() {
+  return 16 + (size_t)kNeStage * sizeof(int4) + sizeof(int) * (kMaxItemsPerBlock + 1);
+}
+
+struct Incidence {
+  const int4 *ne;   // records of the block, from its first node's first record
+  const int *nep;   // per local node: first record (minus sub)
+  int sub;
+};
+
+template <typename R>
+__device__ __forceinline__ Incidence stage_incidence(const DMeshT<R> &m, const CellMap &cm, void *region) {
+  int4 *s_ne = reinterpret_cast<int4 *>(((uintptr_t)region + 15) & ~(uintptr_t)15);
+  int *s_nep = reinterpret_cast<int *>(s_ne + kNeStage);
+  const int p0 = m.ne_ptr[cm.i0], p1 = m.ne_ptr[cm.i0 + cm.ni];
+  Incidence r;
+  if (p1 - p0 <= kNeStage) {
+    for (int i = threadIdx.x; i < p1 - p0; i += blockDim.x) s_ne[i] = m.ne4[p0 + i];
+    for (int j = threadIdx.x; j <= cm.ni; j += blockDim.x) s_nep[j] = m.ne_ptr[cm.i0 + j] - p0;
+    r.ne = s_ne;
+    r.nep = s_nep;
+    r.sub = 0;
+  } else {
+    r.ne = m.ne4 + p0;
+    r.nep = m.ne_ptr + cm.i0;
+    r.sub = p0;
+  }
+  __syncthreads();
+  return r;
+}
+
 // ---------------------------------------------------------------------------
 // k_grad: ring-mean gradients of valuesAB (lib/oce_muscl_adv.F90:400-450:
 // the mean of tr_xy over the node's ring, weighted by element area), for the
@@ -537,6 +573,7 @@ __device__ __forceinline__ void col2_block(const DMeshT<R> &m, const FusedArgs<R
   s_mx = (R *)(((uintptr_t)s_mx + 15) & ~(uintptr_t)15);
   R *s_mn = s_mx + NT * kMaxCellsPerBlock;
   const CellMap cm = map_cells(m.node_sched, blk, s_off, s_item);
+  const Incidence inc = stage_incidence(m, cm, s_mn + NT * kMaxCellsPerBlock);
   const int S = m.S;
   const R big = R(1e3);
 
@@ -556,8 +593,8 @@ __device__ __forceinline__ void col2_block(const DMeshT<R> &m, const FusedArgs<R
       }
 #pragma unroll 4
   #pragma unroll 4
-    for (int p = m.ne_ptr[n]; p < m.ne_ptr[n + 1]; p++) {
-        const int4 q = m.ne4[p];
+    for (int p = inc.nep[j] - inc.sub, pe = inc.nep[j + 1] - inc.sub; p < pe; p++) {
+        const int4 q = inc.ne[p];
         if (nz > q.z) continue;
         const size_t o = (size_t)q.y * S + k;
         for (int t = 0; t < NT; t++) {
@@ -622,8 +659,8 @@ __device__ __forceinline__ void col2_block(const DMeshT<R> &m, const FusedArgs<R
       fm[t] = R(0) + (fmin2(R(0), av[k]) + fmin2(R(0), -av[k + 1]));
     }
 #pragma unroll 4
-    for (int p = m.ne_ptr[n]; p < m.ne_ptr[n + 1]; p++) {
-      const int4 q = m.ne4[p];
+    for (int p = inc.nep[j] - inc.sub, pe = inc.nep[j + 1] - inc.sub; p < pe; p++) {
+      const int4 q = inc.ne[p];
       if (nz > q.z) continue;
       for (int t = 0; t < NT; t++) {
         const R f = a.adf_h[t][(size_t)(q.x >> 1) * S + k];
@@ -698,6 +735,7 @@ template <typename R, typename TS, int NT, int LIM>
 __device__ __forceinline__ void col3_block(const DMeshT<R> &m, const FusedArgs<R, TS> &a, int blk, int *smem) {
   int *s_off = smem, *s_item = smem + kMaxItemsPerBlock + 1;
   const CellMap cm = map_cells(m.node_sched, blk, s_off, s_item);
+  const Incidence inc = stage_incidence(m, cm, smem + kMaxItemsPerBlock + 1 + kMaxCellsPerBlock + 1);
   const int S = m.S;
   for (int lc = threadIdx.x; lc < cm.nc; lc += blockDim.x) {
     const int j = s_item[lc], n = cm.i0 + j, k = lc - (s_off[j] - cm.c0), nz = k + 1;
@@ -726,8 +764,8 @@ __device__ __forceinline__ void col3_block(const DMeshT<R> &m, const FusedArgs<R
         rms[t] = a.rm[t][o];
       }
 #pragma unroll 4
-    for (int p = m.ne_ptr[n]; p < m.ne_ptr[n + 1]; p++) {
-      const int4 q = m.ne4[p];
+    for (int p = inc.nep[j] - inc.sub, pe = inc.nep[j + 1] - inc.sub; p < pe; p++) {
+      const int4 q = inc.ne[p];
       if (nz > q.z) continue;
       const bool second = q.x & 1;
       const size_t oo = (size_t)q.y * S + k;  // the edge's other node
@@ -771,6 +809,11 @@ constexpr size_t smem_edge() { return sizeof(int) * (kMaxItemsPerBlock + 1 + kMa
 template <typename R>
 constexpr size_t smem_col(int nt, int arrays) {
   return sizeof(int) * (kMaxItemsPerBlock + 1 + kMaxCellsPerBlock + 1) + 16 + sizeof(R) * (size_t)arrays * nt * kMaxCellsPerBlock;
+}
+// k_col2 / k_col3: their arrays plus the staged incidence records
+template <typename R>
+constexpr size_t smem_col_staged(int nt, int arrays) {
+  return smem_col<R>(nt, arrays) + smem_stage();
 }
 
 }  // namespace fesom
