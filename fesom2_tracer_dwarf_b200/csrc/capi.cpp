@@ -914,7 +914,9 @@ int tracer_learn_step(const double *T_in, const double *T_target, double dt, dou
     if (!T_in || !T_target || !loss) return fail("null argument");
     if (check_ready()) return -1;
     ensure_engine();
-    *loss = g.eng->learn_step(T_in, T_target, dt, lr, update != 0, fct != 0);
+    // fct: 0 no limiter; 1 limiter, gradient through its ratios; 2 limiter,
+    // its factors held fixed in the gradient
+    *loss = g.eng->learn_step(T_in, T_target, dt, lr, update != 0, fct != 0, fct != 2);
     return 0;
   });
 }

@@ -71,10 +71,11 @@ class Engine {
   // One training step on tracer 0: values := T_in, one MUSCL+PPM step (with
   // the FCT limiter when fct) and the learned correction, loss =
   // volume-weighted mean squared difference to T_target; with update, one
-  // Adam step of rate lr on the MLP, the limiter's factors held at their
-  // forward values in the gradient.  Returns the loss before the update.
-  // Both arrays (nl-1, nod2D).
-  double learn_step(const double *T_in, const double *T_target, double dt, double lr, bool update, bool fct = false);
+  // Adam step of rate lr on the MLP.  With the limiter the gradient goes
+  // through its ratios R+/- (fct_grad) or holds its factors at their forward
+  // values.  Returns the loss before the update.  Both arrays (nl-1, nod2D).
+  double learn_step(const double *T_in, const double *T_target, double dt, double lr, bool update, bool fct = false,
+                    bool fct_grad = true);
 
   void set_velocity(const double *uv, const double *w);
   void set_velocity_zero();

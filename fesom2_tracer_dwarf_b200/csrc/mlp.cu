@@ -513,7 +513,7 @@ struct LearnedState {
   long long ncells = 0;  // edge cells of the dense edge schedule
   __nv_bfloat16 *feat[kBatchMax] = {};
   float *fscale[kBatchMax] = {}, *y[kBatchMax] = {};
-  float *dy = nullptr, *target = nullptr;
+  float *dy = nullptr, *target = nullptr, *hp = nullptr, *hm = nullptr;
   double *red = nullptr;  // per-block partial sums
   double volume = 0.0;    // sum of areasvol * hnode_new over wet cells
   float adam_b1 = 0.9f, adam_b2 = 0.999f;
@@ -551,6 +551,118 @@ __global__ void __launch_bounds__(kThreads) k_learn_dy(DMeshT<float> m, const fl
       ae = f >= 0.0f ? fminf(1.0f, fminf(rp[o1], rm[o2])) : fminf(1.0f, fminf(rm[o1], rp[o2]));
     }
     dy[cell] = ae * scale[cell] * c * ((T[o1] - target[o1]) - (T[o2] - target[o2]));
+  }
+}
+
+// ---- gradient through the FCT limiter (Zalesak) ------------------------------
+// rho = dL/d(flux into a cell) = 2 dt (T - target) / sum V for every cell (the
+// update divides a flux by areasvol * hnode_new, the loss weights by it).
+__device__ __forceinline__ float learn_rho(const float *T, const float *target, size_t o, float c) {
+  return c * (T[o] - target[o]);
+}
+
+// Per node level: G+/- = sum over every limited flux (incident edges, the
+// column's interfaces) whose limiting factor is this cell's R+/- (the active
+// argument of the min, ties as in k_col3) of dL/d(limited flux) * flux; then
+// dL/dP+/- = G+/- * dR+/-/dP+/- where R+/- < 1 (R = Q / (P dt / V +- eps)).
+__global__ void __launch_bounds__(kThreads) k_learn_fct_g(DMeshT<float> m, const float *T, const float *target,
+                                                         float c, const float *adfh, const float *adfv,
+                                                         const float *rp, const float *rm, float dt, float *hp,
+                                                         float *hm) {
+  extern __shared__ int smem[];
+  int *s_off = smem, *s_item = smem + kMaxItemsPerBlock + 1;
+  const CellMap cm = map_cells(m.node_sched, blockIdx.x, s_off, s_item);
+  const int S = m.S;
+  for (int lc = threadIdx.x; lc < cm.nc; lc += blockDim.x) {
+    const int j = s_item[lc], n = cm.i0 + j, k = lc - (s_off[j] - cm.c0), nz = k + 1;
+    const size_t col = (size_t)n * S, o = col + k;
+    const int nlev = m.nlev_node[n];
+    const float *av = adfv + col;
+    const float rpn = rp[o], rmn = rm[o];
+    const float rho = learn_rho(T, target, o, c);
+    float gp = 0.f, gm = 0.f;
+    float fp = 0.f + (fmax2(0.f, av[k]) + fmax2(0.f, -av[k + 1]));
+    float fm = 0.f + (fmin2(0.f, av[k]) + fmin2(0.f, -av[k + 1]));
+    for (int p = m.ne_ptr[n]; p < m.ne_ptr[n + 1]; p++) {
+      const int4 q = m.ne4[p];
+      if (nz > q.z) continue;
+      const bool second = q.x & 1;
+      const float f = adfh[(size_t)(q.x >> 1) * S + k];
+      if (second) { fp = fp + fmax2(0.f, -f); fm = fm + fmin2(0.f, -f); }
+      else { fp = fp + fmax2(0.f, f); fm = fm + fmin2(0.f, f); }
+      const size_t oo = (size_t)q.y * S + k;
+      const float rpo = rp[oo], rmo = rm[oo], rho_o = learn_rho(T, target, oo, c);
+      const float rp1 = second ? rpo : rpn, rm1 = second ? rmo : rmn, rp2 = second ? rpn : rpo, rm2 = second ? rmn : rmo;
+      const float dLdF = second ? (rho_o - rho) : (rho - rho_o);  // first node gains the flux
+      if (f >= 0.f) {
+        const float a1 = rp1 < 1.f ? rp1 : 1.f;
+        if (rm2 < a1) { if (second) gm += dLdF * f; }       // node 2's R- limits
+        else if (rp1 < 1.f) { if (!second) gp += dLdF * f; }  // node 1's R+ limits
+      } else {
+        const float a1 = rm1 < 1.f ? rm1 : 1.f;
+        if (rp2 < a1) { if (second) gp += dLdF * f; }
+        else if (rm1 < 1.f) { if (!second) gm += dLdF * f; }
+      }
+    }
+    // interface i = nz (top of this cell): the cell is the limiter's "below" cell
+    {
+      const int i = nz;
+      if (i < nlev) {
+        const float f = av[i - 1];
+        const float dLdF = rho - (i >= 2 ? learn_rho(T, target, col + i - 2, c) : 0.f);
+        if (i == 1) {
+          if (f >= 0.f) { if (rpn < 1.f) gp += dLdF * f; }
+          else if (rmn < 1.f) gm += dLdF * f;
+        } else if (f >= 0.f) {
+          const float r_up = rm[col + i - 2], a1 = r_up < 1.f ? r_up : 1.f;
+          if (rpn < a1) gp += dLdF * f;
+        } else {
+          const float r_up = rp[col + i - 2], a1 = r_up < 1.f ? r_up : 1.f;
+          if (rmn < a1) gm += dLdF * f;
+        }
+      }
+    }
+    // interface i = nz + 1 (bottom of this cell): the cell is the "above" cell
+    {
+      const int i = nz + 1;
+      if (i < nlev) {
+        const float f = av[i - 1];
+        const float dLdF = learn_rho(T, target, col + i - 1, c) - rho;
+        if (f >= 0.f) {
+          const float a1 = rmn < 1.f ? rmn : 1.f;
+          if (!(rp[col + i - 1] < a1) && rmn < 1.f) gm += dLdF * f;
+        } else {
+          const float a1 = rpn < 1.f ? rpn : 1.f;
+          if (!(rm[col + i - 1] < a1) && rpn < 1.f) gp += dLdF * f;
+        }
+      }
+    }
+    const double dtv = (double)dt / (double)m.areasvol[o], e64 = (double)1e-16f;
+    const double fluxp = (double)fp * dtv + e64, fluxm = (double)fm * dtv - e64;
+    hp[o] = rpn < 1.f ? (float)((double)gp * (-(double)rpn / fluxp) * dtv) : 0.f;
+    hm[o] = rmn < 1.f ? (float)((double)gm * (-(double)rmn / fluxm) * dtv) : 0.f;
+  }
+}
+
+// dL/dy per edge cell through the limited update: the limited flux ae * f
+// plus f's share of both nodes' P+/- sums
+__global__ void __launch_bounds__(kThreads) k_learn_dy_fct(DMeshT<float> m, const float *T, const float *target,
+                                                          float c, const float *scale, const float *adfh,
+                                                          const float *rp, const float *rm, const float *hp,
+                                                          const float *hm, float *dy) {
+  extern __shared__ int smem[];
+  int *s_off = smem, *s_item = smem + kMaxItemsPerBlock + 1;
+  const CellMap cm = map_cells(m.edge_sched, blockIdx.x, s_off, s_item);
+  for (int lc = threadIdx.x; lc < cm.nc; lc += blockDim.x) {
+    const int j = s_item[lc], e = cm.i0 + j, k = lc - (s_off[j] - cm.c0), cell = cm.c0 + lc;
+    const int2 nn = m.edge_nodes[e];
+    const size_t o1 = (size_t)nn.x * m.S + k, o2 = (size_t)nn.y * m.S + k;
+    const float f = adfh[(size_t)e * m.S + k];
+    const float ae = f >= 0.f ? fmin2(fmin2(1.f, rp[o1]), rm[o2]) : fmin2(fmin2(1.f, rm[o1]), rp[o2]);
+    float g = ae * (learn_rho(T, target, o1, c) - learn_rho(T, target, o2, c));
+    if (f > 0.f) g += hp[o1] - hm[o2];
+    else if (f < 0.f) g += hm[o1] - hp[o2];
+    dy[cell] = scale[cell] * g;
   }
 }
 
@@ -607,6 +719,8 @@ void learned_release(EngineImpl &P) {
   }
   cudaFree(L.dy);
   cudaFree(L.target);
+  cudaFree(L.hp);
+  cudaFree(L.hm);
   cudaFree(L.red);
   delete P.learn;
   P.learn = nullptr;
@@ -684,7 +798,8 @@ void Engine::get_learned(float *params) const {
   CK(cudaMemcpy(params, p_->learn->mlp.p, kParams * sizeof(float), cudaMemcpyDeviceToHost));
 }
 
-double Engine::learn_step(const double *T_in, const double *T_target, double dt, double lr, bool update, bool fct) {
+double Engine::learn_step(const double *T_in, const double *T_target, double dt, double lr, bool update, bool fct,
+                          bool fct_grad) {
   EngineImpl &P = *p_;
   if (!P.learn) throw std::runtime_error("no learned flux: call set_learned first");
   if (P.tr.empty()) throw std::runtime_error("no tracers");
@@ -716,9 +831,24 @@ double Engine::learn_step(const double *T_in, const double *T_target, double dt,
   std::vector<double> part(std::max(1, m.node_sched.nblk));
   CK(cudaMemcpyAsync(part.data(), L.red, part.size() * sizeof(double), cudaMemcpyDeviceToHost, P.stream));
   if (update) {
-    k_learn_dy<<<m.edge_sched.nblk, kThreads, smem_edge(), P.stream>>>(
-        m, T, L.target, L.fscale[0], (float)(2.0 * dt / L.volume), (const float *)P.adfh[0],
-        fct ? (const float *)P.rp[0] : nullptr, fct ? (const float *)P.rm[0] : nullptr, L.dy);
+    const float c = (float)(2.0 * dt / L.volume);
+    if (fct && fct_grad) {
+      if (!L.hp) {
+        L.hp = dmalloc<float>((size_t)P.mesh.nod2D * P.S);
+        L.hm = dmalloc<float>((size_t)P.mesh.nod2D * P.S);
+      }
+      k_learn_fct_g<<<m.node_sched.nblk, kThreads, smem_edge(), P.stream>>>(
+          m, T, L.target, c, (const float *)P.adfh[0], (const float *)P.adfv[0], (const float *)P.rp[0],
+          (const float *)P.rm[0], (float)dt, L.hp, L.hm);
+      CK(cudaGetLastError());
+      k_learn_dy_fct<<<m.edge_sched.nblk, kThreads, smem_edge(), P.stream>>>(
+          m, T, L.target, c, L.fscale[0], (const float *)P.adfh[0], (const float *)P.rp[0], (const float *)P.rm[0],
+          L.hp, L.hm, L.dy);
+    } else {
+      k_learn_dy<<<m.edge_sched.nblk, kThreads, smem_edge(), P.stream>>>(
+          m, T, L.target, L.fscale[0], c, (const float *)P.adfh[0], fct ? (const float *)P.rp[0] : nullptr,
+          fct ? (const float *)P.rm[0] : nullptr, L.dy);
+    }
     CK(cudaGetLastError());
     CK(cudaMemsetAsync(L.mlp.grad, 0, kParams * sizeof(float), P.stream));
     if (mlp_grads_dev(L.mlp, L.feat[0], L.dy, L.ncells, P.stream) != 0)

@@ -302,10 +302,11 @@ int tracer_learn_get(float *params);
  * that step's parameter update. */
 int tracer_learn_grad(float *grad);
 /* One training step on tracer 1 (see Engine::learn_step): values := T_in,
- * one MUSCL+PPM step (FCT-limited when fct = 1) with the learned correction,
- * *loss = volume-weighted mean squared difference to T_target; update = 1
- * applies one Adam step of rate lr (the limiter's factors held at their
- * forward values in the gradient).  T_in, T_target (nl-1, nod2D). */
+ * one MUSCL+PPM step with the learned correction (fct = 0: no limiter;
+ * 1: FCT, the gradient taken through the limiter's ratios R+/-; 2: FCT, the
+ * limiter's factors held fixed in the gradient), *loss = volume-weighted mean
+ * squared difference to T_target; update = 1 applies one Adam step of rate
+ * lr.  T_in, T_target (nl-1, nod2D). */
 int tracer_learn_step(const double *T_in, const double *T_target, double dt, double lr, int update, int fct,
                       double *loss);
 
