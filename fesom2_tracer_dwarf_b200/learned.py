@@ -243,11 +243,12 @@ TRAINED = __import__("pathlib").Path(__file__).resolve().parent / "data" / "lear
 
 def trained_params():
     """Parameters trained on the 500x500x32 configuration (4x refined,
-    limiter-blind training), shipped with the package."""
+    trained through the FCT step and its limiter ratios), shipped with the
+    package."""
     return np.load(TRAINED).astype(np.float32)
 
 
-def study(nx=500, nl=32, refine=4, train_seeds=(1, 2, 3), val_seed=11, nsteps=20, iters=600, lr=2e-3, fct=False):
+def study(nx=500, nl=32, refine=4, train_seeds=(1, 2, 3), val_seed=11, nsteps=20, iters=600, lr=2e-3, fct=True):
     t0 = time.perf_counter()
     data = make_dataset(nx, nl, list(train_seeds) + [val_seed], nsteps, refine)
     t_data = time.perf_counter() - t0
@@ -285,11 +286,11 @@ def main():
     a.add_argument("--iters", type=int, default=600)
     a.add_argument("--lr", type=float, default=2e-3)
     a.add_argument("--params-out", default=None)
-    a.add_argument("--fct-training", action="store_true",
-                   help="train through the FCT step with the limiter's factors held fixed")
+    a.add_argument("--unlimited-training", action="store_true",
+                   help="train on the unlimited step instead of through the FCT limiter")
     args = a.parse_args()
     out = study(args.nx, args.nl, args.refine, nsteps=args.steps, iters=args.iters, lr=args.lr,
-                fct=args.fct_training)
+                fct=not args.unlimited_training)
     if args.params_out:
         np.save(args.params_out, np.array(out["params"], dtype=np.float32))
     out.pop("params")

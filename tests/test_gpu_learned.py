@@ -81,7 +81,20 @@ def test_training_gradient_matches_finite_differences(api, fct, tol):
 @pytest.fixture(scope="module")
 def small_study():
     from fesom2_tracer_dwarf_b200.learned import study
-    return study(nx=65, nl=12, refine=4, train_seeds=(1, 2, 3), val_seed=11, nsteps=12, iters=500, lr=3e-3)
+    return study(nx=65, nl=12, refine=4, train_seeds=(1, 2, 3), val_seed=11, nsteps=12, iters=500, lr=3e-3,
+                 fct=False)
+
+
+def test_limiter_aware_training_lowers_the_limited_error():
+    """Trained through the FCT step (gradient through the limiter ratios), the
+    network lowers the one-step error of the limited scheme on an unseen
+    trajectory."""
+    from fesom2_tracer_dwarf_b200.learned import study
+    out = study(nx=65, nl=12, refine=4, train_seeds=(1, 2, 3), val_seed=11, nsteps=12, iters=500, lr=3e-3,
+                fct=True)
+    f = out["one_step_loss"]["fct"]
+    assert f["val_learned"] < 0.98 * f["val_plain"], f
+    assert abs(out["rollout_val"]["learned"][1]) < 1e-6
 
 
 def test_training_beats_plain_scheme_on_held_out_data(small_study):
