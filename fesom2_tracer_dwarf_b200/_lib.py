@@ -111,6 +111,10 @@ SIGNATURES = {
     "tracer_learn_grad": (ctypes.c_int, [_vp]),
     "tracer_learn_step": (ctypes.c_int, [_vp, _vp, ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_int,
                                          ctypes.POINTER(ctypes.c_double)]),
+    "tracer_write_mesh": (ctypes.c_int, [ctypes.c_char_p]),
+    "tracer_scalar_output_open": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int]),
+    "tracer_scalar_output_write": (ctypes.c_int, []),
+    "tracer_scalar_output_close": (ctypes.c_int, []),
     "tracer_advect_device_noalloc": (ctypes.c_int, [ctypes.c_int, _vp, _vp, _vp, ctypes.c_double]),
     "tracer_noalloc_scratch_bytes": (ctypes.c_longlong, []),
     "tracer_last_error": (ctypes.c_char_p, []),

@@ -13,6 +13,7 @@
 #include "../../include/fesom_tracer.h"
 #include "batch.hpp"
 #include "engine.hpp"
+#include "output.hpp"
 
 using namespace fesom;
 
@@ -917,6 +918,52 @@ int tracer_learn_step(const double *T_in, const double *T_target, double dt, dou
     // fct: 0 no limiter; 1 limiter, gradient through its ratios; 2 limiter,
     // its factors held fixed in the gradient
     *loss = g.eng->learn_step(T_in, T_target, dt, lr, update != 0, fct != 0, fct != 2);
+    return 0;
+  });
+}
+
+// ---------------------------------------------------------------------------
+// raw binary output for the reference's plotting scripts (output.hpp)
+// ---------------------------------------------------------------------------
+namespace {
+ScalarOutput g_scalars;
+}
+
+int tracer_write_mesh(const char *output_dir) {
+  return guarded([&] {
+    if (!output_dir) return fail("null output directory");
+    if (!g.mesh) return fail("no mesh");
+    write_mesh_files(*g.mesh, output_dir);
+    return 0;
+  });
+}
+
+int tracer_scalar_output_open(const char *output_dir, int nsteps) {
+  return guarded([&] {
+    if (!output_dir) return fail("null output directory");
+    if (check_ready()) return -1;
+    if (g.ntr < 1) return fail("no tracers allocated");
+    const int wp = g.prec == Precision::FP64 ? 8 : (g.prec == Precision::FP32 ? 4 : 2);
+    g_scalars.open(output_dir, g.nod2D, g.nl - 1, nsteps, g.ntr, wp);
+    return 0;
+  });
+}
+
+int tracer_scalar_output_write(void) {
+  return guarded([&] {
+    if (!g_scalars.is_open()) return fail("scalar output is not open");
+    std::vector<double> v((size_t)(g.nl - 1) * g.nod2D);
+    for (int t = 0; t < g_scalars.tracers(); t++) {
+      if (tracer_get_values_id(t + 1, v.data(), g.nl - 1, g.nod2D) != 0) return -1;
+      g_scalars.write(t, v.data());
+    }
+    return 0;
+  });
+}
+
+int tracer_scalar_output_close(void) {
+  return guarded([&] {
+    g_scalars.close();
     return 0;
   });
 }

@@ -199,6 +199,20 @@ class FESOMTracerAdvection:
         _lib.check(self.lib, self.lib.tracer_time_steps(nsteps, dt, ctypes.byref(ms)), "tracer_time_steps")
         return ms.value
 
+    def write_mesh(self, output_dir):
+        """Mesh files for the reference's plotting scripts (tracer_write_mesh)."""
+        _lib.check(self.lib, self.lib.tracer_write_mesh(str(output_dir).encode()), "tracer_write_mesh")
+
+    def open_scalar_output(self, output_dir, nsteps):
+        _lib.check(self.lib, self.lib.tracer_scalar_output_open(str(output_dir).encode(), nsteps),
+                   "tracer_scalar_output_open")
+
+    def write_scalar_step(self):
+        _lib.check(self.lib, self.lib.tracer_scalar_output_write(), "tracer_scalar_output_write")
+
+    def close_scalar_output(self):
+        _lib.check(self.lib, self.lib.tracer_scalar_output_close(), "tracer_scalar_output_close")
+
     def cleanup(self):
         return self.lib.tracer_cleanup()
 

@@ -310,6 +310,20 @@ int tracer_learn_grad(float *grad);
 int tracer_learn_step(const double *T_in, const double *T_target, double dt, double lr, int update, int fct,
                       double *loss);
 
+/* ---- raw binary output for the reference's plotting scripts ---------------
+ * The files of lib/mesh_output.F90:19-161 (read by visualization/plot_mesh.py
+ * and plot_scalars.py).  tracer_write_mesh replaces write_mesh_for_python
+ * (:19): mesh_info.txt, coord_nod2D.bin (metres), elem2D_nodes.bin (0-based),
+ * zbar.bin, depth.bin (bottom of each node's column).  The scalar calls
+ * replace open_scalar_output (:97), write_scalar_step (:136) and
+ * close_scalar_output (:154): one FP64 (nl-1, nod2D) frame of every
+ * allocated tracer per write (temperature.bin, salinity.bin, tracer3.bin, ...;
+ * wp = 8, 4 or 2 after the precision mode). */
+int tracer_write_mesh(const char *output_dir);
+int tracer_scalar_output_open(const char *output_dir, int nsteps);
+int tracer_scalar_output_write(void);
+int tracer_scalar_output_close(void);
+
 /* Last error message of this thread ("" if none). */
 const char *tracer_last_error(void);
 
