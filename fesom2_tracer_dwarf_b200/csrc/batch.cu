@@ -134,7 +134,8 @@ BatchKernel pick_kernel_b(const TracerScheme &s) {
 
 // the register budget follows the resident threads per SM the tile asks for
 BatchKernel pick_kernel(const TracerScheme &s, int threads = 256, int blocks_per_sm = 2) {
-  const int minb = std::max(2, std::min(4, (threads * blocks_per_sm + 255) / 256));
+  const int minb = std::max(2, std::min(5, (threads * blocks_per_sm + 255) / 256));
+  if (minb == 5) return pick_kernel_b<5>(s);
   if (minb == 4) return pick_kernel_b<4>(s);
   if (minb == 3) return pick_kernel_b<3>(s);
   return pick_kernel_b<2>(s);
@@ -565,7 +566,7 @@ std::string Batch::autotune(int steps_per_candidate) {
     for (int wave : {1, 2, 4}) {
       if (wave > max_batches && wave != 1) continue;
       for (int threads : {128, 256}) {
-        for (int bps : {2, 3, 4, 6}) {
+        for (int bps : {2, 3, 4, 5, 6, 8, 10}) {
           BatchTile t;
           t.cells_per_block = cells;
           t.wave = wave;
