@@ -217,18 +217,9 @@ def run_reference(args):
 # GPU arm
 # ---------------------------------------------------------------------------
 def run_ours(args):
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    dist = None
-    if world > 1:
-        import datetime
-        import torch
-        import torch.distributed as tdist
-        torch.cuda.set_device(local)
-        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
-                                 device_id=torch.device("cuda", local))
-        dist = tdist
+    from fesom2_tracer_dwarf_b200.replicas import from_env, job_rate
+    ranks = from_env("nccl")
+    rank, world, local = ranks.rank, ranks.world, ranks.local
 
     from fesom2_tracer_dwarf_b200 import FESOMTracerAdvection
     api = FESOMTracerAdvection()
@@ -253,9 +244,7 @@ def run_ours(args):
     launches_per_step = api.lib.tracer_launches_per_step()
     dev_bytes = api.lib.tracer_device_bytes()
 
-    def barrier():
-        if dist is not None:
-            dist.barrier()
+    barrier = ranks.barrier
 
     # device-resident throughput, CUDA events on the engine's stream
     clock = ClockSampler(local)
@@ -264,13 +253,9 @@ def run_ours(args):
     ms = api.time_steps(args.steps, dt)
     barrier()
     clocks = clock.stop()
-    if dist is not None:
-        import torch
-        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = ranks.max(ms)
     ms_per_step = ms / args.steps
-    value = world * 2 * cells / (ms_per_step / 1e3)
+    value = job_rate(2 * cells, world, ms_per_step / 1e3)
 
     # per-kernel breakdown (events around each launch), untimed otherwise
     nk = 8
@@ -302,13 +287,7 @@ def run_ours(args):
                 raise RuntimeError(api.lib.tracer_last_error().decode())
             api.lib.tracer_get_values_id(1, outT.ctypes.data_as(ctypes.c_void_p), L, N)
             api.lib.tracer_get_values_id(2, outS.ctypes.data_as(ctypes.c_void_p), L, N)
-        sec = (time.perf_counter() - t0) / args.e2e_steps
-        if dist is not None:
-            import torch
-            t = torch.tensor([sec], dtype=torch.float64, device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            sec = float(t.item())
-        return sec
+        return ranks.max((time.perf_counter() - t0) / args.e2e_steps)
 
     host = [np.asfortranarray(api.get_tracer_values(1)), np.asfortranarray(api.get_tracer_values(2)),
             np.zeros((L, N), order="F"), np.zeros((L, N), order="F")]
@@ -350,9 +329,7 @@ def run_ours(args):
             "gpu_launches": launches_per_step * args.steps,
             "clocks": clocks,
         }
-    if dist is not None:
-        dist.barrier()
-        dist.destroy_process_group()
+    ranks.close()
     api.cleanup()
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         rate, threads, sample, _ = cpu_rate(min(args.nx, 300), args.nl, 3)
