@@ -161,10 +161,10 @@ def committed_traffic():
 # ---------------------------------------------------------------------------
 # CPU arm: the oracle on a bounded sample
 # ---------------------------------------------------------------------------
-def cpu_rate(nx_sample, nl, steps, warmup=1):
-    """Cell-updates/s of the OpenMP oracle on a periodic nx_sample^2 x nl
-    mesh drawn like the GPU workload.  Returns (rate, threads, sample text,
-    per-step seconds)."""
+def cpu_rate(nx_sample, nl, steps, warmup=1, serial=False):
+    """Cell-updates/s of the oracle (OpenMP on every host thread, or the
+    serial build) on a periodic nx_sample^2 x nl mesh drawn like the GPU
+    workload.  Returns (rate, threads, sample text, per-step seconds)."""
     sys.path.insert(0, str(ROOT / "oracle"))
     import pyoracle
     from fesom2_tracer_dwarf_b200 import FESOMTracerAdvection
@@ -172,8 +172,9 @@ def cpu_rate(nx_sample, nl, steps, warmup=1):
     api.cleanup()
     K, uv, w, T, S, dt, cells = make_inputs(api, nx_sample, nl)
     api.cleanup()
-    o = pyoracle.Oracle(openmp=True)
-    o.set_threads(os.cpu_count() or 1)
+    o = pyoracle.Oracle(openmp=not serial)
+    if not serial:
+        o.set_threads(os.cpu_count() or 1)
     m = pyoracle.OracleMesh(o, nx_sample, nx_sample, nl, periodic=True, full_rings=True, node_K=K,
                             left_oriented=True)
     N = m.nod2D
@@ -189,7 +190,7 @@ def cpu_rate(nx_sample, nl, steps, warmup=1):
     rate = 2 * cells / sec
     sample = (f"periodic {nx_sample}x{nx_sample}x{nl} ({N} nodes, {cells} wet cells), same bathymetry/flow/tracer "
               f"distributions, 2 tracers, median of {steps} steps after {warmup} warm-up")
-    return rate, o.threads(), sample, per
+    return rate, (1 if serial else o.threads()), sample, per
 
 
 def run_reference(args):
@@ -335,6 +336,10 @@ def run_ours(args):
         rate, threads, sample, _ = cpu_rate(min(args.nx, 300), args.nl, 3)
         result["cpu_baseline"] = {"value": rate, "unit": "cell-updates/s", "cores": threads, "kind": "port",
                                   "sample": sample}
+        # the reference's own build is serial: the same oracle on one thread
+        rate1, _, sample1, _ = cpu_rate(min(args.nx, 150), args.nl, 3, serial=True)
+        result["cpu_baseline_serial"] = {"value": rate1, "unit": "cell-updates/s", "cores": 1, "kind": "port",
+                                         "sample": sample1}
     if rank == 0:
         print(json.dumps(result))
     return 0
