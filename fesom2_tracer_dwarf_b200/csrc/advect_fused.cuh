@@ -380,41 +380,17 @@ __device__ __forceinline__ R ppm_slope(R Tm1, R T0, R Tp1, R c1, R c2, R c3) {
 template <typename R, typename TS, int NT, int VER, int LIM>
 __device__ __forceinline__ void col1_block(const DMeshT<R> &m, const FusedArgs<R, TS> &a, int blk, int *smem) {
   int *s_off = smem, *s_item = smem + kMaxItemsPerBlock + 1;
-  R *s_acc = (R *)(smem + kMaxItemsPerBlock + 1 + kMaxCellsPerBlock + 1);  // 8-byte aligned below
-  s_acc = (R *)(((uintptr_t)s_acc + 15) & ~(uintptr_t)15);
-  R *s_slope = s_acc + NT * kMaxCellsPerBlock;
+  R *s_slope = (R *)(smem + kMaxItemsPerBlock + 1 + kMaxCellsPerBlock + 1);  // 16-byte aligned below
+  s_slope = (R *)(((uintptr_t)s_slope + 15) & ~(uintptr_t)15);
   R *s_tv = s_slope + NT * kMaxCellsPerBlock;
   R *s_fv = s_tv + NT * kMaxCellsPerBlock;
   const CellMap cm = map_cells(m.node_sched, blk, s_off, s_item);
+  const Incidence inc = stage_incidence(m, cm, s_fv + NT * kMaxCellsPerBlock);
   const int S = m.S;
 
-  // stage A: horizontal LO gather and PPM slopes
+  // stage A: PPM slopes
   for (int lc = threadIdx.x; lc < cm.nc; lc += blockDim.x) {
     const int j = s_item[lc], n = cm.i0 + j, k = lc - (s_off[j] - cm.c0), nz = k + 1;
-    if (LIM == LIM_FCT) {
-      R acc[NTMAX], tself[NTMAX];
-      const size_t on = (size_t)n * S + k;
-      for (int t = 0; t < NT; t++) {
-        acc[t] = R(0);
-        tself[t] = ldT(a.T[t], on, a.off[t]);
-      }
-#pragma unroll 4
-  #pragma unroll 4
-    for (int p = m.ne_ptr[n]; p < m.ne_ptr[n + 1]; p++) {
-        const int4 q = m.ne4[p];
-        if (nz > q.z) continue;
-        const bool second = q.x & 1;
-        const R vf = a.vflux[(size_t)(q.x >> 1) * S + k];
-        const size_t oo = (size_t)q.y * S + k;  // the edge's other node
-        for (int t = 0; t < NT; t++) {
-          const R to = ldT(a.T[t], oo, a.off[t]);
-          // upw1_flux(vf, T(first node), T(second node))
-          const R F = second ? upw1_flux(vf, to, tself[t]) : upw1_flux(vf, tself[t], to);
-          acc[t] = second ? acc[t] - F : acc[t] + F;
-        }
-      }
-      for (int t = 0; t < NT; t++) s_acc[t * kMaxCellsPerBlock + lc] = acc[t];
-    }
     if (VER == VER_PPM) {
       const int nlev = m.nlev_node[n];
       if (nz >= 2 && nz <= nlev - 2) {
@@ -540,18 +516,36 @@ __device__ __forceinline__ void col1_block(const DMeshT<R> &m, const FusedArgs<R
   if (LIM != LIM_FCT) return;
   __syncthreads();
 
-  // stage D: LO solution (lib/oce_adv_tra_driver.F90:202-211)
+  // stage D: horizontal LO gather and the LO solution
+  // (lib/oce_adv_tra_driver.F90:122-181, :202-211)
   for (int lc = threadIdx.x; lc < cm.nc; lc += blockDim.x) {
-    const int j = s_item[lc], n = cm.i0 + j, k = lc - (s_off[j] - cm.c0);
+    const int j = s_item[lc], n = cm.i0 + j, k = lc - (s_off[j] - cm.c0), nz = k + 1;
     const size_t o = (size_t)n * S + k;
     const int nlev = m.nlev_node[n];
+    R acc[NTMAX], tself[NTMAX];
+    for (int t = 0; t < NT; t++) {
+      acc[t] = R(0);
+      tself[t] = ldT(a.T[t], o, a.off[t]);
+    }
+    for (int p = inc.nep[j] - inc.sub, pe = inc.nep[j + 1] - inc.sub; p < pe; p++) {
+      const int4 q = inc.ne[p];
+      if (nz > q.z) continue;
+      const bool second = q.x & 1;
+      const R vf = a.vflux[(size_t)(q.x >> 1) * S + k];
+      const size_t oo = (size_t)q.y * S + k;  // the edge's other node
+      for (int t = 0; t < NT; t++) {
+        const R to = ldT(a.T[t], oo, a.off[t]);
+        // upw1_flux(vf, T(first node), T(second node))
+        const R F = second ? upw1_flux(vf, to, tself[t]) : upw1_flux(vf, tself[t], to);
+        acc[t] = second ? acc[t] - F : acc[t] + F;
+      }
+    }
     const R asv = m.areasvol[o], hn = m.hnode_new[o], h = m.hnode[o];
     const R yasv = R(1) / asv, yhn = R(1) / hn;
     for (int t = 0; t < NT; t++) {
       const R fk = s_fv[t * kMaxCellsPerBlock + lc];
       const R fk1 = (k + 2 == nlev) ? R(0) : s_fv[t * kMaxCellsPerBlock + lc + 1];
-      const R acc = s_acc[t * kMaxCellsPerBlock + lc];
-      const R num = ldT(a.T[t], o, a.off[t]) * h + div_rcp((acc + (fk - fk1)) * a.dt, asv, yasv);
+      const R num = tself[t] * h + div_rcp((acc[t] + (fk - fk1)) * a.dt, asv, yasv);
       a.lo[t][o] = div_rcp(num, hn, yhn);
     }
   }
