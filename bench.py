@@ -143,11 +143,13 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def committed_traffic():
-    """DRAM bytes per step of the plain FP64 step from the committed ncu
-    summary (profiles/step_c2_fp64.md, line 'dram_bytes_per_step_scaled: X')."""
+def committed_traffic(args):
+    """DRAM bytes per step of the plain FP64 step at 1000x1000x64 from the
+    committed ncu summary (profiles/step_c2_fp64.md, line
+    'dram_bytes_per_step_scaled: X'); None for any other workload or
+    precision, which that capture does not cover."""
     p = ROOT / "profiles" / "step_c2_fp64.md"
-    if not p.exists():
+    if args.precision != "fp64" or args.learned or args.nx != 1000 or args.nl != 64 or not p.exists():
         return None
     for line in p.read_text().splitlines():
         if line.strip().startswith("dram_bytes_per_step_scaled:"):
@@ -307,7 +309,7 @@ def run_ours(args):
         peak, peak_kind = measured_peaks()
         alg_bytes_step = BYTES_PER_CELL[args.precision] * cells * 2
         achieved = alg_bytes_step / (ms_per_step / 1e3) / 1e9
-        traffic = committed_traffic()
+        traffic = committed_traffic(args)
         result = {
             "metric": "tracer cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,

@@ -112,6 +112,10 @@ struct FusedArgs {
   R off[NTMAX];           // storage offsets (16-bit storage)
   uint32_t seed[NTMAX];   // per-step random stream of each tracer (stochastic rounding)
   int sround;             // 1: stochastic rounding of 16-bit stores
+  // edge volume fluxes: 0 computed from the velocity (stored in vflux when the
+  // limiter needs them), 1 computed and stored, 2 loaded from vflux (stored
+  // by an earlier launch with the same velocity)
+  int vflux_mode;
 };
 
 // ---------------------------------------------------------------------------
@@ -263,11 +267,16 @@ __device__ __forceinline__ void edge_block(const DMeshT<R> &m, const FusedArgs<R
   const R re = R(kREarthD), sixth = R(1.0 / 6.0);
   for (int lc = threadIdx.x; lc < cm.nc; lc += blockDim.x) {
     const int j = s_item[lc], e = cm.i0 + j, k = lc - (s_off[j] - cm.c0);
-    const EdgeCtx<R> c = edge_ctx(m, e);
-    const R vflux = edge_vflux(m, c, a.vel, k);
     const size_t o = (size_t)e * m.S + k;
-    if (LIM == LIM_FCT) a.vflux[o] = vflux;
-    const size_t o1 = (size_t)c.n1 * m.S + k, o2 = (size_t)c.n2 * m.S + k;
+    const int2 nn = m.edge_nodes[e];
+    R vflux;
+    if (a.vflux_mode == 2) {
+      vflux = a.vflux[o];
+    } else {
+      vflux = edge_vflux(m, edge_ctx(m, e), a.vel, k);
+      if (LIM == LIM_FCT || a.vflux_mode == 1) a.vflux[o] = vflux;
+    }
+    const size_t o1 = (size_t)nn.x * m.S + k, o2 = (size_t)nn.y * m.S + k;
     if (HOR == HOR_UPW1) {
       for (int t = 0; t < NT; t++) {
         const R flo = (LIM == LIM_FCT) ? upw1_flux(vflux, ldT(a.T[t], o1, a.off[t]), ldT(a.T[t], o2, a.off[t])) : R(0);
@@ -279,7 +288,7 @@ __device__ __forceinline__ void edge_block(const DMeshT<R> &m, const FusedArgs<R
     R gux[NTMAX], guy[NTMAX], gdx[NTMAX], gdy[NTMAX];
     const int2 ud = m.up_dn[e];
     bool shared = false;
-    if (ud.x >= 0 && ud.y >= 0) shared = (k + 1) <= min(m.nlev_node_min[c.n1], m.nlev_node_min[c.n2]) - 1;
+    if (ud.x >= 0 && ud.y >= 0) shared = (k + 1) <= min(m.nlev_node_min[nn.x], m.nlev_node_min[nn.y]) - 1;
     if (shared) {
       trxy_n(m, a.TAB, a.off, NT, ud.x, k, gux, guy);
       trxy_n(m, a.TAB, a.off, NT, ud.y, k, gdx, gdy);
@@ -293,8 +302,8 @@ __device__ __forceinline__ void edge_block(const DMeshT<R> &m, const FusedArgs<R
     const R ex = m.edge_dxdy[2 * e], ey = m.edge_dxdy[2 * e + 1], aa = m.edge_a[e];
     R c_lo1 = R(1), c_lo2 = R(1);
     if (HOR == HOR_MUSCL) {
-      c_lo1 = (m.nbl[c.n1] - (k + 1) >= 0) ? R(1) : R(0);
-      c_lo2 = (m.nbl[c.n2] - (k + 1) >= 0) ? R(1) : R(0);
+      c_lo1 = (m.nbl[nn.x] - (k + 1) >= 0) ? R(1) : R(0);
+      c_lo2 = (m.nbl[nn.y] - (k + 1) >= 0) ? R(1) : R(0);
     }
     for (int t = 0; t < NT; t++) {
       const R t1 = ldT(a.TAB[t], o1, a.off[t]), t2 = ldT(a.TAB[t], o2, a.off[t]);

@@ -245,6 +245,7 @@ int Engine::num_tracers() const { return (int)p_->tr.size(); }
 
 void Engine::set_velocity(const double *uv, const double *w) {
   EngineImpl &P = *p_;
+  P.vflux_valid = false;
   const MeshHost &M = P.mesh;
   const int L = M.nl - 1, T = M.elem2D, N = M.nod2D;
   std::vector<double> st((size_t)2 * T * P.S, 0.0), wst((size_t)N * P.S, 0.0);
@@ -266,6 +267,7 @@ void Engine::set_velocity(const double *uv, const double *w) {
 
 void Engine::set_velocity_zero() {
   EngineImpl &P = *p_;
+  P.vflux_valid = false;
   CK(cudaMemsetAsync(P.vel, 0, P.r_bytes * 2 * P.mesh.elem2D * P.S, P.stream));
   CK(cudaMemsetAsync(P.W, 0, P.r_bytes * P.mesh.nod2D * P.S, P.stream));
   CK(cudaStreamSynchronize(P.stream));
@@ -296,6 +298,7 @@ void Engine::release_work() {
   }
   P.dfree(P.vflux);
   P.vflux = nullptr;
+  P.vflux_valid = false;
   P.slots = 0;
 }
 
@@ -418,8 +421,12 @@ static void run_batch(EngineImpl &P, int first, int nt, double dt, bool refresh_
     tr.nstep++;
   }
   b.sround = storage16(P) ? P.sround : 0;
+  // the velocity only changes through set_velocity: the first launch after it
+  // stores the edge volume fluxes, later ones load them
   b.vflux = P.vflux;
+  b.vflux_mode = P.vflux_valid ? 2 : 1;
   dispatch(P, P.tr[first].sch, nt, b, dt);
+  P.vflux_valid = true;
   for (int t = 0; t < nt; t++) std::swap(P.tr[first + t].T, P.tr[first + t].Tout);
 }
 

@@ -33,6 +33,7 @@ struct BatchPtrs {
   void *rp[kBatchMax] = {};
   void *rm[kBatchMax] = {};
   void *vflux = nullptr;
+  int vflux_mode = 0;             // edge volume fluxes (FusedArgs::vflux_mode)
   void *gradn[kBatchMax] = {};
   void *feat[kBatchMax] = {};     // learned flux: features (BF16 x 16) per edge cell
   void *fscale[kBatchMax] = {};   // learned flux: correction scale per edge cell
@@ -75,6 +76,7 @@ struct EngineImpl {
   std::vector<Tracer> tr;
   int slots = 0;
   void *vflux = nullptr;
+  bool vflux_valid = false;  // vflux holds the edge volume fluxes of the current velocity
   void *adfh[kBatchMax] = {}, *adfv[kBatchMax] = {}, *lo[kBatchMax] = {}, *rp[kBatchMax] = {}, *rm[kBatchMax] = {};
   void *gradn[kBatchMax] = {};
 

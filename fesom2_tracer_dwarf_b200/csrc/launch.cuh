@@ -116,6 +116,7 @@ void launch_batch_t(EngineImpl &P, const TracerScheme &sc, int nt, const BatchPt
     a.seed[t] = b.seed[t];
   }
   a.sround = b.sround;
+  a.vflux_mode = b.vflux_mode;
   const bool fct = sc.lim == 1;
   if (nt == 4) fct ? run_group<R, TS, 4, LIM_FCT>(P, sc, a) : run_group<R, TS, 4, LIM_NONE>(P, sc, a);
   else if (nt == 2) fct ? run_group<R, TS, 2, LIM_FCT>(P, sc, a) : run_group<R, TS, 2, LIM_NONE>(P, sc, a);

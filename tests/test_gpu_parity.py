@@ -104,6 +104,28 @@ def test_scheme_matrix_bitwise(api, oracle, hor, ver, lim):
         assert_bitwise(api.get_tracer_values(1), To, f"{hor}/{ver}/{lim} step {step + 1}")
 
 
+@pytest.mark.parametrize("lim", ["FCT", "NONE"])
+def test_velocity_changes_between_steps_bitwise(api, oracle, lim):
+    """The edge volume fluxes the engine keeps from step to step follow every
+    new velocity: two steps with one flow, two with another, one with the
+    first again, then one with zero velocity, each bit-identical to the
+    oracle stepping with the velocity of that step."""
+    nx, ny, nl = 21, 18, 9
+    K, uv1, w1, T, S, dt = synth_case(api, nx, ny, nl, True, 31)
+    uv2, w2 = api.synth_velocity(seed=77, umax=0.8, mode2=0.3)
+    zuv, zw = np.zeros_like(uv1), np.zeros_like(w1)
+    sch = ("MUSCL", "PPM", lim, 1.0, 1.0)
+    m = setup_pair(api, oracle, nx, ny, nl, True, True, K, [T], uv1, w1, [sch], True)
+    To = T.copy(order="F")
+    plan = [(uv1, w1), (uv1, w1), (uv2, w2), (uv2, w2), (uv1, w1), (zuv, zw)]
+    for step, (uv, w) in enumerate(plan):
+        if step > 0 and uv is not plan[step - 1][0]:
+            api.set_velocity(uv, w)
+        api.advect_steps(1, dt)
+        m.step(To, To.copy(order="F"), uv, w, dt, "MUSCL", "PPM", lim)
+        assert_bitwise(api.get_tracer_values(1), To, f"{lim} step {step + 1}")
+
+
 @pytest.mark.parametrize("ph", [1.0, 0.75, 0.0])
 def test_closed_wall_bathymetry_bitwise(api, oracle, ph):
     """Closed-wall analytic mesh (boundary edges, nboundary_lay = 0 on the
