@@ -51,6 +51,18 @@ constexpr int kThreads = 256;
 #ifndef FESOM_MINB_GRAD
 #define FESOM_MINB_GRAD 5
 #endif
+// The LO gather of k_col1 issues the loads of this many incident edges
+// together before using any of them.  Every (edge, level) and (node, level)
+// address of a cell's level lies inside its padded column, so the loads of
+// dry edge levels, and of the clamped records past the node's last edge, are
+// in bounds; their values are discarded.  The fluxes are still accumulated
+// one edge at a time in ascending incidence order.  (Measured per kernel: 2
+// is faster than 1 or 4 for k_col1; the same form is slower in k_col2 and
+// k_col3, whose loops stay one edge at a time.)
+#ifndef FESOM_GCHUNK_COL1
+#define FESOM_GCHUNK_COL1 2
+#endif
+constexpr int kGChunkCol1 = FESOM_GCHUNK_COL1;
 constexpr int kCellsPerBlock = 512;      // schedule target: wet cells per block
 constexpr int kMaxCellsPerBlock = 576;   // upper bound (target + deepest column)
 constexpr int kMaxItemsPerBlock = 512;
@@ -536,17 +548,25 @@ __device__ __forceinline__ void col1_block(const DMeshT<R> &m, const FusedArgs<R
       acc[t] = R(0);
       tself[t] = ldT(a.T[t], o, a.off[t]);
     }
-    for (int p = inc.nep[j] - inc.sub, pe = inc.nep[j + 1] - inc.sub; p < pe; p++) {
-      const int4 q = inc.ne[p];
-      if (nz > q.z) continue;
-      const bool second = q.x & 1;
-      const R vf = a.vflux[(size_t)(q.x >> 1) * S + k];
-      const size_t oo = (size_t)q.y * S + k;  // the edge's other node
-      for (int t = 0; t < NT; t++) {
-        const R to = ldT(a.T[t], oo, a.off[t]);
-        // upw1_flux(vf, T(first node), T(second node))
-        const R F = second ? upw1_flux(vf, to, tself[t]) : upw1_flux(vf, tself[t], to);
-        acc[t] = second ? acc[t] - F : acc[t] + F;
+    for (int p = inc.nep[j] - inc.sub, pe = inc.nep[j + 1] - inc.sub; p < pe; p += kGChunkCol1) {
+      int4 qs[kGChunkCol1];
+      R vfs[kGChunkCol1], tos[kGChunkCol1][NT];
+#pragma unroll
+      for (int u = 0; u < kGChunkCol1; u++) {
+        qs[u] = inc.ne[min(p + u, pe - 1)];
+        vfs[u] = a.vflux[(size_t)(qs[u].x >> 1) * S + k];
+        const size_t oo = (size_t)qs[u].y * S + k;  // the edge's other node
+        for (int t = 0; t < NT; t++) tos[u][t] = ldT(a.T[t], oo, a.off[t]);
+      }
+#pragma unroll
+      for (int u = 0; u < kGChunkCol1; u++) {
+        if (p + u >= pe || nz > qs[u].z) continue;
+        const bool second = qs[u].x & 1;
+        for (int t = 0; t < NT; t++) {
+          // upw1_flux(vf, T(first node), T(second node))
+          const R F = second ? upw1_flux(vfs[u], tos[u][t], tself[t]) : upw1_flux(vfs[u], tself[t], tos[u][t]);
+          acc[t] = second ? acc[t] - F : acc[t] + F;
+        }
       }
     }
     const R asv = m.areasvol[o], hn = m.hnode_new[o], h = m.hnode[o];
@@ -595,7 +615,6 @@ __device__ __forceinline__ void col2_block(const DMeshT<R> &m, const FusedArgs<R
         tmn[t] = fmin2(l, tt);
       }
 #pragma unroll 4
-  #pragma unroll 4
     for (int p = inc.nep[j] - inc.sub, pe = inc.nep[j + 1] - inc.sub; p < pe; p++) {
         const int4 q = inc.ne[p];
         if (nz > q.z) continue;
