@@ -43,6 +43,9 @@ SIGNATURES = {
     "tracer_init_complete": (ctypes.c_int, []),
     "tracer_load_mesh_partition": (ctypes.c_int, [ctypes.c_char_p]),
     "tracer_load_mesh_from_files": (ctypes.c_int, [ctypes.c_char_p]),
+    "tracer_load_mesh_from_files_opts": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.c_double,
+                                                        ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                                        ctypes.c_double]),
     "tracer_init_ale_arrays": (ctypes.c_int, []),
     "tracer_init_for_advection": (ctypes.c_int, []),
     # extensions

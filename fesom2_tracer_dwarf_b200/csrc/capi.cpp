@@ -135,8 +135,27 @@ int tracer_run_workflow(const char *restart_dir, int, double) { return tracer_in
 int tracer_load_mesh_partition(const char *restart_dir) {
   return fail(std::string("binary restart input is not supported by this build (") + (restart_dir ? restart_dir : "") + ")");
 }
+int tracer_load_mesh_from_files_opts(const char *mesh_path, int rotate, double alpha, double beta, double gamma,
+                                     double angle_scale, double cyclic_length) {
+  return guarded([&] {
+    if (!mesh_path) return fail("tracer_load_mesh_from_files: null path");
+    if (!(cyclic_length > 0.0)) return fail("tracer_load_mesh_from_files: cyclic_length must be positive");
+    MeshFileOptions o;
+    o.rotate = rotate != 0;
+    o.alpha = alpha;
+    o.beta = beta;
+    o.gamma = gamma;
+    o.angle_scale = angle_scale;
+    o.cyclic_length = cyclic_length;
+    install_mesh(load_mesh_files(mesh_path, o));
+    g.initialized = true;
+    return 0;
+  });
+}
 int tracer_load_mesh_from_files(const char *mesh_path) {
-  return fail(std::string("the ASCII mesh reader is not part of this build (") + (mesh_path ? mesh_path : "") + ")");
+  const MeshFileOptions o;
+  return tracer_load_mesh_from_files_opts(mesh_path, o.rotate ? 1 : 0, o.alpha, o.beta, o.gamma, o.angle_scale,
+                                          o.cyclic_length);
 }
 
 int tracer_cleanup(void) {
@@ -599,6 +618,7 @@ static bool mesh_field(const char *name, const std::vector<int> **vi, const std:
   else if (s == "edge_dxdy") *vd = &m.edge_dxdy;
   else if (s == "edge_cross_dxdy") *vd = &m.edge_cross;
   else if (s == "gradient_sca") *vd = &m.grad_sca;
+  else if (s == "elem_cos") *vd = &m.elem_cos;
   else if (s == "hnode") *vd = &m.hnode;
   else if (s == "hnode_new") *vd = &m.hnode_new;
   else if (s == "helem") *vd = &m.helem;

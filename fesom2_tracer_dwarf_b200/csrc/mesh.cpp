@@ -21,9 +21,9 @@ namespace fesom {
 
 namespace {
 
-inline void trim_cyclic(double &b) {  // lib/gen_modules_rotate_grid.F90:216-223
-  if (b > kCyclicLength / 2.0) b = b - kCyclicLength;
-  if (b < -kCyclicLength / 2.0) b = b + kCyclicLength;
+inline void trim_cyclic(double &b, double L = kCyclicLength) {  // lib/gen_modules_rotate_grid.F90:216-223
+  if (b > L / 2.0) b = b - L;
+  if (b < -L / 2.0) b = b + L;
 }
 inline void trim_period(double &v, double P) {
   if (v > 0.5 * P) v = v - P;
@@ -386,7 +386,7 @@ void MeshHost::finalize_tables() {
     for (int side = 0; side < 2; side++) {
       int node = side == 0 ? a : b;
       double x0 = coord[2 * b] - coord[2 * a], x1 = coord[2 * b + 1] - coord[2 * a + 1];
-      trim_cyclic(x0);
+      trim_cyclic(x0, cyclic_length);
       if (periodic) { trim_period(x0, Px); trim_period(x1, Py); }
       if (side == 0) { x0 = -x0; x1 = -x1; }
       for (int p = ring_ptr[node]; p < ring_ptr[node + 1]; p++) {
@@ -397,8 +397,8 @@ void MeshHost::finalize_tables() {
         int i2 = i0 == 2 ? 1 : 2;
         double b0 = coord[2 * el[i1]] - coord[2 * el[i0]], b1 = coord[2 * el[i1] + 1] - coord[2 * el[i0] + 1];
         double c0 = coord[2 * el[i2]] - coord[2 * el[i0]], c1 = coord[2 * el[i2] + 1] - coord[2 * el[i0] + 1];
-        trim_cyclic(b0);
-        trim_cyclic(c0);
+        trim_cyclic(b0, cyclic_length);
+        trim_cyclic(c0, cyclic_length);
         if (periodic) { trim_period(b0, Px); trim_period(b1, Py); trim_period(c0, Px); trim_period(c1, Py); }
         double cr = c0 * c0 + c1 * c1;
         double bx = (b0 * c0 + b1 * c1) / cr;

@@ -51,6 +51,9 @@ struct MeshHost {
   bool periodic = false;
   bool full_rings = true;
   double Lx = 0, Ly = 0, max_depth = 0;
+  // cyclic_length in the units of coord (the reference keeps 360 while its
+  // coordinates are radians, so its trim never fires)
+  double cyclic_length = kCyclicLength;
 
   std::vector<double> coord;        // (2, nod2D) radians
   std::vector<int> elem_nodes;      // (3, elem2D)
@@ -101,6 +104,24 @@ MeshHost build_analytic_mesh(int nx, int ny, int nl, double Lx, double Ly, doubl
 
 // Number of 2D nodes of the analytic mesh.
 int analytic_nodes(int nx, int ny, bool periodic);
+
+// Mesh read from the ASCII mesh files of a FESOM2 mesh directory (nod2d.out,
+// elem2d.out, aux3d.out, edgenum.out, edges.out, edge_tri.out, elvls.out,
+// nlvls.out) as mesh_setup does on one process (lib/oce_mesh.F90:49-94),
+// followed by the thicknesses of tracer_init_ale_arrays
+// (lib/tracer_c_interface.F90:875-929).  The defaults are the reference's:
+// coordinates rotated with the Euler angles (50, 15, -90) passed to cos/sin
+// as they are (lib/gen_modules_rotate_grid.F90:42-44) and cyclic_length 360
+// against coordinates in radians; angle_scale = pi/180 and cyclic_length =
+// 2 pi give FESOM2's conventions.  Throws std::runtime_error naming the file
+// on malformed input.
+struct MeshFileOptions {
+  bool rotate = true;
+  double alpha = 50.0, beta = 15.0, gamma = -90.0;
+  double angle_scale = 1.0;
+  double cyclic_length = kCyclicLength;
+};
+MeshHost load_mesh_files(const std::string &dir, const MeshFileOptions &opt);
 
 // Seeded per-node bottom level index, uniform in [3, nl] (std::mt19937_64).
 std::vector<int> synth_bathymetry(int nnodes, int nl, uint64_t seed);

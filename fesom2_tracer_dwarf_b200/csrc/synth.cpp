@@ -152,6 +152,7 @@ void synth_velocity(const MeshHost &m, uint64_t seed, double umax, double mode1_
       }
     }
   }
+  std::vector<double> c1(L), c2(L);
   for (int e = 0; e < T; e++) {
     const int *en = &m.elem_nodes[3 * e];
     const double *gs = &m.grad_sca[6 * e];
@@ -159,12 +160,23 @@ void synth_velocity(const MeshHost &m, uint64_t seed, double umax, double mode1_
     auto gy = [&](const std::vector<double> &f) { return gs[3] * f[en[0]] + gs[4] * f[en[1]] + gs[5] * f[en[2]]; };
     const double u1 = -gy(f1), v1 = gx(f1);
     const double u2 = -gy(f2) + gx(f3), v2 = gx(f2) + gy(f3);
-    // vertical modes with zero mean over the element's own water column, so
-    // the column integral of every edge flux vanishes
+    // vertical modes with zero thickness-weighted mean over the element's
+    // own water column (helem), so the column integral of every edge flux
+    // vanishes on uniform and on stretched level sets alike
     const int M = m.nlev_elem[e] - 1;
+    const double *h = &m.helem[(size_t)e * L];
+    double s1 = 0.0, s2 = 0.0, hs = 0.0;
     for (int k = 0; k < M; k++) {
-      const double a1 = mode1_frac * std::cos(kPiRef * ((double)k + 0.5) / (double)M);
-      const double a2 = mode2_frac * std::cos(2.0 * kPiRef * ((double)k + 0.5) / (double)M);
+      c1[k] = std::cos(kPiRef * ((double)k + 0.5) / (double)M);
+      c2[k] = std::cos(2.0 * kPiRef * ((double)k + 0.5) / (double)M);
+      s1 += c1[k] * h[k];
+      s2 += c2[k] * h[k];
+      hs += h[k];
+    }
+    s1 /= hs;
+    s2 /= hs;
+    for (int k = 0; k < M; k++) {
+      const double a1 = mode1_frac * (c1[k] - s1), a2 = mode2_frac * (c2[k] - s2);
       uv[2 * ((size_t)e * L + k)] += a1 * u1 + a2 * u2;
       uv[2 * ((size_t)e * L + k) + 1] += a1 * v1 + a2 * v2;
     }

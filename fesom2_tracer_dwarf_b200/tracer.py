@@ -82,6 +82,22 @@ class FESOMTracerAdvection:
         self.dims = self.mesh_dims()
         return rc
 
+    def load_mesh_from_files(self, mesh_path, rotate=True, alpha=50.0, beta=15.0, gamma=-90.0, angle_scale=1.0,
+                             cyclic_length=360.0):
+        """Mesh from a FESOM2 ASCII mesh directory (tracer_load_mesh_from_files).
+        The defaults are the reference's conventions; angle_scale=pi/180 and
+        cyclic_length=2*pi give FESOM2's (angles in degrees, longitude wrapped
+        at the seam)."""
+        path = str(mesh_path).encode()
+        if (rotate, alpha, beta, gamma, angle_scale, cyclic_length) == (True, 50.0, 15.0, -90.0, 1.0, 360.0):
+            rc = self.lib.tracer_load_mesh_from_files(path)
+        else:
+            rc = self.lib.tracer_load_mesh_from_files_opts(path, int(bool(rotate)), alpha, beta, gamma, angle_scale,
+                                                           cyclic_length)
+        _lib.check(self.lib, rc, "tracer_load_mesh_from_files")
+        self.dims = self.mesh_dims()
+        return rc
+
     def mesh_dims(self):
         d = np.zeros(6, dtype=np.int32)
         _lib.check(self.lib, self.lib.tracer_mesh_dims(_lib.ptr(d)), "tracer_mesh_dims")

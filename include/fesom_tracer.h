@@ -21,10 +21,10 @@
  *    ELEMENTS, the mesh entity velocity lives on; the reference allocated it
  *    by edges and the kernels then read it as (2, nl-1, elem) (:694-725).
  * Restart files (tracer_init, tracer_finalize, tracer_run_workflow,
- * tracer_load_mesh_partition) and the ASCII mesh reader
- * (tracer_load_mesh_from_files) are not provided by this build: they return
- * -1 with a message.  Meshes come from tracer_init_analytic or
- * tracer_set_mesh_arrays.
+ * tracer_load_mesh_partition) are not provided by this build: they return
+ * -1 with a message.  Meshes come from tracer_init_analytic,
+ * tracer_set_mesh_arrays or the ASCII mesh files
+ * (tracer_load_mesh_from_files, one process, no partition files).
  */
 #ifndef FESOM_TRACER_H
 #define FESOM_TRACER_H
@@ -76,7 +76,16 @@ int tracer_set_velocity(const double *uv, const double *w, int nl, int nod2D, in
 int tracer_init_complete(void);
 /* :769 tracer_load_mesh_partition -- binary restarts are not supported: -1. */
 int tracer_load_mesh_partition(const char *restart_dir);
-/* :830 tracer_load_mesh_from_files -- the ASCII mesh reader is not part of this build: -1. */
+/* :830 tracer_load_mesh_from_files -- reads the mesh directory's nod2d.out,
+ * elem2d.out, aux3d.out, edgenum.out, edges.out, edge_tri.out, elvls.out and
+ * nlvls.out as mesh_setup does (lib/oce_mesh.F90:49-94), on one process
+ * (the reference reads them through its dist_<npes> partition lists), with
+ * the reference's conventions: rotation by the Euler angles (50, 15, -90)
+ * given to cos/sin as they are (lib/gen_modules_rotate_grid.F90:42-44) and
+ * cyclic_length = 360 against coordinates in radians, which leaves elements
+ * that straddle the longitude seam with their unwrapped (oversized) geometry
+ * exactly as the reference computes it.  Layer thicknesses are those of
+ * tracer_init_ale_arrays.  -1 with a message on a missing or malformed file. */
 int tracer_load_mesh_from_files(const char *mesh_path);
 /* :875 tracer_init_ale_arrays -- hnode = hnode_new = zbar(k)-zbar(k+1). */
 int tracer_init_ale_arrays(void);
@@ -84,6 +93,14 @@ int tracer_init_ale_arrays(void);
 int tracer_init_for_advection(void);
 
 /* ---- additive extensions ------------------------------------------------ */
+
+/* tracer_load_mesh_from_files with explicit conventions: rotate (0/1), Euler
+ * angles alpha, beta, gamma multiplied by angle_scale before cos/sin, and the
+ * cyclic length in radians of longitude.  (1, 50, 15, -90, 1, 360) is the
+ * reference's behaviour; (1, 50, 15, -90, pi/180, 2 pi) gives FESOM2's
+ * (angles in degrees, longitude wrapped at the seam). */
+int tracer_load_mesh_from_files_opts(const char *mesh_path, int rotate, double alpha, double beta, double gamma,
+                                     double angle_scale, double cyclic_length);
 
 /* Analytic mesh of lib/analytic_mesh.F90:114 (generate_analytic_mesh) with
  * the ALE arrays of src/fesom_analytic.F90:206-244.  node_K (nullable,

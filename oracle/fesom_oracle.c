@@ -21,6 +21,7 @@
 
 #include <math.h>
 #include <stdint.h>
+#include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
 #ifdef _OPENMP
@@ -48,6 +49,7 @@ static inline int imin2(int a, int b) { return a < b ? a : b; }
 struct om_mesh {
   int nx, ny, nl, periodic, full_rings;
   double Lx, Ly, max_depth;
+  double cyclic;            /* cyclic_length in the units of coord         */
   int nod2D, nod2D_total, elem2D, edge2D, max_nie;
   double *coord;            /* (2, nod2D_total), radians                   */
   int *elem2D_nodes;        /* (3, elem2D), after the periodic remap       */
@@ -114,12 +116,19 @@ static void trim_cyclic(double *b) { /* lib/gen_modules_rotate_grid.F90:216-223 
   if (*b < -CYCLIC_LENGTH / 2.0) *b = *b + CYCLIC_LENGTH;
 }
 
+/* trim_cyclic with the mesh's cyclic length */
+static void trim_cyc(double *b, double L) {
+  if (*b > L / 2.0) *b = *b - L;
+  if (*b < -L / 2.0) *b = *b + L;
+}
+
 /* lib/oce_mesh.F90:2001-2019 */
 static void edge_center(const om_mesh *m, int n1, int n2, double *x, double *y) {
+  const double L = m->cyclic;
   double a1 = A2(m->coord, 1, n1, 2), a2 = A2(m->coord, 2, n1, 2);
   double b1 = A2(m->coord, 1, n2, 2), b2 = A2(m->coord, 2, n2, 2);
-  if (a1 - b1 > CYCLIC_LENGTH / 2.0) a1 = a1 - CYCLIC_LENGTH;
-  if (a1 - b1 < -CYCLIC_LENGTH / 2.0) b1 = b1 - CYCLIC_LENGTH;
+  if (a1 - b1 > L / 2.0) a1 = a1 - L;
+  if (a1 - b1 < -L / 2.0) b1 = b1 - L;
   *x = 0.5 * (a1 + b1);
   *y = 0.5 * (a2 + b2);
 }
@@ -130,8 +139,8 @@ static void elem_center(const om_mesh *m, const int *elnodes, double *x, double 
   for (int k = 0; k < 3; k++) ax[k] = A2(m->coord, 1, elnodes[k], 2);
   double amin = fmin3(ax[0], ax[1], ax[2]);
   for (int k = 0; k < 3; k++) {
-    if (ax[k] - amin >= CYCLIC_LENGTH / 2.0) ax[k] = ax[k] - CYCLIC_LENGTH;
-    if (ax[k] - amin < -CYCLIC_LENGTH / 2.0) ax[k] = ax[k] + CYCLIC_LENGTH;
+    if (ax[k] - amin >= m->cyclic / 2.0) ax[k] = ax[k] - m->cyclic;
+    if (ax[k] - amin < -m->cyclic / 2.0) ax[k] = ax[k] + m->cyclic;
   }
   *x = ((ax[0] + ax[1]) + ax[2]) / 3.0;
   *y = ((A2(m->coord, 2, elnodes[0], 2) + A2(m->coord, 2, elnodes[1], 2)) +
@@ -160,7 +169,7 @@ static void find_up_downwind_triangles(om_mesh *m) {
       double x[2];
       x[0] = A2(m->coord, 1, ed2, 2) - A2(m->coord, 1, ed1, 2);
       x[1] = A2(m->coord, 2, ed2, 2) - A2(m->coord, 2, ed1, 2);
-      trim_cyclic(&x[0]);
+      trim_cyc(&x[0], m->cyclic);
       if (periodic) { trim_period(&x[0], Px); trim_period(&x[1], Py); }
       if (side == 0) { x[0] = -x[0]; x[1] = -x[1]; }
       for (int k = 1; k <= m->nod_in_elem2D_num[ednode - 1]; k++) {
@@ -175,8 +184,8 @@ static void find_up_downwind_triangles(om_mesh *m) {
         b[1] = A2(m->coord, 2, en[i1], 2) - A2(m->coord, 2, en[i0], 2);
         c[0] = A2(m->coord, 1, en[i2], 2) - A2(m->coord, 1, en[i0], 2);
         c[1] = A2(m->coord, 2, en[i2], 2) - A2(m->coord, 2, en[i0], 2);
-        trim_cyclic(&b[0]);
-        trim_cyclic(&c[0]);
+        trim_cyc(&b[0], m->cyclic);
+        trim_cyc(&c[0], m->cyclic);
         if (periodic) {
           trim_period(&b[0], Px); trim_period(&b[1], Py);
           trim_period(&c[0], Px); trim_period(&c[1], Py);
@@ -238,6 +247,7 @@ om_mesh *om_mesh_analytic(int nx, int ny, int nl, double Lx, double Ly,
                           const int *node_K) {
   if (nx < 2 || ny < 2 || nl < 3) return NULL;
   om_mesh *m = (om_mesh *)calloc(1, sizeof(om_mesh));
+  m->cyclic = CYCLIC_LENGTH;
   m->nx = nx; m->ny = ny; m->nl = nl; m->periodic = periodic ? 1 : 0;
   m->full_rings = (options & OM_FULL_RINGS) ? 1 : 0;
   const int left = (options & OM_LEFT_ORIENTED) ? 1 : 0;
@@ -627,6 +637,374 @@ om_mesh *om_mesh_analytic(int nx, int ny, int nl, double Lx, double Ly,
   init_nboundary_lay(m);
   return m;
 }
+
+/* ------------------------------------------------------------------------ */
+/* mesh from the ASCII mesh files: mesh_setup (lib/oce_mesh.F90:49-94) on one */
+/* process, followed by the ALE arrays of tracer_init_ale_arrays             */
+/* (lib/tracer_c_interface.F90:875-929) and the MUSCL set-up                 */
+/* ------------------------------------------------------------------------ */
+
+/* r2g_matrix (lib/gen_modules_rotate_grid.F90:33-56); R[i][j] = r2g_matrix(i+1, j+1) */
+static void rot_matrix(double al, double be, double ga, double R[3][3]) {
+  R[0][0] = cos(ga) * cos(al) - sin(ga) * cos(be) * sin(al);
+  R[0][1] = cos(ga) * sin(al) + sin(ga) * cos(be) * cos(al);
+  R[0][2] = sin(ga) * sin(be);
+  R[1][0] = -sin(ga) * cos(al) - cos(ga) * cos(be) * sin(al);
+  R[1][1] = -sin(ga) * sin(al) + cos(ga) * cos(be) * cos(al);
+  R[1][2] = cos(ga) * sin(be);
+  R[2][0] = sin(be) * sin(al);
+  R[2][1] = -sin(be) * cos(al);
+  R[2][2] = cos(be);
+}
+
+/* lib/gen_modules_rotate_grid.F90:58-80 (rotated -> geographical) */
+static void rot_r2g(double R[3][3], double rlon, double rlat, double *glon, double *glat) {
+  double xr = cos(rlat) * cos(rlon), yr = cos(rlat) * sin(rlon), zr = sin(rlat);
+  double xg = R[0][0] * xr + R[1][0] * yr + R[2][0] * zr;
+  double yg = R[0][1] * xr + R[1][1] * yr + R[2][1] * zr;
+  double zg = R[0][2] * xr + R[1][2] * yr + R[2][2] * zr;
+  *glat = asin(zg);
+  *glon = (yg == 0.0 && xg == 0.0) ? 0.0 : atan2(yg, xg);
+}
+
+/* lib/gen_modules_rotate_grid.F90:84-106 (geographical -> rotated) */
+static void rot_g2r(double R[3][3], double glon, double glat, double *rlon, double *rlat) {
+  double xg = cos(glat) * cos(glon), yg = cos(glat) * sin(glon), zg = sin(glat);
+  double xr = R[0][0] * xg + R[0][1] * yg + R[0][2] * zg;
+  double yr = R[1][0] * xg + R[1][1] * yg + R[1][2] * zg;
+  double zr = R[2][0] * xg + R[2][1] * yg + R[2][2] * zg;
+  *rlat = asin(zr);
+  *rlon = (yr == 0.0 && xr == 0.0) ? 0.0 : atan2(yr, xr);
+}
+
+static FILE *open_mesh_file(const char *dir, const char *name, char *err, int errlen) {
+  char path[4096];
+  snprintf(path, sizeof path, "%s/%s", dir, name);
+  FILE *f = fopen(path, "r");
+  if (!f && err) snprintf(err, (size_t)errlen, "cannot open %s", path);
+  return f;
+}
+
+static int read_ints(FILE *f, int *v, long n) {
+  for (long i = 0; i < n; i++)
+    if (fscanf(f, "%d", &v[i]) != 1) return -1;
+  return 0;
+}
+static int read_dbls(FILE *f, double *v, long n) {
+  for (long i = 0; i < n; i++)
+    if (fscanf(f, "%lf", &v[i]) != 1) return -1;
+  return 0;
+}
+
+#define MESH_FAIL(...)                                          \
+  do {                                                          \
+    if (err) snprintf(err, (size_t)errlen, __VA_ARGS__);        \
+    if (f) fclose(f);                                           \
+    om_mesh_free(m);                                            \
+    return NULL;                                                \
+  } while (0)
+
+om_mesh *om_mesh_from_files(const char *dir, int rotate, double alpha, double beta, double gamma,
+                            double angle_scale, double cyclic_length, char *err, int errlen) {
+  om_mesh *m = (om_mesh *)calloc(1, sizeof(om_mesh));
+  FILE *f = NULL;
+  const double rad = PI_F / 180.0; /* lib/oce_modules.F90:20 */
+  double R[3][3];
+  rot_matrix(alpha * angle_scale, beta * angle_scale, gamma * angle_scale, R);
+  m->cyclic = cyclic_length;
+  m->full_rings = 1;
+
+  /* nod2d.out and the rotation (lib/oce_mesh.F90:221-368) */
+  if (!(f = open_mesh_file(dir, "nod2d.out", err, errlen))) MESH_FAIL("cannot open nod2d.out");
+  int N = 0;
+  if (fscanf(f, "%d", &N) != 1 || N < 3) MESH_FAIL("nod2d.out: bad node count");
+  m->nod2D = m->nod2D_total = N;
+  m->coord = (double *)calloc((size_t)2 * N, sizeof(double));
+  double xp, yp;
+  rot_r2g(R, 0.0 * rad, 90.0 * rad, &xp, &yp);
+  xp = xp / rad;
+  yp = yp / rad;
+  const double dbox = 2.5;
+  int isrot = 0, mustrot = 1;
+  for (int n = 1; n <= N; n++) {
+    int id, flag;
+    double lon, lat;
+    if (fscanf(f, "%d %lf %lf %d", &id, &lon, &lat, &flag) != 4) MESH_FAIL("nod2d.out: short record %d", n);
+    double offset = 0.0;
+    if (lon > 180.0) offset = -360.0;
+    else if (lon < -180.0) offset = 360.0;
+    int inbox = lon + offset >= xp - dbox && lon + offset <= xp + dbox && lat >= yp - dbox && lat <= yp + dbox;
+    if (rotate && inbox) isrot = 1;
+    if (!rotate && inbox) mustrot = 0;
+    double x = lon * rad, y = lat * rad;
+    if (rotate) {
+      double rx = x, ry = y;
+      rot_g2r(R, rx, ry, &x, &y);
+    }
+    A2(m->coord, 1, n, 2) = x;
+    A2(m->coord, 2, n, 2) = y;
+  }
+  fclose(f);
+  f = NULL;
+  if (rotate && isrot) MESH_FAIL("the mesh seems to be rotated already (ocean nodes next to the rotated pole)");
+  if (!rotate && mustrot) MESH_FAIL("the mesh seems to be unrotated (no ocean nodes next to the rotated pole)");
+
+  /* elem2d.out (lib/oce_mesh.F90:370-437) and test_tri (:1565-1615) */
+  if (!(f = open_mesh_file(dir, "elem2d.out", err, errlen))) MESH_FAIL("cannot open elem2d.out");
+  int T = 0;
+  if (fscanf(f, "%d", &T) != 1 || T < 1) MESH_FAIL("elem2d.out: bad element count");
+  m->elem2D = T;
+  m->elem2D_nodes = (int *)calloc((size_t)3 * T, sizeof(int));
+  if (read_ints(f, m->elem2D_nodes, 3L * T)) MESH_FAIL("elem2d.out: short file");
+  fclose(f);
+  f = NULL;
+  for (long i = 0; i < 3L * T; i++)
+    if (m->elem2D_nodes[i] < 1 || m->elem2D_nodes[i] > N) MESH_FAIL("elem2d.out: node out of range");
+  for (int e = 1; e <= T; e++) {
+    int *el = &A2(m->elem2D_nodes, 1, e, 3);
+    double a1 = A2(m->coord, 1, el[0], 2), a2 = A2(m->coord, 2, el[0], 2);
+    double b1 = A2(m->coord, 1, el[1], 2) - a1, b2 = A2(m->coord, 2, el[1], 2) - a2;
+    double c1 = A2(m->coord, 1, el[2], 2) - a1, c2 = A2(m->coord, 2, el[2], 2) - a2;
+    trim_cyc(&b1, m->cyclic);
+    trim_cyc(&c1, m->cyclic);
+    double r = b1 * c2 - b2 * c1;
+    if (r > 0.0) {
+      int t = el[1];
+      el[1] = el[2];
+      el[2] = t;
+    }
+  }
+
+  /* aux3d.out: levels and depths (lib/oce_mesh.F90:439-600) */
+  if (!(f = open_mesh_file(dir, "aux3d.out", err, errlen))) MESH_FAIL("cannot open aux3d.out");
+  int nl = 0;
+  if (fscanf(f, "%d", &nl) != 1 || nl < 3) MESH_FAIL("aux3d.out: nl < 3");
+  m->nl = nl;
+  m->zbar = (double *)calloc((size_t)nl, sizeof(double));
+  m->Z = (double *)calloc((size_t)nl - 1, sizeof(double));
+  if (read_dbls(f, m->zbar, nl)) MESH_FAIL("aux3d.out: short level list");
+  if (m->zbar[1] > 0.0)
+    for (int k = 0; k < nl; k++) m->zbar[k] = -m->zbar[k];
+  for (int k = 0; k < nl - 1; k++) m->Z[k] = 0.5 * (m->zbar[k] + m->zbar[k + 1]);
+  double *depth = (double *)calloc((size_t)N, sizeof(double));
+  int bad = read_dbls(f, depth, N);
+  free(depth);
+  if (bad) MESH_FAIL("aux3d.out: short depth list");
+  fclose(f);
+  f = NULL;
+  m->max_depth = -m->zbar[nl - 1];
+
+  /* edgenum.out, edges.out, edge_tri.out (lib/oce_mesh.F90:1617-1848) */
+  if (!(f = open_mesh_file(dir, "edgenum.out", err, errlen))) MESH_FAIL("cannot open edgenum.out");
+  int E = 0, E_in = 0;
+  if (fscanf(f, "%d %d", &E, &E_in) != 2 || E < 1) MESH_FAIL("edgenum.out: bad edge count");
+  fclose(f);
+  f = NULL;
+  m->edge2D = E;
+  m->edges = (int *)calloc((size_t)2 * E, sizeof(int));
+  m->edge_tri = (int *)calloc((size_t)2 * E, sizeof(int));
+  if (!(f = open_mesh_file(dir, "edges.out", err, errlen))) MESH_FAIL("cannot open edges.out");
+  if (read_ints(f, m->edges, 2L * E)) MESH_FAIL("edges.out: short file");
+  fclose(f);
+  f = NULL;
+  if (!(f = open_mesh_file(dir, "edge_tri.out", err, errlen))) MESH_FAIL("cannot open edge_tri.out");
+  if (read_ints(f, m->edge_tri, 2L * E)) MESH_FAIL("edge_tri.out: short file");
+  fclose(f);
+  f = NULL;
+  for (long i = 0; i < 2L * E; i++) {
+    if (m->edges[i] < 1 || m->edges[i] > N) MESH_FAIL("edges.out: node out of range");
+    if (m->edge_tri[i] < 0) m->edge_tri[i] = 0;
+    if (m->edge_tri[i] > T) MESH_FAIL("edge_tri.out: element out of range");
+  }
+  for (int e = 1; e <= E; e++)
+    if (A2(m->edge_tri, 1, e, 2) < 1) MESH_FAIL("edge_tri.out: edge %d has no first element", e);
+
+  /* find_neighbors (lib/oce_mesh.F90:1850-1999): nod_in_elem2D in ascending
+   * element order, and every element needs at least two neighbours */
+  build_nod_in_elem(m, N);
+  {
+    int *cnt = (int *)calloc((size_t)T, sizeof(int));
+    int *nb = (int *)calloc((size_t)T, sizeof(int));
+    for (int e = 1; e <= E; e++)
+      for (int k = 1; k <= 2; k++) {
+        int q = A2(m->edge_tri, k, e, 2);
+        if (q > 0) {
+          cnt[q - 1]++;
+          int other = A2(m->edge_tri, 3 - k, e, 2);
+          if (other > 0) nb[q - 1]++;
+        }
+      }
+    int ok = 1;
+    for (int t = 0; t < T; t++)
+      if (cnt[t] != 3 || nb[t] < 2) ok = 0;
+    free(cnt);
+    free(nb);
+    if (!ok) MESH_FAIL("an element has not three edges or fewer than two neighbours");
+  }
+
+  /* find_levels (lib/oce_mesh.F90:807-1001): elvls.out, nlvls.out */
+  m->nlevels = (int *)calloc((size_t)T, sizeof(int));
+  m->ulevels = (int *)calloc((size_t)T, sizeof(int));
+  m->nlevels_nod2D = (int *)calloc((size_t)N, sizeof(int));
+  m->ulevels_nod2D = (int *)calloc((size_t)N, sizeof(int));
+  if (!(f = open_mesh_file(dir, "elvls.out", err, errlen))) MESH_FAIL("cannot open elvls.out");
+  if (read_ints(f, m->nlevels, T)) MESH_FAIL("elvls.out: short file");
+  fclose(f);
+  f = NULL;
+  if (!(f = open_mesh_file(dir, "nlvls.out", err, errlen))) MESH_FAIL("cannot open nlvls.out");
+  if (read_ints(f, m->nlevels_nod2D, N)) MESH_FAIL("nlvls.out: short file");
+  fclose(f);
+  f = NULL;
+  for (int t = 0; t < T; t++) {
+    m->ulevels[t] = 1;
+    if (m->nlevels[t] < 3 || m->nlevels[t] > nl) MESH_FAIL("elvls.out: level outside [3, nl]");
+  }
+  for (int n = 0; n < N; n++) {
+    m->ulevels_nod2D[n] = 1;
+    if (m->nlevels_nod2D[n] < 3 || m->nlevels_nod2D[n] > nl) MESH_FAIL("nlvls.out: level outside [3, nl]");
+  }
+
+  /* find_levels_min_e2n (lib/oce_mesh.F90:1522-1560) */
+  m->nlevels_nod2D_min = (int *)calloc((size_t)N, sizeof(int));
+  m->ulevels_nod2D_max = (int *)calloc((size_t)N, sizeof(int));
+  for (int node = 1; node <= N; node++) {
+    int mn = 1 << 30, mx = -(1 << 30);
+    for (int j = 1; j <= m->nod_in_elem2D_num[node - 1]; j++) {
+      int e = A2(m->nod_in_elem2D, j, node, m->max_nie);
+      mn = imin2(mn, m->nlevels[e - 1]);
+      mx = imax2(mx, m->ulevels[e - 1]);
+    }
+    m->nlevels_nod2D_min[node - 1] = mn;
+    m->ulevels_nod2D_max[node - 1] = mx;
+  }
+
+  /* mesh_areas (lib/oce_mesh.F90:2043-2309), no cavities */
+  m->elem_area = (double *)calloc((size_t)T, sizeof(double));
+  m->area = (double *)calloc((size_t)nl * N, sizeof(double));
+  m->areasvol = (double *)calloc((size_t)nl * N, sizeof(double));
+  for (int e = 1; e <= T; e++) {
+    const int *el = &A2(m->elem2D_nodes, 1, e, 3);
+    double ay = (A2(m->coord, 2, el[0], 2) + A2(m->coord, 2, el[1], 2) + A2(m->coord, 2, el[2], 2)) / 3.0;
+    ay = cos(ay);
+    double a1 = A2(m->coord, 1, el[1], 2) - A2(m->coord, 1, el[0], 2);
+    double a2 = A2(m->coord, 2, el[1], 2) - A2(m->coord, 2, el[0], 2);
+    double b1 = A2(m->coord, 1, el[2], 2) - A2(m->coord, 1, el[0], 2);
+    double b2 = A2(m->coord, 2, el[2], 2) - A2(m->coord, 2, el[0], 2);
+    trim_cyc(&a1, m->cyclic);
+    trim_cyc(&b1, m->cyclic);
+    a1 = a1 * ay;
+    b1 = b1 * ay;
+    m->elem_area[e - 1] = 0.5 * fabs(a1 * b2 - b1 * a2);
+  }
+  for (int n = 1; n <= N; n++)
+    for (int j = 1; j <= m->nod_in_elem2D_num[n - 1]; j++) {
+      int elem = A2(m->nod_in_elem2D, j, n, m->max_nie);
+      for (int nz = m->ulevels[elem - 1]; nz <= m->nlevels[elem - 1] - 1; nz++)
+        A2(m->area, nz, n, nl) = A2(m->area, nz, n, nl) + m->elem_area[elem - 1] / 3.0;
+    }
+  for (int n = 1; n <= N; n++)
+    for (int nz = m->ulevels_nod2D[n - 1]; nz <= m->nlevels_nod2D[n - 1] - 1; nz++)
+      A2(m->areasvol, nz, n, nl) = A2(m->area, nz, n, nl);
+  for (int e = 0; e < T; e++) m->elem_area[e] = m->elem_area[e] * R_EARTH * R_EARTH;
+  for (long i = 0; i < (long)nl * N; i++) {
+    m->area[i] = m->area[i] * R_EARTH * R_EARTH;
+    m->areasvol[i] = m->areasvol[i] * R_EARTH * R_EARTH;
+  }
+
+  /* mesh_auxiliary_arrays (lib/oce_mesh.F90:2313-2534), the arrays the
+   * advection reads */
+  m->elem_cos = (double *)calloc((size_t)T, sizeof(double));
+  double *cx = (double *)calloc((size_t)T, sizeof(double));
+  double *cy = (double *)calloc((size_t)T, sizeof(double));
+  for (int e = 1; e <= T; e++) {
+    elem_center(m, &A2(m->elem2D_nodes, 1, e, 3), &cx[e - 1], &cy[e - 1]);
+    m->elem_cos[e - 1] = cos(cy[e - 1]);
+  }
+  m->edge_dxdy = (double *)calloc((size_t)2 * E, sizeof(double));
+  m->edge_cross_dxdy = (double *)calloc((size_t)4 * E, sizeof(double));
+  for (int n = 1; n <= E; n++) {
+    int ed1 = A2(m->edges, 1, n, 2), ed2 = A2(m->edges, 2, n, 2);
+    double a1 = A2(m->coord, 1, ed2, 2) - A2(m->coord, 1, ed1, 2);
+    double a2 = A2(m->coord, 2, ed2, 2) - A2(m->coord, 2, ed1, 2);
+    trim_cyc(&a1, m->cyclic);
+    A2(m->edge_dxdy, 1, n, 2) = a1;
+    A2(m->edge_dxdy, 2, n, 2) = a2;
+    double ex, ey;
+    edge_center(m, ed1, ed2, &ex, &ey);
+    for (int s = 1; s <= 2; s++) {
+      int el = A2(m->edge_tri, s, n, 2);
+      if (el <= 0) {
+        A2(m->edge_cross_dxdy, 2 * s - 1, n, 4) = 0.0;
+        A2(m->edge_cross_dxdy, 2 * s, n, 4) = 0.0;
+        continue;
+      }
+      double b1 = cx[el - 1] - ex, b2 = cy[el - 1] - ey;
+      trim_cyc(&b1, m->cyclic);
+      b1 = b1 * m->elem_cos[el - 1];
+      b1 = b1 * R_EARTH;
+      b2 = b2 * R_EARTH;
+      A2(m->edge_cross_dxdy, 2 * s - 1, n, 4) = b1;
+      A2(m->edge_cross_dxdy, 2 * s, n, 4) = b2;
+    }
+  }
+  free(cx);
+  free(cy);
+  m->gradient_sca = (double *)calloc((size_t)6 * T, sizeof(double));
+  for (int e = 1; e <= T; e++) {
+    const int *el = &A2(m->elem2D_nodes, 1, e, 3);
+    double dX31 = A2(m->coord, 1, el[2], 2) - A2(m->coord, 1, el[0], 2);
+    trim_cyc(&dX31, m->cyclic);
+    dX31 = m->elem_cos[e - 1] * dX31;
+    double dX21 = A2(m->coord, 1, el[1], 2) - A2(m->coord, 1, el[0], 2);
+    trim_cyc(&dX21, m->cyclic);
+    dX21 = m->elem_cos[e - 1] * dX21;
+    double dY31 = A2(m->coord, 2, el[2], 2) - A2(m->coord, 2, el[0], 2);
+    double dY21 = A2(m->coord, 2, el[1], 2) - A2(m->coord, 2, el[0], 2);
+    double fac = -0.5 * R_EARTH / m->elem_area[e - 1];
+    double *gs = &A2(m->gradient_sca, 1, e, 6);
+    gs[0] = (-dY31 + dY21) * fac;
+    gs[1] = dY31 * fac;
+    gs[2] = -dY21 * fac;
+    gs[3] = (dX31 - dX21) * fac;
+    gs[4] = -dX31 * fac;
+    gs[5] = dX21 * fac;
+  }
+
+  /* coordinate extents (the domain box of the seeded synthetic fields) */
+  double x0 = A2(m->coord, 1, 1, 2), x1 = x0, y0 = A2(m->coord, 2, 1, 2), y1 = y0;
+  for (int n = 2; n <= N; n++) {
+    x0 = fmin2(x0, A2(m->coord, 1, n, 2)); x1 = fmax2(x1, A2(m->coord, 1, n, 2));
+    y0 = fmin2(y0, A2(m->coord, 2, n, 2)); y1 = fmax2(y1, A2(m->coord, 2, n, 2));
+  }
+  m->Lx = (x1 - x0) * R_EARTH;
+  m->Ly = (y1 - y0) * R_EARTH;
+
+  /* ALE arrays (lib/tracer_c_interface.F90:875-929) */
+  const int nz = nl - 1;
+  m->hnode = (double *)calloc((size_t)nz * N, sizeof(double));
+  m->hnode_new = (double *)calloc((size_t)nz * N, sizeof(double));
+  m->helem = (double *)calloc((size_t)nz * T, sizeof(double));
+  m->zbar_3d_n = (double *)calloc((size_t)nl * N, sizeof(double));
+  m->Z_3d_n = (double *)calloc((size_t)nz * N, sizeof(double));
+  for (int n = 1; n <= N; n++) {
+    for (int k = 1; k <= nz; k++) {
+      A2(m->hnode, k, n, nz) = m->zbar[k - 1] - m->zbar[k];
+      A2(m->hnode_new, k, n, nz) = A2(m->hnode, k, n, nz);
+      A2(m->Z_3d_n, k, n, nz) = m->Z[k - 1];
+    }
+    for (int k = 1; k <= nl; k++) A2(m->zbar_3d_n, k, n, nl) = m->zbar[k - 1];
+  }
+  for (int e = 1; e <= T; e++)
+    for (int k = 1; k <= nz; k++) A2(m->helem, k, e, nz) = m->zbar[k - 1] - m->zbar[k];
+
+  /* MUSCL set-up (lib/oce_muscl_adv.F90:38-357) */
+  m->edge_up_dn_tri = (int *)calloc((size_t)2 * E, sizeof(int));
+  m->nboundary_lay = (int *)calloc((size_t)N, sizeof(int));
+  find_up_downwind_triangles(m);
+  init_nboundary_lay(m);
+  return m;
+}
+#undef MESH_FAIL
 
 static void work_free(struct om_work_s *w);
 void om_mesh_free(om_mesh *m) {

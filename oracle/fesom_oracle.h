@@ -42,6 +42,19 @@ enum { OM_FULL_RINGS = 1, OM_LEFT_ORIENTED = 2 };
 om_mesh *om_mesh_analytic(int nx, int ny, int nl, double Lx, double Ly,
                           double max_depth, int periodic, int options,
                           const int *node_K);
+/* Build a mesh from the reference's ASCII mesh files in dir (nod2d.out,
+ * elem2d.out, aux3d.out, edgenum.out, edges.out, edge_tri.out, elvls.out,
+ * nlvls.out) as mesh_setup does on one process (lib/oce_mesh.F90:49-94):
+ * node coordinates in degrees -> radians, rotated by the Euler angles
+ * (alpha, beta, gamma) x angle_scale when rotate != 0, elements oriented by
+ * test_tri, levels from elvls/nlvls, spherical areas and auxiliary arrays with
+ * the given cyclic_length (in radians of longitude), then the ALE thicknesses
+ * of tracer_init_ale_arrays and the MUSCL tables.  The reference's defaults
+ * are rotate = 1, (50, 15, -90), angle_scale = 1 (its
+ * set_mesh_transform_matrix passes the values to cos/sin as they are) and
+ * cyclic_length = 360.  NULL on failure, with a message in err. */
+om_mesh *om_mesh_from_files(const char *dir, int rotate, double alpha, double beta, double gamma,
+                            double angle_scale, double cyclic_length, char *err, int errlen);
 void om_mesh_free(om_mesh *m);
 
 /* dims[0..5] = nl, nod2D, elem2D, edge2D, max_nod_in_elem, periodic */

@@ -44,6 +44,8 @@ class Oracle:
         lib.om_mesh_analytic.restype = vp
         lib.om_mesh_analytic.argtypes = [ci, ci, ci, cd, cd, cd, ci, ci, vp]
         lib.om_mesh_free.argtypes = [vp]
+        lib.om_mesh_from_files.restype = vp
+        lib.om_mesh_from_files.argtypes = [ctypes.c_char_p, ci, cd, cd, cd, cd, cd, ctypes.c_char_p, ci]
         lib.om_mesh_dims.argtypes = [vp, vp]
         lib.om_mesh_len.restype = ctypes.c_long
         lib.om_mesh_len.argtypes = [vp, ctypes.c_char_p]
@@ -79,6 +81,24 @@ class OracleMesh:
         d = np.zeros(6, dtype=np.int32)
         oracle.lib.om_mesh_dims(self.h, _p(d))
         self.nl, self.nod2D, self.elem2D, self.edge2D, self.max_nie = (int(x) for x in d[:5])
+
+    @classmethod
+    def from_files(cls, oracle: Oracle, mesh_dir, rotate=True, alpha=50.0, beta=15.0, gamma=-90.0,
+                   angle_scale=1.0, cyclic_length=360.0):
+        """A mesh read from the reference's ASCII mesh files (mesh_setup of
+        lib/oce_mesh.F90:49-94 restated; defaults are the reference's)."""
+        self = cls.__new__(cls)
+        self.o = oracle
+        err = ctypes.create_string_buffer(512)
+        h = oracle.lib.om_mesh_from_files(str(mesh_dir).encode(), int(bool(rotate)), alpha, beta, gamma,
+                                          angle_scale, cyclic_length, err, len(err))
+        if not h:
+            raise ValueError("oracle mesh: " + err.value.decode())
+        self.h = ctypes.c_void_p(h)
+        d = np.zeros(6, dtype=np.int32)
+        oracle.lib.om_mesh_dims(self.h, _p(d))
+        self.nl, self.nod2D, self.elem2D, self.edge2D, self.max_nie = (int(x) for x in d[:5])
+        return self
 
     def __del__(self):
         try:

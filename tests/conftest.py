@@ -43,3 +43,14 @@ def api(lib):
 
 def f64(a):
     return np.asfortranarray(np.asarray(a, dtype=np.float64))
+
+
+@pytest.fixture(scope="session")
+def pi_mesh_dir(tmp_path_factory):
+    """The reference's ASCII pi mesh (tests/golden/pi/*.out.gz, byte copies),
+    unpacked into a temporary mesh directory."""
+    import gzip
+    d = tmp_path_factory.mktemp("pi_mesh")
+    for gz in (ROOT / "tests" / "golden" / "pi").glob("*.out.gz"):
+        (d / gz.name[:-3]).write_bytes(gzip.decompress(gz.read_bytes()))
+    return d
