@@ -1,6 +1,6 @@
 """The CUDA step on the reference's pi mesh (irregular spherical triangles,
-elem_cos != 1, valence 3 to 8, real bathymetry of 5 to 47 levels, closed
-coastlines), read through tracer_load_mesh_from_files: bit-identical to the
+elem_cos != 1, 2 to 8 elements per node, real bathymetry of 4 to 45 wet
+layers, closed coastlines), read through tracer_load_mesh_from_files: bit-identical to the
 oracle stepping on its own restatement of the same mesh files, in the
 reference's conventions and in FESOM2's; conservation, constant preservation
 and the FCT bounds over longer runs."""
