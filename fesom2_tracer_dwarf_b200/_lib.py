@@ -121,6 +121,23 @@ SIGNATURES = {
     "tracer_advect_device_noalloc": (ctypes.c_int, [ctypes.c_int, _vp, _vp, _vp, ctypes.c_double]),
     "tracer_noalloc_scratch_bytes": (ctypes.c_longlong, []),
     "tracer_last_error": (ctypes.c_char_p, []),
+    "tracer_partition_read_dist": (ctypes.c_int, [ctypes.c_char_p, _vp, _vp]),
+    "tracer_partition_halo": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp,
+                                             ctypes.c_int]),
+    "tracer_partition_part_dims": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp]),
+    "tracer_dd_setup": (ctypes.c_int, [_vp, ctypes.c_int, _vp, ctypes.c_int, ctypes.c_int]),
+    "tracer_dd_destroy": (ctypes.c_int, []),
+    "tracer_dd_part_info": (ctypes.c_int, [ctypes.c_int, _vp]),
+    "tracer_dd_allocate_tracers": (ctypes.c_int, [ctypes.c_int]),
+    "tracer_dd_set_scheme": (ctypes.c_int, [ctypes.c_int, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p,
+                                            ctypes.c_double, ctypes.c_double]),
+    "tracer_dd_set_velocity": (ctypes.c_int, [_vp, _vp]),
+    "tracer_dd_set_values": (ctypes.c_int, [ctypes.c_int, _vp]),
+    "tracer_dd_get_values": (ctypes.c_int, [ctypes.c_int, _vp]),
+    "tracer_dd_steps": (ctypes.c_int, [ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_int]),
+    "tracer_dd_transfer_nodes": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int]),
+    "tracer_dd_pack": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp]),
+    "tracer_dd_unpack": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp]),
 }
 
 REFERENCE_SYMBOLS = [

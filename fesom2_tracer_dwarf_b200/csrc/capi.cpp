@@ -12,8 +12,10 @@
 
 #include "../../include/fesom_tracer.h"
 #include "batch.hpp"
+#include "dd.hpp"
 #include "engine.hpp"
 #include "output.hpp"
+#include "partition.hpp"
 
 using namespace fesom;
 
@@ -38,6 +40,7 @@ struct State {
   int sround = 0;  // rounding of 16-bit stores (tracer_set_rounding)
 };
 State g;
+std::unique_ptr<Decomposition> g_dd;  // domain-decomposed runner (tracer_dd_*)
 
 int fail(const std::string &msg) {
   set_last_error(msg);
@@ -160,6 +163,7 @@ int tracer_load_mesh_from_files(const char *mesh_path) {
 
 int tracer_cleanup(void) {
   return guarded([&] {
+    g_dd.reset();
     g.eng.reset();
     g = State();
     return 0;
@@ -947,6 +951,150 @@ int tracer_learn_step(const double *T_in, const double *T_target, double dt, dou
 // ---------------------------------------------------------------------------
 namespace {
 ScalarOutput g_scalars;
+}
+
+int tracer_partition_read_dist(const char *dist_dir, int *node_part, int *nparts) {
+  return guarded([&] {
+    if (!g.mesh) return fail("tracer_partition_read_dist: no mesh");
+    if (!dist_dir || !node_part || !nparts) return fail("tracer_partition_read_dist: null argument");
+    int np = 0;
+    std::vector<int> p = read_dist_partition(dist_dir, g.mesh->nod2D, &np);
+    std::memcpy(node_part, p.data(), p.size() * sizeof(int));
+    *nparts = np;
+    return 0;
+  });
+}
+
+static std::vector<int> part_map(const int *node_part, int nparts) {
+  if (!g.mesh) throw std::runtime_error("no mesh");
+  if (!node_part) throw std::invalid_argument("null node_part");
+  std::vector<int> p(node_part, node_part + g.mesh->nod2D);
+  for (int q : p)
+    if (q < 0 || q >= nparts) throw std::invalid_argument("node part outside [0, nparts)");
+  return p;
+}
+
+int tracer_partition_halo(const int *node_part, int nparts, int from, int to, int rings, int *out, int capacity) {
+  return guarded([&] {
+    const std::vector<int> v = halo_transfer(*g.mesh, part_map(node_part, nparts), from, to, rings);
+    if ((int)v.size() > capacity) return fail("tracer_partition_halo: capacity too small");
+    for (size_t i = 0; i < v.size(); i++) out[i] = v[i] + 1;
+    return (int)v.size();
+  });
+}
+
+int tracer_partition_part_dims(const int *node_part, int nparts, int part, int rings, int *dims4) {
+  return guarded([&] {
+    const MeshPart mp = build_mesh_part(*g.mesh, part_map(node_part, nparts), part, rings);
+    dims4[0] = mp.owned;
+    dims4[1] = mp.mesh.nod2D;
+    dims4[2] = mp.mesh.elem2D;
+    dims4[3] = mp.mesh.edge2D;
+    return 0;
+  });
+}
+
+int tracer_dd_setup(const int *node_part, int nparts, const int *local_parts, int nlocal, int rings) {
+  return guarded([&] {
+    if (!local_parts || nlocal < 1) return fail("tracer_dd_setup: no local part");
+    g_dd.reset();
+    g_dd.reset(new Decomposition(*g.mesh, part_map(node_part, nparts), nparts,
+                                 std::vector<int>(local_parts, local_parts + nlocal), rings, g.prec));
+    return 0;
+  });
+}
+
+static Decomposition &dd() {
+  if (!g_dd) throw std::runtime_error("no domain decomposition: call tracer_dd_setup");
+  return *g_dd;
+}
+
+int tracer_dd_destroy(void) {
+  return guarded([&] {
+    g_dd.reset();
+    return 0;
+  });
+}
+
+int tracer_dd_part_info(int i, int *info5) {
+  return guarded([&] {
+    const MeshPart &mp = dd().part(i);
+    info5[0] = mp.part;
+    info5[1] = mp.owned;
+    info5[2] = mp.mesh.nod2D;
+    info5[3] = mp.mesh.elem2D;
+    info5[4] = mp.mesh.edge2D;
+    return 0;
+  });
+}
+
+int tracer_dd_allocate_tracers(int ntr) {
+  return guarded([&] {
+    if (ntr < 1) return fail("tracer_dd_allocate_tracers: ntr < 1");
+    dd().allocate_tracers(ntr);
+    return 0;
+  });
+}
+
+int tracer_dd_set_scheme(int tracer_id, const char *hor, const char *ver, const char *lim, double ph, double pv) {
+  return guarded([&] {
+    dd().set_scheme(tracer_id - 1, parse_scheme(hor, ver, lim, ph, pv));
+    return 0;
+  });
+}
+
+int tracer_dd_set_velocity(const double *uv, const double *w) {
+  return guarded([&] {
+    if (!uv || !w) return fail("tracer_dd_set_velocity: null array");
+    dd().set_velocity(uv, w);
+    return 0;
+  });
+}
+
+int tracer_dd_set_values(int tracer_id, const double *values) {
+  return guarded([&] {
+    if (!values) return fail("tracer_dd_set_values: null array");
+    dd().set_values(tracer_id - 1, values);
+    return 0;
+  });
+}
+
+int tracer_dd_get_values(int tracer_id, double *values) {
+  return guarded([&] {
+    if (!values) return fail("tracer_dd_get_values: null array");
+    dd().get_values(tracer_id - 1, values);
+    return 0;
+  });
+}
+
+int tracer_dd_steps(int nsteps, double dt, int refresh_ab, int exchange) {
+  return guarded([&] {
+    Decomposition &d = dd();
+    for (int s = 0; s < nsteps; s++) {
+      d.step(dt, refresh_ab != 0);
+      if (exchange) d.exchange_local();
+    }
+    d.synchronize();
+    return 0;
+  });
+}
+
+int tracer_dd_transfer_nodes(int i, int peer, int send) {
+  return guarded([&] { return dd().transfer_nodes(i, peer, send != 0); });
+}
+
+int tracer_dd_pack(int i, int tracer_id, int peer, double *dev_out) {
+  return guarded([&] {
+    dd().pack(i, tracer_id - 1, peer, dev_out);
+    return 0;
+  });
+}
+
+int tracer_dd_unpack(int i, int tracer_id, int peer, const double *dev_in) {
+  return guarded([&] {
+    dd().unpack(i, tracer_id - 1, peer, dev_in);
+    return 0;
+  });
 }
 
 int tracer_write_mesh(const char *output_dir) {

@@ -344,6 +344,46 @@ int tracer_scalar_output_close(void);
 /* Last error message of this thread ("" if none). */
 const char *tracer_last_error(void);
 
+/* ---- domain decomposition ------------------------------------------------
+ * Parts of the loaded mesh, each owning a set of nodes (node_part, nod2D
+ * entries in [0, nparts)) and holding `rings` (>= 3) rings of halo nodes;
+ * every part runs the ordinary step on its local mesh and only the halo
+ * values are exchanged after a step (the reference exchanges the LO
+ * solution, the FCT ratios and the new values: lib/oce_adv_tra_driver.F90:234,
+ * lib/oce_adv_tra_fct.F90:383, partitioned by lib/gen_modules_partitioning.F90).
+ * Owned values are bit-identical to a step of the whole mesh.  FP64 and FP32
+ * modes. */
+/* node -> part map (0-based) of a partition directory dist_<n> of the loaded
+ * mesh: rpart.out and the owned nodes of every my_list<part>.out
+ * (lib/oce_mesh.F90:150-200) */
+int tracer_partition_read_dist(const char *dist_dir, int *node_part, int *nparts);
+/* 1-based global ids of the nodes `from` owns in the halo of `to`, ascending;
+ * returns their count (or -1) */
+int tracer_partition_halo(const int *node_part, int nparts, int from, int to, int rings, int *out, int capacity);
+/* owned nodes, local nodes, local elements, local edges of one part (host only) */
+int tracer_partition_part_dims(const int *node_part, int nparts, int part, int rings, int *dims4);
+/* engines for local_parts[0..nlocal) of the decomposition, on this process's GPU */
+int tracer_dd_setup(const int *node_part, int nparts, const int *local_parts, int nlocal, int rings);
+int tracer_dd_destroy(void);
+/* part id, owned nodes, local nodes, local elements, local edges of local part i */
+int tracer_dd_part_info(int i, int *info5);
+int tracer_dd_allocate_tracers(int ntr);
+int tracer_dd_set_scheme(int tracer_id, const char *hor, const char *ver, const char *lim, double ph, double pv);
+/* whole-mesh arrays: uv(2, nl-1, elem2D), w(nl, nod2D), values(nl-1, nod2D) */
+int tracer_dd_set_velocity(const double *uv, const double *w);
+int tracer_dd_set_values(int tracer_id, const double *values);
+/* writes the rows of the nodes the local parts own */
+int tracer_dd_get_values(int tracer_id, double *values);
+/* nsteps steps of every tracer on every local part; exchange != 0 exchanges
+ * the halos between the local parts after each step */
+int tracer_dd_steps(int nsteps, double dt, int refresh_ab, int exchange);
+/* halo transfer of local part i with part `peer`: node count (send != 0: to
+ * the peer), and packing / unpacking of one tracer as (nl-1) x n FP64 values
+ * in device memory, in ascending global node order */
+int tracer_dd_transfer_nodes(int i, int peer, int send);
+int tracer_dd_pack(int i, int tracer_id, int peer, double *dev_out);
+int tracer_dd_unpack(int i, int tracer_id, int peer, const double *dev_in);
+
 #ifdef __cplusplus
 }
 #endif

@@ -52,5 +52,7 @@ def pi_mesh_dir(tmp_path_factory):
     import gzip
     d = tmp_path_factory.mktemp("pi_mesh")
     for gz in (ROOT / "tests" / "golden" / "pi").glob("*.out.gz"):
-        (d / gz.name[:-3]).write_bytes(gzip.decompress(gz.read_bytes()))
+        target = d / gz.name[:-3].replace("__", "/")  # dist_8__rpart.out -> dist_8/rpart.out
+        target.parent.mkdir(exist_ok=True)
+        target.write_bytes(gzip.decompress(gz.read_bytes()))
     return d

@@ -1,0 +1,104 @@
+"""Domain decomposition on the host: part maps (the reference's METIS
+partitions of the pi mesh and index strips of the analytic mesh), halo
+transfer lists, local part sizes, and the point-to-point halo exchange with
+two gloo ranks on the CPU."""
+import os
+import sys
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from test_replicas import _launch
+
+ROOT = Path(__file__).resolve().parents[1]
+
+
+def _check_plans(api, part, nparts):
+    from fesom2_tracer_dwarf_b200 import decomp
+    owned = [set(np.flatnonzero(part == p)) for p in range(nparts)]
+    assert sum(len(o) for o in owned) == part.size
+    for q in range(nparts):
+        dims = decomp.part_dims(api, part, nparts, q)
+        assert dims["owned"] == len(owned[q])
+        into_q = 0
+        for p in range(nparts):
+            if p == q:
+                continue
+            t = decomp.halo_transfer(api, part, nparts, p, q)
+            assert np.all(np.diff(t) > 0)                  # ascending global ids
+            assert set(t.tolist()) <= owned[p]             # only nodes p owns
+            into_q += t.size
+        assert dims["nodes"] == dims["owned"] + into_q      # the halo is exactly what the peers send
+        assert into_q > 0 and dims["elements"] > 0 and dims["edges"] > 0
+
+
+@pytest.mark.parametrize("n", [2, 8])
+def test_pi_mesh_metis_partitions(api, pi_mesh_dir, n):
+    from fesom2_tracer_dwarf_b200 import decomp
+    api.load_mesh_from_files(pi_mesh_dir)
+    part, nparts = decomp.read_dist(api, pi_mesh_dir / f"dist_{n}")
+    assert nparts == n
+    _check_plans(api, part, nparts)
+
+
+@pytest.mark.parametrize("n", [2, 3, 5])
+def test_analytic_strips(api, n):
+    from fesom2_tracer_dwarf_b200 import decomp
+    api.init_analytic(30, 24, 8, periodic=True, full_rings=True)
+    part = decomp.partition_by_index(api.mesh_dims()["nod2D"], n)
+    _check_plans(api, part, n)
+
+
+def test_bad_partition_files_fail_cleanly(api, pi_mesh_dir, tmp_path):
+    import shutil
+    from fesom2_tracer_dwarf_b200 import decomp
+    api.load_mesh_from_files(pi_mesh_dir)
+    d = tmp_path / "dist_2"
+    shutil.copytree(pi_mesh_dir / "dist_2", d)
+    (d / "my_list00001.out").unlink()
+    with pytest.raises(RuntimeError, match="my_list00001"):
+        decomp.read_dist(api, d)
+    shutil.copy(pi_mesh_dir / "dist_2" / "my_list00000.out", d / "my_list00001.out")
+    with pytest.raises(RuntimeError, match="bad header|disagrees|owned twice"):
+        decomp.read_dist(api, d)
+
+
+WORKER = r'''
+import json, sys
+sys.path.insert(0, sys.argv[1])
+import numpy as np, torch
+import torch.distributed as dist
+from fesom2_tracer_dwarf_b200 import FESOMTracerAdvection, decomp
+from fesom2_tracer_dwarf_b200.replicas import from_env
+r = from_env("gloo", timeout_s=60)
+api = FESOMTracerAdvection()
+api.init_analytic(20, 16, 6, periodic=True, full_rings=True)
+N, L = api.mesh_dims()["nod2D"], 5
+part = decomp.partition_by_index(N, r.world)
+send_ids = {p: decomp.halo_transfer(api, part, r.world, r.rank, p) for p in range(r.world) if p != r.rank}
+recv_ids = {p: decomp.halo_transfer(api, part, r.world, p, r.rank) for p in range(r.world) if p != r.rank}
+# every rank's copy of the field: its own rows hold 1000 * node + level, halo rows -1
+field = np.full((N, L), -1.0)
+mine = np.flatnonzero(part == r.rank)
+field[mine] = 1000.0 * mine[:, None] + np.arange(L)[None, :]
+hx = decomp.HaloExchange({p: v.size * L for p, v in send_ids.items()}, {p: v.size * L for p, v in recv_ids.items()}, "cpu")
+def pack(peer):
+    return torch.from_numpy(np.ascontiguousarray(field[send_ids[peer]]).ravel())
+def unpack(peer, buf):
+    field[recv_ids[peer]] = buf.numpy().reshape(-1, L)
+hx.exchange(pack, unpack)
+hx.exchange(pack, unpack)  # idempotent
+halo = np.concatenate([v for v in recv_ids.values()])
+ok = bool(np.array_equal(field[halo], 1000.0 * halo[:, None] + np.arange(L)[None, :]))
+print(json.dumps({"rank": r.rank, "ok": ok, "halo": int(halo.size)}))
+r.close()
+'''
+
+
+def test_halo_exchange_two_gloo_ranks():
+    import json
+    outs = _launch(["-c", WORKER, str(ROOT)])
+    res = [json.loads(o.strip().splitlines()[-1]) for o in outs]
+    assert all(d["ok"] for d in res)
+    assert all(d["halo"] > 0 for d in res)
