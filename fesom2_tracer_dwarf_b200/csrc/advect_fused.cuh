@@ -51,6 +51,36 @@ constexpr int kThreads = 256;
 #ifndef FESOM_MINB_GRAD
 #define FESOM_MINB_GRAD 5
 #endif
+// The same for the FP32-arithmetic kernels (FP32 and 16-bit storage), which
+// need fewer registers: timed on the same workload in FP32, 4 / 5 / 6 / 7
+// blocks (col2, col3: up to 8): edge best at 6 (1.98 ms), col1 at 7 (2.07),
+// col2 and col3 at 7 (1.68, 1.65; 8 no better), against 1.99 / 2.38 / 1.86 /
+// 1.97 ms with the FP64 budgets.
+#ifndef FESOM_MINB32_EDGE
+#define FESOM_MINB32_EDGE 6
+#endif
+#ifndef FESOM_MINB32_COL1
+#define FESOM_MINB32_COL1 7
+#endif
+#ifndef FESOM_MINB32_COL2
+#define FESOM_MINB32_COL2 7
+#endif
+#ifndef FESOM_MINB32_COL3
+#define FESOM_MINB32_COL3 7
+#endif
+#ifndef FESOM_MINB32_GRAD
+#define FESOM_MINB32_GRAD 5
+#endif
+template <typename R>
+struct MinBlocks {
+  static constexpr int grad = FESOM_MINB_GRAD, edge = FESOM_MINB_EDGE, col1 = FESOM_MINB_COL1, col2 = FESOM_MINB_COL2,
+                       col3 = FESOM_MINB_COL3;
+};
+template <>
+struct MinBlocks<float> {
+  static constexpr int grad = FESOM_MINB32_GRAD, edge = FESOM_MINB32_EDGE, col1 = FESOM_MINB32_COL1,
+                       col2 = FESOM_MINB32_COL2, col3 = FESOM_MINB32_COL3;
+};
 // The LO gather of k_col1 issues the loads of this many incident edges
 // together before using any of them.  Every (edge, level) and (node, level)
 // address of a cell's level lies inside its padded column, so the loads of
@@ -226,7 +256,7 @@ __device__ __forceinline__ void grad_block(const DMeshT<R> &m, const FusedArgs<R
 }
 
 template <typename R, typename TS, int NT>
-__global__ void __launch_bounds__(kThreads, FESOM_MINB_GRAD) k_grad(DMeshT<R> m, FusedArgs<R, TS> a) {
+__global__ void __launch_bounds__(kThreads, MinBlocks<R>::grad) k_grad(DMeshT<R> m, FusedArgs<R, TS> a) {
   extern __shared__ int smem[];
   grad_block<R, TS, NT>(m, a, blockIdx.x, smem);
 }
@@ -378,7 +408,7 @@ __device__ __forceinline__ void edge_block(const DMeshT<R> &m, const FusedArgs<R
 }
 
 template <typename R, typename TS, int NT, int HOR, int LIM>
-__global__ void __launch_bounds__(kThreads, FESOM_MINB_EDGE) k_edge(DMeshT<R> m, FusedArgs<R, TS> a) {
+__global__ void __launch_bounds__(kThreads, MinBlocks<R>::edge) k_edge(DMeshT<R> m, FusedArgs<R, TS> a) {
   extern __shared__ int smem[];
   edge_block<R, TS, NT, HOR, LIM>(m, a, blockIdx.x, smem);
 }
@@ -503,14 +533,15 @@ __device__ __forceinline__ void col1_block(const DMeshT<R> &m, const FusedArgs<R
             const int sl = lc + (jl - i);                        // its cell slot
             const R dzj = m.hnode[col + jl - 1];
             const R x = (w > R(0)) ? fmin2(w * a.dt / dzj, R(1)) : fmin2(-(w * a.dt / dzj), R(1));
-            const R two3 = R(2.0 / 3.0);
+            const R two3 = R(2.0 / 3.0), sixth = R(1.0 / 6.0);
             for (int t = 0; t < NT; t++) {
               const R Tc = ldT(a.TAB[t], col + jl - 1, a.off[t]);
               R aL = s_tv[t * kMaxCellsPerBlock + sl];
               R aR = (jl + 1 == nlev) ? ldT(a.TAB[t], col + nlev - 2, a.off[t]) : s_tv[t * kMaxCellsPerBlock + sl + 1];
               if ((aR - Tc) * (Tc - aL) <= R(0)) { aL = Tc; aR = Tc; }
-              if ((aR - aL) * (Tc - R(0.5) * (aL + aR)) > (aR - aL) * (aR - aL) / R(6)) aL = R(3) * Tc - R(2) * aR;
-              if ((aR - aL) * (Tc - R(0.5) * (aR + aL)) < -((aR - aL) * (aR - aL) / R(6))) aR = R(3) * Tc - R(2) * aL;
+              // x / 6 by the corrected reciprocal (correctly rounded, as in the MUSCL fluxes)
+              if ((aR - aL) * (Tc - R(0.5) * (aL + aR)) > div_rcp((aR - aL) * (aR - aL), R(6), sixth)) aL = R(3) * Tc - R(2) * aR;
+              if ((aR - aL) * (Tc - R(0.5) * (aR + aL)) < -div_rcp((aR - aL) * (aR - aL), R(6), sixth)) aR = R(3) * Tc - R(2) * aL;
               const R aj = R(6) * (Tc - R(0.5) * (aL + aR));
               R tt;
               if (w > R(0)) tt = (-aL - R(0.5) * x * (aR - aL + (R(1) - two3 * x) * aj));
@@ -581,7 +612,7 @@ __device__ __forceinline__ void col1_block(const DMeshT<R> &m, const FusedArgs<R
 }
 
 template <typename R, typename TS, int NT, int VER, int LIM>
-__global__ void __launch_bounds__(kThreads, FESOM_MINB_COL1) k_col1(DMeshT<R> m, FusedArgs<R, TS> a) {
+__global__ void __launch_bounds__(kThreads, MinBlocks<R>::col1) k_col1(DMeshT<R> m, FusedArgs<R, TS> a) {
   extern __shared__ int smem[];
   col1_block<R, TS, NT, VER, LIM>(m, a, blockIdx.x, smem);
 }
@@ -727,7 +758,7 @@ __device__ __forceinline__ void col2_block(const DMeshT<R> &m, const FusedArgs<R
 }
 
 template <typename R, typename TS, int NT>
-__global__ void __launch_bounds__(kThreads, FESOM_MINB_COL2) k_col2(DMeshT<R> m, FusedArgs<R, TS> a) {
+__global__ void __launch_bounds__(kThreads, MinBlocks<R>::col2) k_col2(DMeshT<R> m, FusedArgs<R, TS> a) {
   extern __shared__ int smem[];
   col2_block<R, TS, NT>(m, a, blockIdx.x, smem);
 }
@@ -821,7 +852,7 @@ __device__ __forceinline__ void col3_block(const DMeshT<R> &m, const FusedArgs<R
 }
 
 template <typename R, typename TS, int NT, int LIM>
-__global__ void __launch_bounds__(kThreads, FESOM_MINB_COL3) k_col3(DMeshT<R> m, FusedArgs<R, TS> a) {
+__global__ void __launch_bounds__(kThreads, MinBlocks<R>::col3) k_col3(DMeshT<R> m, FusedArgs<R, TS> a) {
   extern __shared__ int smem[];
   col3_block<R, TS, NT, LIM>(m, a, blockIdx.x, smem);
 }
