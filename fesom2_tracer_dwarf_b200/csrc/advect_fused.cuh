@@ -784,6 +784,20 @@ __device__ __forceinline__ R limit_v(const R *av, const R *rp, const R *rm, int 
 // ---------------------------------------------------------------------------
 // k_col3: limiting + flux2dtracer + update
 // ---------------------------------------------------------------------------
+// Reciprocals of the static cell geometry for k_col3 (computed per step
+// they cost two divisions per cell; measured: loading them is 2-3 % faster
+// there, while the same for k_col1's PPM weights was slower).
+template <typename R>
+__global__ void k_rcp_planes(DMeshT<R> m, R *rcp) {
+  const size_t plane = (size_t)m.S * m.N;
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < plane; q += (size_t)gridDim.x * blockDim.x) {
+    const int n = (int)(q / m.S), k = (int)(q - (size_t)n * m.S);
+    if (k >= m.nlev_node[n] - 1) continue;  // dry cells stay zero
+    rcp[q] = R(1) / m.areasvol[q];
+    rcp[plane + q] = R(1) / m.hnode_new[q];
+  }
+}
+
 template <typename R, typename TS, int NT, int LIM>
 __device__ __forceinline__ void col3_block(const DMeshT<R> &m, const FusedArgs<R, TS> &a, int blk, int *smem) {
   int *s_off = smem, *s_item = smem + kMaxItemsPerBlock + 1;
@@ -795,7 +809,7 @@ __device__ __forceinline__ void col3_block(const DMeshT<R> &m, const FusedArgs<R
     const size_t col = (size_t)n * S, o = col + k;
     const int nlev = m.nlev_node[n];
     const R asv = m.areasvol[o], hn = m.hnode_new[o];
-    const R yasv = R(1) / asv, yhn = R(1) / hn;
+    const R yasv = m.rcp[o], yhn = m.rcp[m.rcp_plane + o];
     R dv[NTMAX], dh[NTMAX];
     for (int t = 0; t < NT; t++) {
       const R *av = a.adf_v[t] + col;

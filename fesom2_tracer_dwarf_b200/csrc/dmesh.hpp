@@ -61,6 +61,10 @@ struct DMeshT {
   const R *hnode;           // node
   const R *hnode_new;       // node
   const R *helem;           // element
+  // reciprocals 1/areasvol (plane 0) and 1/hnode_new (plane 1) of the wet
+  // cells, S x N each, computed once per mesh (k_rcp_planes)
+  const R *rcp;
+  size_t rcp_plane;         // S * N
   DSched node_sched;        // items = nodes, levels = nlev_node - 1
   DSched edge_sched;        // items = edges, levels = edge levels
   // node-levels whose MUSCL gradient is the ring mean for some incident edge

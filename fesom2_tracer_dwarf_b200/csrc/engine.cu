@@ -206,8 +206,13 @@ Engine::Engine(const MeshHost &mesh, Precision prec) : p_(new EngineImpl) {
   });
   for (int s = 0; s < E; s++) edge_slot[slot_edge[s]] = s;
   P.slot_edge = slot_edge;
-  if (prec == Precision::FP64) build_dmesh<double>(P, P.dm64, slot_edge, edge_slot);
-  else build_dmesh<float>(P, P.dm32, slot_edge, edge_slot);
+  if (prec == Precision::FP64) {
+    build_dmesh<double>(P, P.dm64, slot_edge, edge_slot);
+    build_rcp_f64(P);
+  } else {
+    build_dmesh<float>(P, P.dm32, slot_edge, edge_slot);
+    build_rcp_f32(P);
+  }
   P.vel = P.dalloc_bytes((size_t)2 * M.elem2D * P.S * P.r_bytes);
   P.W = P.dalloc_bytes((size_t)M.nod2D * P.S * P.r_bytes);
   CK(cudaStreamSynchronize(P.stream));

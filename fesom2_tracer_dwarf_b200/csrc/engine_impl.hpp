@@ -151,6 +151,9 @@ enum { KK_EDGE = 0, KK_COL1, KK_COL2, KK_COL3, KK_GRAD, KK_COUNT };
 // Launch one batch of nt tracers (kernels in step_f64.cu / step_f32.cu).
 void launch_batch_f64(EngineImpl &P, const TracerScheme &sc, int nt, const BatchPtrs &b, double dt);
 void launch_batch_f32(EngineImpl &P, const TracerScheme &sc, int nt, const BatchPtrs &b, double dt);
+// Geometry reciprocals of k_col3 (step_f64.cu / step_f32.cu).
+void build_rcp_f64(EngineImpl &P);
+void build_rcp_f32(EngineImpl &P);
 // Compensated FP64 sums of T and of T * areasvol * hnode_new over the wet
 // cells of one tracer.
 void volume_sum_f64(EngineImpl &P, const void *T, double out[2]);

@@ -89,6 +89,19 @@ void run_group(EngineImpl &P, const TracerScheme &sc, const FusedArgs<R, TS> &a)
   P.mark_end();
 }
 
+// Geometry reciprocals of k_col3 (k_rcp_planes), once per mesh.
+template <typename R>
+void build_rcp_planes_t(EngineImpl &P, DMeshT<R> &d) {
+  const size_t plane = (size_t)d.S * d.N;
+  R *rcp = (R *)P.dalloc_bytes(2 * plane * sizeof(R));
+  const int grid = (int)std::min<size_t>((plane + 255) / 256, (size_t)148 * 32);
+  k_rcp_planes<R><<<std::max(grid, 1), 256, 0, P.stream>>>(d, rcp);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(P.stream));
+  d.rcp = rcp;
+  d.rcp_plane = plane;
+}
+
 template <typename R, typename TS>
 void launch_batch_t(EngineImpl &P, const TracerScheme &sc, int nt, const BatchPtrs &b, double dt) {
   FusedArgs<R, TS> a{};

@@ -13,6 +13,8 @@ void launch_batch_f32(EngineImpl &P, const TracerScheme &sc, int nt, const Batch
   }
 }
 
+void build_rcp_f32(EngineImpl &P) { build_rcp_planes_t<float>(P, P.dm32); }
+
 void volume_sum_f32(EngineImpl &P, const void *T, double off, double out[2]) {
   switch (P.prec) {
     case Precision::BF16: volume_sum_t<float, __nv_bfloat16>(P, T, off, out); break;
