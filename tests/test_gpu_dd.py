@@ -83,6 +83,31 @@ def test_pi_mesh_metis_partitions_bitwise(api, pi_mesh_dir, n, sch):
     assert_bitwise(d2, g2, f"pi dist_{n} {sch} S")
 
 
+def test_frozen_values_ab_bitwise(api):
+    """valuesAB frozen at its initial value (the analytic driver's mode): the
+    halo rows of valuesAB are set once and stay right."""
+    from fesom2_tracer_dwarf_b200.decomp import DomainDecomposition, partition_by_index
+    T, S, uv, w, dt = _analytic(api)
+    sch = ("MUSCL", "PPM", "FCT")
+    api.allocate_tracers(1)
+    api.set_values(1, T)
+    api.set_scheme(1, *sch)
+    api.set_velocity(uv, w)
+    api.set_ab_refresh(False)
+    api.advect_steps(4, dt)
+    g1 = api.get_tracer_values(1)
+    part = partition_by_index(api.mesh_dims()["nod2D"], 3)
+    dd = DomainDecomposition(api, part, 3)
+    dd.allocate_tracers(1)
+    dd.set_scheme(1, *sch)
+    dd.set_velocity(uv, w)
+    dd.set_values(1, T)
+    dd.steps(4, dt, refresh_ab=False, exchange=True)
+    d1 = dd.get_values(1)
+    dd.destroy()
+    assert_bitwise(d1, g1, "frozen valuesAB")
+
+
 def test_without_exchange_the_halo_goes_stale(api):
     """Control: skipping the exchange changes owned values within a few steps."""
     from fesom2_tracer_dwarf_b200.decomp import partition_by_index

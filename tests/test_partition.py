@@ -102,3 +102,21 @@ def test_halo_exchange_two_gloo_ranks():
     res = [json.loads(o.strip().splitlines()[-1]) for o in outs]
     assert all(d["ok"] for d in res)
     assert all(d["halo"] > 0 for d in res)
+
+
+def test_decomposition_refuses_unsupported_setups(api):
+    """16-bit storage (per-part storage offsets would differ) and fewer than
+    three halo rings are refused before any device work."""
+    from fesom2_tracer_dwarf_b200.decomp import DomainDecomposition, partition_by_index
+    api.init_analytic(20, 16, 6, periodic=True, full_rings=True)
+    part = partition_by_index(api.mesh_dims()["nod2D"], 2)
+    with pytest.raises(RuntimeError, match="at least 3 halo rings"):
+        DomainDecomposition(api, part, 2, rings=2)
+    with pytest.raises(RuntimeError, match="outside"):
+        DomainDecomposition(api, np.where(part == 1, 5, 0).astype(np.int32), 2)
+    api.set_precision("bf16")
+    try:
+        with pytest.raises(RuntimeError, match="FP64 and FP32"):
+            DomainDecomposition(api, part, 2)
+    finally:
+        api.set_precision("fp64")
