@@ -434,9 +434,12 @@ __device__ __forceinline__ void col1_block(const DMeshT<R> &m, const FusedArgs<R
   R *s_slope = (R *)(smem + kMaxItemsPerBlock + 1 + kMaxCellsPerBlock + 1);  // 16-byte aligned below
   s_slope = (R *)(((uintptr_t)s_slope + 15) & ~(uintptr_t)15);
   R *s_tv = s_slope + NT * kMaxCellsPerBlock;
-  R *s_fv = s_tv + NT * kMaxCellsPerBlock;
+  // the vertical LO fluxes of stage C reuse the slopes' storage, dead after
+  // stage B: two arrays of shared memory instead of three leave more of the
+  // SM's unified L1 to the column and neighbour re-reads
+  R *s_fv = s_slope;
   const CellMap cm = map_cells(m.node_sched, blk, s_off, s_item);
-  const Incidence inc = stage_incidence(m, cm, s_fv + NT * kMaxCellsPerBlock);
+  const Incidence inc = stage_incidence(m, cm, s_tv + NT * kMaxCellsPerBlock);
   const int S = m.S;
 
   // stage A: PPM slopes

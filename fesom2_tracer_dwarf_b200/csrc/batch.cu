@@ -63,8 +63,7 @@ enum { PH_GRAD = 0, PH_EDGE, PH_COL1, PH_COL2, PH_COL3, PH_COUNT };
 
 constexpr size_t kTaskSmem = (sizeof(BatchTask) + 15) / 16 * 16;
 size_t batch_smem() {
-  return kTaskSmem + std::max(smem_col_staged<float>(kNT, 3),
-                              std::max(smem_col_staged<float>(kNT, 2), smem_col_staged<float>(kNT, 0)));
+  return kTaskSmem + std::max(smem_col_staged<float>(kNT, 2), smem_col_staged<float>(kNT, 0));
 }
 
 // prefix: PH_COUNT rows of (ntasks + 1) running totals of each task's blocks;

@@ -41,7 +41,7 @@ void launch_edge(EngineImpl &P, const FusedArgs<R, TS> &a) {
 template <typename R, typename TS, int NT, int VER, int LIM>
 void launch_col1(EngineImpl &P, const FusedArgs<R, TS> &a) {
   const DMeshT<R> &m = dmesh<R>(P);
-  const size_t sm = smem_col_staged<R>(NT, 3);
+  const size_t sm = smem_col_staged<R>(NT, 2);
   set_smem(k_col1<R, TS, NT, VER, LIM>, sm);
   P.mark_begin(KK_COL1);
   k_col1<R, TS, NT, VER, LIM><<<m.node_sched.nblk, kThreads, sm, P.stream>>>(m, a);
