@@ -81,6 +81,20 @@ struct MinBlocks<float> {
   static constexpr int grad = FESOM_MINB32_GRAD, edge = FESOM_MINB32_EDGE, col1 = FESOM_MINB32_COL1,
                        col2 = FESOM_MINB32_COL2, col3 = FESOM_MINB32_COL3;
 };
+// Incidence records of each node kernel's block staged in shared memory or
+// read through L1, per arithmetic type.  Measured on the 1000x1000x64 step:
+// FP64 staged k_col1 3.28 ms (unstaged 3.34), k_col2 2.39 (2.50), k_col3 2.75
+// (2.75); FP32 unstaged k_col1 1.81 (staged 1.84), k_col2 1.61 (1.68), k_col3
+// 1.57 (1.60) -- the FP32 kernels keep more blocks resident, whose shared
+// memory would otherwise crowd out the L1.
+template <typename R>
+struct StageIncidence {
+  static constexpr bool col1 = true, col2 = true, col3 = true;
+};
+template <>
+struct StageIncidence<float> {
+  static constexpr bool col1 = false, col2 = false, col3 = false;
+};
 // The LO gather of k_col1 issues the loads of this many incident edges
 // together before using any of them.  Every (edge, level) and (node, level)
 // address of a cell's level lies inside its padded column, so the loads of
@@ -199,13 +213,15 @@ struct Incidence {
   int sub;
 };
 
-template <typename R>
+// STAGE = false reads the records from global memory (through L1) and needs
+// no shared memory for them.
+template <bool STAGE = true, typename R>
 __device__ __forceinline__ Incidence stage_incidence(const DMeshT<R> &m, const CellMap &cm, void *region) {
   int4 *s_ne = reinterpret_cast<int4 *>(((uintptr_t)region + 15) & ~(uintptr_t)15);
   int *s_nep = reinterpret_cast<int *>(s_ne + kNeStage);
   const int p0 = m.ne_ptr[cm.i0], p1 = m.ne_ptr[cm.i0 + cm.ni];
   Incidence r;
-  if (p1 - p0 <= kNeStage) {
+  if (STAGE && p1 - p0 <= kNeStage) {
     for (int i = threadIdx.x; i < p1 - p0; i += blockDim.x) s_ne[i] = m.ne4[p0 + i];
     for (int j = threadIdx.x; j <= cm.ni; j += blockDim.x) s_nep[j] = m.ne_ptr[cm.i0 + j] - p0;
     r.ne = s_ne;
@@ -439,7 +455,7 @@ __device__ __forceinline__ void col1_block(const DMeshT<R> &m, const FusedArgs<R
   // SM's unified L1 to the column and neighbour re-reads
   R *s_fv = s_slope;
   const CellMap cm = map_cells(m.node_sched, blk, s_off, s_item);
-  const Incidence inc = stage_incidence(m, cm, s_tv + NT * kMaxCellsPerBlock);
+  const Incidence inc = stage_incidence<StageIncidence<R>::col1>(m, cm, s_tv + NT * kMaxCellsPerBlock);
   const int S = m.S;
 
   // stage A: PPM slopes
@@ -630,7 +646,7 @@ __device__ __forceinline__ void col2_block(const DMeshT<R> &m, const FusedArgs<R
   s_mx = (R *)(((uintptr_t)s_mx + 15) & ~(uintptr_t)15);
   R *s_mn = s_mx + NT * kMaxCellsPerBlock;
   const CellMap cm = map_cells(m.node_sched, blk, s_off, s_item);
-  const Incidence inc = stage_incidence(m, cm, s_mn + NT * kMaxCellsPerBlock);
+  const Incidence inc = stage_incidence<StageIncidence<R>::col2>(m, cm, s_mn + NT * kMaxCellsPerBlock);
   const int S = m.S;
   const R big = R(1e3);
 
@@ -805,7 +821,7 @@ template <typename R, typename TS, int NT, int LIM>
 __device__ __forceinline__ void col3_block(const DMeshT<R> &m, const FusedArgs<R, TS> &a, int blk, int *smem) {
   int *s_off = smem, *s_item = smem + kMaxItemsPerBlock + 1;
   const CellMap cm = map_cells(m.node_sched, blk, s_off, s_item);
-  const Incidence inc = stage_incidence(m, cm, smem + kMaxItemsPerBlock + 1 + kMaxCellsPerBlock + 1);
+  const Incidence inc = stage_incidence<StageIncidence<R>::col3>(m, cm, smem + kMaxItemsPerBlock + 1 + kMaxCellsPerBlock + 1);
   const int S = m.S;
   for (int lc = threadIdx.x; lc < cm.nc; lc += blockDim.x) {
     const int j = s_item[lc], n = cm.i0 + j, k = lc - (s_off[j] - cm.c0), nz = k + 1;

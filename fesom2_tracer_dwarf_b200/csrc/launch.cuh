@@ -41,7 +41,7 @@ void launch_edge(EngineImpl &P, const FusedArgs<R, TS> &a) {
 template <typename R, typename TS, int NT, int VER, int LIM>
 void launch_col1(EngineImpl &P, const FusedArgs<R, TS> &a) {
   const DMeshT<R> &m = dmesh<R>(P);
-  const size_t sm = smem_col_staged<R>(NT, 2);
+  const size_t sm = StageIncidence<R>::col1 ? smem_col_staged<R>(NT, 2) : smem_col<R>(NT, 2);
   set_smem(k_col1<R, TS, NT, VER, LIM>, sm);
   P.mark_begin(KK_COL1);
   k_col1<R, TS, NT, VER, LIM><<<m.node_sched.nblk, kThreads, sm, P.stream>>>(m, a);
@@ -76,13 +76,13 @@ void run_group(EngineImpl &P, const TracerScheme &sc, const FusedArgs<R, TS> &a)
   }
   const DMeshT<R> &m = dmesh<R>(P);
   if (LIM == LIM_FCT) {
-    const size_t sm2 = smem_col_staged<R>(NT, 2);
+    const size_t sm2 = StageIncidence<R>::col2 ? smem_col_staged<R>(NT, 2) : smem_col<R>(NT, 2);
     set_smem(k_col2<R, TS, NT>, sm2);
     P.mark_begin(KK_COL2);
     k_col2<R, TS, NT><<<m.node_sched.nblk, kThreads, sm2, P.stream>>>(m, a);
     P.mark_end();
   }
-  const size_t sm3 = smem_col_staged<R>(NT, 0);
+  const size_t sm3 = StageIncidence<R>::col3 ? smem_col_staged<R>(NT, 0) : smem_col<R>(NT, 0);
   set_smem(k_col3<R, TS, NT, LIM>, sm3);
   P.mark_begin(KK_COL3);
   k_col3<R, TS, NT, LIM><<<m.node_sched.nblk, kThreads, sm3, P.stream>>>(m, a);
