@@ -125,6 +125,8 @@ SIGNATURES = {
     "tracer_partition_halo": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp,
                                              ctypes.c_int]),
     "tracer_partition_part_dims": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp]),
+    "tracer_partition_install_part": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp]),
+    "tracer_partition_part_ids": (ctypes.c_int, [_vp, _vp]),
     "tracer_dd_setup": (ctypes.c_int, [_vp, ctypes.c_int, _vp, ctypes.c_int, ctypes.c_int]),
     "tracer_dd_destroy": (ctypes.c_int, []),
     "tracer_dd_part_info": (ctypes.c_int, [ctypes.c_int, _vp]),

@@ -41,6 +41,8 @@ struct State {
 };
 State g;
 std::unique_ptr<Decomposition> g_dd;  // domain-decomposed runner (tracer_dd_*)
+// global ids of the part installed by tracer_partition_install_part
+std::vector<int> g_part_nodes, g_part_elems;
 
 int fail(const std::string &msg) {
   set_last_error(msg);
@@ -636,6 +638,8 @@ static bool mesh_field(const char *name, const std::vector<int> **vi, const std:
   else if (s == "edge_up_dn_tri") *vi = &m.up_dn_tri;
   else if (s == "nboundary_lay") *vi = &m.nboundary_lay;
   else if (s == "ring_num") *vi = &m.ring_ptr;
+  else if (s == "ring_elem") *vi = &m.ring_elem;
+  else if (s == "Z") *vd = &m.Z;
   else return false;
   return true;
 }
@@ -659,7 +663,8 @@ int tracer_mesh_get_int(const char *name, int *out) {
     for (int n = 0; n < g.mesh->nod2D; n++) out[n] = g.mesh->ring_ptr[n + 1] - g.mesh->ring_ptr[n];
     return 0;
   }
-  const bool index = (s == "elem2D_nodes" || s == "edges" || s == "edge_tri" || s == "edge_up_dn_tri");
+  const bool index = (s == "elem2D_nodes" || s == "edges" || s == "edge_tri" || s == "edge_up_dn_tri" ||
+                       s == "ring_elem");
   for (size_t i = 0; i < vi->size(); i++) out[i] = index ? ((*vi)[i] >= 0 ? (*vi)[i] + 1 : 0) : (*vi)[i];
   return 0;
 }
@@ -992,6 +997,28 @@ int tracer_partition_part_dims(const int *node_part, int nparts, int part, int r
     dims4[3] = mp.mesh.edge2D;
     return 0;
   });
+}
+
+int tracer_partition_install_part(const int *node_part, int nparts, int part, int rings, int *dims4) {
+  return guarded([&] {
+    MeshPart mp = build_mesh_part(*g.mesh, part_map(node_part, nparts), part, rings);
+    dims4[0] = mp.owned;
+    dims4[1] = mp.mesh.nod2D;
+    dims4[2] = mp.mesh.elem2D;
+    dims4[3] = mp.mesh.edge2D;
+    g_part_nodes = mp.node_global;
+    g_part_elems = mp.elem_global;
+    install_mesh(std::move(mp.mesh));
+    g.initialized = true;
+    return 0;
+  });
+}
+
+int tracer_partition_part_ids(int *nodes, int *elems) {
+  if (g_part_nodes.empty()) return fail("tracer_partition_part_ids: no part installed");
+  for (size_t i = 0; i < g_part_nodes.size(); i++) nodes[i] = g_part_nodes[i] + 1;
+  for (size_t i = 0; i < g_part_elems.size(); i++) elems[i] = g_part_elems[i] + 1;
+  return 0;
 }
 
 int tracer_dd_setup(const int *node_part, int nparts, const int *local_parts, int nlocal, int rings) {

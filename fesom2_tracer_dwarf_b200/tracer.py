@@ -17,7 +17,7 @@ from . import _lib
 
 
 _INT_MESH_ARRAYS = {"elem2D_nodes", "edges", "edge_tri", "nlevels", "nlevels_nod2D", "nlevels_nod2D_min",
-                    "edge_up_dn_tri", "nboundary_lay", "ring_num"}
+                    "edge_up_dn_tri", "nboundary_lay", "ring_num", "ring_elem"}
 
 
 def _f64(a, shape):

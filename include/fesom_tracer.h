@@ -362,6 +362,11 @@ int tracer_partition_read_dist(const char *dist_dir, int *node_part, int *nparts
 int tracer_partition_halo(const int *node_part, int nparts, int from, int to, int rings, int *out, int capacity);
 /* owned nodes, local nodes, local elements, local edges of one part (host only) */
 int tracer_partition_part_dims(const int *node_part, int nparts, int part, int rings, int *dims4);
+/* host only: make part `part`'s local mesh the current mesh (for inspection
+ * and host-side checks), dims4 as tracer_partition_part_dims; its 1-based
+ * global node and element ids (local order) by tracer_partition_part_ids */
+int tracer_partition_install_part(const int *node_part, int nparts, int part, int rings, int *dims4);
+int tracer_partition_part_ids(int *nodes, int *elems);
 /* engines for local_parts[0..nlocal) of the decomposition, on this process's GPU */
 int tracer_dd_setup(const int *node_part, int nparts, const int *local_parts, int nlocal, int rings);
 int tracer_dd_destroy(void);

@@ -1006,6 +1006,79 @@ om_mesh *om_mesh_from_files(const char *dir, int rotate, double alpha, double be
 }
 #undef MESH_FAIL
 
+/* ------------------------------------------------------------------------ */
+/* mesh from given arrays (every table as passed, the MUSCL ones included)   */
+/* ------------------------------------------------------------------------ */
+static void *dup_bytes(const void *src, size_t bytes) {
+  void *p = malloc(bytes ? bytes : 1);
+  if (bytes) memcpy(p, src, bytes);
+  return p;
+}
+
+om_mesh *om_mesh_from_arrays(int nl, int nod2D, int elem2D, int edge2D, int periodic, double Lx, double Ly,
+                             const double *coord, const int *elem2D_nodes, const int *edges, const int *edge_tri,
+                             const int *nlevels, const int *nlevels_nod2D, const int *nlevels_nod2D_min,
+                             const int *ring_num, const int *ring_elem, const double *elem_area, const double *area,
+                             const double *areasvol, const double *edge_dxdy, const double *edge_cross_dxdy,
+                             const double *gradient_sca, const double *elem_cos, const double *zbar,
+                             const double *hnode, const double *hnode_new, const double *helem,
+                             const int *edge_up_dn_tri, const int *nboundary_lay) {
+  if (nl < 3 || nod2D < 1 || elem2D < 1 || edge2D < 1) return NULL;
+  om_mesh *m = (om_mesh *)calloc(1, sizeof(om_mesh));
+  const size_t N = (size_t)nod2D, T = (size_t)elem2D, E = (size_t)edge2D, L = (size_t)nl - 1;
+  m->nl = nl;
+  m->nod2D = m->nod2D_total = nod2D;
+  m->elem2D = elem2D;
+  m->edge2D = edge2D;
+  m->periodic = periodic;
+  m->full_rings = 1;
+  m->Lx = Lx;
+  m->Ly = Ly;
+  m->cyclic = CYCLIC_LENGTH;
+  m->coord = (double *)dup_bytes(coord, 2 * N * sizeof(double));
+  m->elem2D_nodes = (int *)dup_bytes(elem2D_nodes, 3 * T * sizeof(int));
+  m->edges = (int *)dup_bytes(edges, 2 * E * sizeof(int));
+  m->edge_tri = (int *)dup_bytes(edge_tri, 2 * E * sizeof(int));
+  m->nlevels = (int *)dup_bytes(nlevels, T * sizeof(int));
+  m->nlevels_nod2D = (int *)dup_bytes(nlevels_nod2D, N * sizeof(int));
+  m->nlevels_nod2D_min = (int *)dup_bytes(nlevels_nod2D_min, N * sizeof(int));
+  m->ulevels = (int *)malloc(T * sizeof(int));
+  for (size_t t = 0; t < T; t++) m->ulevels[t] = 1;
+  m->ulevels_nod2D = (int *)malloc(N * sizeof(int));
+  m->ulevels_nod2D_max = (int *)malloc(N * sizeof(int));
+  for (size_t n = 0; n < N; n++) m->ulevels_nod2D[n] = m->ulevels_nod2D_max[n] = 1;
+  int mx = 0;
+  for (size_t n = 0; n < N; n++) mx = imax2(mx, ring_num[n]);
+  m->max_nie = mx;
+  m->nod_in_elem2D_num = (int *)dup_bytes(ring_num, N * sizeof(int));
+  m->nod_in_elem2D = (int *)calloc((size_t)mx * N, sizeof(int));
+  for (size_t n = 0, p = 0; n < N; n++)
+    for (int j = 1; j <= ring_num[n]; j++) A2(m->nod_in_elem2D, j, (int)n + 1, mx) = ring_elem[p++];
+  m->elem_area = (double *)dup_bytes(elem_area, T * sizeof(double));
+  m->area = (double *)dup_bytes(area, (size_t)nl * N * sizeof(double));
+  m->areasvol = (double *)dup_bytes(areasvol, (size_t)nl * N * sizeof(double));
+  m->edge_dxdy = (double *)dup_bytes(edge_dxdy, 2 * E * sizeof(double));
+  m->edge_cross_dxdy = (double *)dup_bytes(edge_cross_dxdy, 4 * E * sizeof(double));
+  m->gradient_sca = (double *)dup_bytes(gradient_sca, 6 * T * sizeof(double));
+  m->elem_cos = (double *)dup_bytes(elem_cos, T * sizeof(double));
+  m->zbar = (double *)dup_bytes(zbar, (size_t)nl * sizeof(double));
+  m->Z = (double *)malloc(L * sizeof(double));
+  for (size_t k = 0; k < L; k++) m->Z[k] = 0.5 * (m->zbar[k] + m->zbar[k + 1]);
+  m->max_depth = -m->zbar[nl - 1];
+  m->hnode = (double *)dup_bytes(hnode, L * N * sizeof(double));
+  m->hnode_new = (double *)dup_bytes(hnode_new, L * N * sizeof(double));
+  m->helem = (double *)dup_bytes(helem, L * T * sizeof(double));
+  m->zbar_3d_n = (double *)malloc((size_t)nl * N * sizeof(double));
+  m->Z_3d_n = (double *)malloc(L * N * sizeof(double));
+  for (size_t n = 0; n < N; n++) {
+    for (size_t k = 0; k < (size_t)nl; k++) m->zbar_3d_n[n * nl + k] = m->zbar[k];
+    for (size_t k = 0; k < L; k++) m->Z_3d_n[n * L + k] = m->Z[k];
+  }
+  m->edge_up_dn_tri = (int *)dup_bytes(edge_up_dn_tri, 2 * E * sizeof(int));
+  m->nboundary_lay = (int *)dup_bytes(nboundary_lay, N * sizeof(int));
+  return m;
+}
+
 static void work_free(struct om_work_s *w);
 void om_mesh_free(om_mesh *m) {
   if (!m) return;

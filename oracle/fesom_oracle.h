@@ -55,6 +55,19 @@ om_mesh *om_mesh_analytic(int nx, int ny, int nl, double Lx, double Ly,
  * cyclic_length = 360.  NULL on failure, with a message in err. */
 om_mesh *om_mesh_from_files(const char *dir, int rotate, double alpha, double beta, double gamma,
                             double angle_scale, double cyclic_length, char *err, int errlen);
+/* A mesh from arrays in the layouts above (index arrays 1-based, 0 = none;
+ * the node rings as counts and their concatenated element lists), with the
+ * MUSCL tables (edge_up_dn_tri, nboundary_lay) taken as given, and
+ * thicknesses as given (zbar_3d_n, Z_3d_n from zbar).  Checks mesh parts of
+ * a domain decomposition against the whole mesh. */
+om_mesh *om_mesh_from_arrays(int nl, int nod2D, int elem2D, int edge2D, int periodic, double Lx, double Ly,
+                             const double *coord, const int *elem2D_nodes, const int *edges, const int *edge_tri,
+                             const int *nlevels, const int *nlevels_nod2D, const int *nlevels_nod2D_min,
+                             const int *ring_num, const int *ring_elem, const double *elem_area, const double *area,
+                             const double *areasvol, const double *edge_dxdy, const double *edge_cross_dxdy,
+                             const double *gradient_sca, const double *elem_cos, const double *zbar,
+                             const double *hnode, const double *hnode_new, const double *helem,
+                             const int *edge_up_dn_tri, const int *nboundary_lay);
 void om_mesh_free(om_mesh *m);
 
 /* dims[0..5] = nl, nod2D, elem2D, edge2D, max_nod_in_elem, periodic */

@@ -45,6 +45,8 @@ class Oracle:
         lib.om_mesh_analytic.argtypes = [ci, ci, ci, cd, cd, cd, ci, ci, vp]
         lib.om_mesh_free.argtypes = [vp]
         lib.om_mesh_from_files.restype = vp
+        lib.om_mesh_from_arrays.restype = vp
+        lib.om_mesh_from_arrays.argtypes = [ci, ci, ci, ci, ci, cd, cd] + [vp] * 22
         lib.om_mesh_from_files.argtypes = [ctypes.c_char_p, ci, cd, cd, cd, cd, cd, ctypes.c_char_p, ci]
         lib.om_mesh_dims.argtypes = [vp, vp]
         lib.om_mesh_len.restype = ctypes.c_long
@@ -94,6 +96,34 @@ class OracleMesh:
                                           angle_scale, cyclic_length, err, len(err))
         if not h:
             raise ValueError("oracle mesh: " + err.value.decode())
+        self.h = ctypes.c_void_p(h)
+        d = np.zeros(6, dtype=np.int32)
+        oracle.lib.om_mesh_dims(self.h, _p(d))
+        self.nl, self.nod2D, self.elem2D, self.edge2D, self.max_nie = (int(x) for x in d[:5])
+        return self
+
+    FROM_ARRAYS = ["coord", "elem2D_nodes", "edges", "edge_tri", "nlevels", "nlevels_nod2D", "nlevels_nod2D_min",
+                   "ring_num", "ring_elem", "elem_area", "area", "areasvol", "edge_dxdy", "edge_cross_dxdy",
+                   "gradient_sca", "elem_cos", "zbar", "hnode", "hnode_new", "helem", "edge_up_dn_tri",
+                   "nboundary_lay"]
+
+    @classmethod
+    def from_arrays(cls, oracle: Oracle, nl, nod2D, elem2D, edge2D, arrays: dict, periodic=False, Lx=0.0, Ly=0.0):
+        """A mesh from arrays (``FROM_ARRAYS``, index arrays 1-based, 0 =
+        none), every table taken as given."""
+        self = cls.__new__(cls)
+        self.o = oracle
+        keep = []
+        ptrs = []
+        for name in cls.FROM_ARRAYS:
+            a = arrays[name]
+            a = np.ascontiguousarray(a, dtype=np.int32 if name in _INT_FIELDS | {"ring_num", "ring_elem"}
+                                     else np.float64)
+            keep.append(a)
+            ptrs.append(_p(a))
+        h = oracle.lib.om_mesh_from_arrays(nl, nod2D, elem2D, edge2D, int(periodic), Lx, Ly, *ptrs)
+        if not h:
+            raise ValueError("oracle mesh from arrays failed")
         self.h = ctypes.c_void_p(h)
         d = np.zeros(6, dtype=np.int32)
         oracle.lib.om_mesh_dims(self.h, _p(d))
