@@ -82,6 +82,12 @@ Decomposition::Decomposition(const MeshHost &g, const std::vector<int> &node_par
   if ((int)node_part.size() != g.nod2D) throw std::invalid_argument("one part per node expected");
   for (int q : node_part)
     if (q < 0 || q >= nparts) throw std::invalid_argument("node part outside [0, nparts)");
+  {
+    std::vector<int> seen(local_parts);
+    std::sort(seen.begin(), seen.end());
+    if (std::adjacent_find(seen.begin(), seen.end()) != seen.end())
+      throw std::invalid_argument("a part is listed twice among the local parts");
+  }
   Impl &P = *p_;
   P.nparts = nparts;
   P.rings = rings;

@@ -114,6 +114,8 @@ def test_decomposition_refuses_unsupported_setups(api):
         DomainDecomposition(api, part, 2, rings=2)
     with pytest.raises(RuntimeError, match="outside"):
         DomainDecomposition(api, np.where(part == 1, 5, 0).astype(np.int32), 2)
+    with pytest.raises(RuntimeError, match="listed twice"):
+        DomainDecomposition(api, part, 2, parts=[1, 1])
     api.set_precision("bf16")
     try:
         with pytest.raises(RuntimeError, match="FP64 and FP32"):
