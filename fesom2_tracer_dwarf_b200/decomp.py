@@ -167,7 +167,10 @@ class DistributedTracer:
         L = self.dd.nl - 1
         send = {p: self.dd.transfer_nodes(0, p, True) * L for p in range(world) if p != rank}
         recv = {p: self.dd.transfer_nodes(0, p, False) * L for p in range(world) if p != rank}
-        self.wire = device if dist.get_backend() == "nccl" else "cpu"
+        backend = dist.get_backend() if dist.is_available() and dist.is_initialized() else None
+        if world > 1 and backend is None:
+            raise RuntimeError("DistributedTracer: initialise torch.distributed for more than one rank")
+        self.wire = device if backend == "nccl" else "cpu"
         self.halo = HaloExchange(send, recv, self.wire)
         self.ntr = 0
 
