@@ -102,3 +102,20 @@ def test_malformed_mesh_directory_fails_cleanly(api, pi_mesh_dir, tmp_path, dama
     # the library stays usable
     api.load_mesh_from_files(pi_mesh_dir)
     assert api.mesh_dims()["nod2D"] == 3140
+
+
+def test_synthetic_flow_keeps_constants_on_stretched_layers(api, oracle, pi_mesh_dir):
+    """The seeded layered flow's vertical modes have zero thickness-weighted
+    column mean, so w from the discrete continuity closes at the surface even
+    on the pi mesh's 5 m to 250 m layers: a constant stays constant under the
+    oracle's MUSCL/PPM/FCT step (and the content is conserved)."""
+    import pyoracle
+    api.load_mesh_from_files(pi_mesh_dir, **FESOM2)
+    uv, w = api.synth_velocity(seed=5, umax=0.5, mode2=0.5)
+    m = pyoracle.OracleMesh.from_files(oracle, pi_mesh_dir, **FESOM2)
+    nlev = api.mesh_array("nlevels_nod2D")
+    wet = np.arange(47)[:, None] < (nlev[None, :] - 1)
+    C = np.asfortranarray(np.where(wet, 7.25, 0.0))
+    for _ in range(5):
+        m.step(C, C.copy(order="F"), uv, w, 600.0, "MUSCL", "PPM", "FCT")
+    assert np.max(np.abs(C[wet] - 7.25)) < 1e-12
