@@ -122,3 +122,23 @@ def test_decomposition_refuses_unsupported_setups(api):
             DomainDecomposition(api, part, 2)
     finally:
         api.set_precision("fp64")
+
+
+@pytest.mark.parametrize("n", [2, 8])
+def test_one_ring_halos_equal_the_reference_partition_lists(api, pi_mesh_dir, n):
+    """The reference's my_list<part>.out files list each part's halo nodes
+    (eDim_nod2D: the nodes of its elements that other parts own, one ring);
+    the library's one-ring halo (union of the transfers into the part) is
+    exactly that set, for every part of both partitions."""
+    from fesom2_tracer_dwarf_b200 import decomp
+    api.load_mesh_from_files(pi_mesh_dir)
+    part, nparts = decomp.read_dist(api, pi_mesh_dir / f"dist_{n}")
+    for r in range(nparts):
+        words = (pi_mesh_dir / f"dist_{n}" / f"my_list{r:05d}.out").read_text().split()
+        my, halo = int(words[1]), int(words[2])
+        ref = set(int(v) - 1 for v in words[3 + my:3 + my + halo])
+        ours = set()
+        for q in range(nparts):
+            if q != r:
+                ours |= set(decomp.halo_transfer(api, part, nparts, q, r, rings=1).tolist())
+        assert ours == ref, f"part {r}"
