@@ -11,9 +11,10 @@ from pathlib import Path
 
 FILES = ["nod2d.out", "elem2d.out", "aux3d.out", "edgenum.out", "edges.out", "edge_tri.out", "elvls.out",
          "nlvls.out"]
-# the partition directories for 2 and 8 parts (rpart.out and the my_list
-# files; stored as dist_2__rpart.out.gz, ..., "__" standing for "/")
-PARTITIONS = [f"dist_{n}/{f}" for n in (2, 8) for f in ["rpart.out"] + [f"my_list{r:05d}.out" for r in range(n)]]
+# the partition directories for 2 and 8 parts (rpart.out, the my_list and
+# com_info files; stored as dist_2__rpart.out.gz, ..., "__" standing for "/")
+PARTITIONS = [f"dist_{n}/{f}" for n in (2, 8)
+              for f in ["rpart.out"] + [f"{kind}{r:05d}.out" for kind in ("my_list", "com_info") for r in range(n)]]
 
 
 def main(reference_root: str) -> None:

@@ -142,3 +142,40 @@ def test_one_ring_halos_equal_the_reference_partition_lists(api, pi_mesh_dir, n)
             if q != r:
                 ours |= set(decomp.halo_transfer(api, part, nparts, q, r, rings=1).tolist())
         assert ours == ref, f"part {r}"
+
+
+def _com_nod2D(path):
+    """Node receive / send structure of a com_info<part>.out file
+    (lib/oce_mesh.F90:686-702): {peer: local 1-based indices} for both."""
+    w = [int(v) for v in path.read_text().split()]
+    i = 1
+    out = []
+    for _ in range(2):  # receive, then send
+        npe = w[i]; i += 1
+        pes = w[i:i + npe]; i += npe
+        ptr = w[i:i + npe + 1]; i += npe + 1
+        lst = w[i:i + ptr[-1] - 1]; i += ptr[-1] - 1
+        out.append({pe: lst[ptr[k] - 1:ptr[k + 1] - 1] for k, pe in enumerate(pes)})
+    return out
+
+
+@pytest.mark.parametrize("n", [2, 8])
+def test_one_ring_transfers_equal_the_reference_communication_lists(api, pi_mesh_dir, n):
+    """Per peer, the nodes a part receives and sends (the reference's
+    com_nod2D lists, local indices into its my_list order) are the library's
+    one-ring halo transfers."""
+    from fesom2_tracer_dwarf_b200 import decomp
+    api.load_mesh_from_files(pi_mesh_dir)
+    part, nparts = decomp.read_dist(api, pi_mesh_dir / f"dist_{n}")
+    for r in range(nparts):
+        words = (pi_mesh_dir / f"dist_{n}" / f"my_list{r:05d}.out").read_text().split()
+        my, halo = int(words[1]), int(words[2])
+        local = [int(v) - 1 for v in words[3:3 + my + halo]]  # local -> global, 0-based
+        recv, send = _com_nod2D(pi_mesh_dir / f"dist_{n}" / f"com_info{r:05d}.out")
+        for q in range(nparts):
+            if q == r:
+                continue
+            ours_in = set(decomp.halo_transfer(api, part, nparts, q, r, rings=1).tolist())
+            ours_out = set(decomp.halo_transfer(api, part, nparts, r, q, rings=1).tolist())
+            assert ours_in == set(local[i - 1] for i in recv.get(q, [])), f"part {r} from {q}"
+            assert ours_out == set(local[i - 1] for i in send.get(q, [])), f"part {r} to {q}"
