@@ -156,42 +156,51 @@ class HaloExchange:
 class DistributedTracer:
     """One part per rank (part = rank, nparts = world size) on this rank's
     GPU; ``steps`` advances every tracer and exchanges the halos with the
-    peers after each step.  The halo rows are packed on the GPU; with the
-    NCCL backend they travel from device memory, with gloo through host
-    memory."""
+    peers after each step, one message per peer holding every tracer's rows.
+    The halo rows are packed on the GPU; with the NCCL backend they travel
+    from device memory, with gloo through host memory."""
 
     def __init__(self, api, node_part: np.ndarray, rank: int, world: int, device, rings: int = RINGS):
         import torch.distributed as dist
         self.dd = DomainDecomposition(api, node_part, world, parts=[rank], rings=rings)
         self.rank, self.world, self.device = rank, world, device
-        L = self.dd.nl - 1
-        send = {p: self.dd.transfer_nodes(0, p, True) * L for p in range(world) if p != rank}
-        recv = {p: self.dd.transfer_nodes(0, p, False) * L for p in range(world) if p != rank}
+        self.L = self.dd.nl - 1
+        self.send_nodes = {p: self.dd.transfer_nodes(0, p, True) for p in range(world) if p != rank}
+        self.recv_nodes = {p: self.dd.transfer_nodes(0, p, False) for p in range(world) if p != rank}
         backend = dist.get_backend() if dist.is_available() and dist.is_initialized() else None
         if world > 1 and backend is None:
             raise RuntimeError("DistributedTracer: initialise torch.distributed for more than one rank")
         self.wire = device if backend == "nccl" else "cpu"
-        self.halo = HaloExchange(send, recv, self.wire)
         self.ntr = 0
+        self.halo = None
 
     def allocate_tracers(self, n: int) -> None:
         self.dd.allocate_tracers(n)
         self.ntr = n
+        self.halo = HaloExchange({p: c * self.L * n for p, c in self.send_nodes.items()},
+                                 {p: c * self.L * n for p, c in self.recv_nodes.items()}, self.wire)
 
     def exchange(self) -> None:
+        """Halo rows of every tracer, tracer after tracer in one buffer per peer."""
         import torch
         lib = self.dd.lib
-        for t in range(1, self.ntr + 1):
-            def pack(peer, t=t):
-                buf = torch.empty(self.halo.send[peer], dtype=torch.float64, device=self.device)
-                _lib.check(lib, lib.tracer_dd_pack(0, t, peer, buf.data_ptr()), "tracer_dd_pack")
-                return buf.to(self.wire)
 
-            def unpack(peer, buf, t=t):
-                dev = buf.to(self.device).contiguous()
-                _lib.check(lib, lib.tracer_dd_unpack(0, t, peer, dev.data_ptr()), "tracer_dd_unpack")
+        def pack(peer):
+            per = self.send_nodes[peer] * self.L
+            buf = torch.empty(per * self.ntr, dtype=torch.float64, device=self.device)
+            for t in range(self.ntr):
+                _lib.check(lib, lib.tracer_dd_pack(0, t + 1, peer, buf[t * per:(t + 1) * per].data_ptr()),
+                           "tracer_dd_pack")
+            return buf.to(self.wire)
 
-            self.halo.exchange(pack, unpack)
+        def unpack(peer, buf):
+            per = self.recv_nodes[peer] * self.L
+            dev = buf.to(self.device).contiguous()
+            for t in range(self.ntr):
+                _lib.check(lib, lib.tracer_dd_unpack(0, t + 1, peer, dev[t * per:(t + 1) * per].data_ptr()),
+                           "tracer_dd_unpack")
+
+        self.halo.exchange(pack, unpack)
 
     def steps(self, nsteps: int, dt: float, refresh_ab: bool = True) -> None:
         for _ in range(nsteps):
