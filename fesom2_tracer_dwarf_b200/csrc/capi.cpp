@@ -123,6 +123,7 @@ Engine *capi_engine() { return g.eng.get(); }
 int capi_num_tracers() { return g.ntr; }
 bool capi_initialized() { return g.initialized; }
 int capi_fail(const std::string &msg) { return fail(msg); }
+std::string noalloc_prepare(int device);  // noalloc.cu
 }  // namespace fesom
 
 extern "C" {
@@ -322,6 +323,10 @@ int tracer_init_for_advection(void) {
   return guarded([&] {
     if (!g.initialized) return fail("tracer_init_for_advection called before mesh loaded");
     ensure_engine();
+    // commit the allocation-free entry point's static work array now, before
+    // a host that reserves the GPU's memory pool takes it
+    const std::string err = noalloc_prepare(g.eng->device());
+    if (!err.empty()) return fail("tracer_init_for_advection: static work array: " + err);
     return 0;
   });
 }

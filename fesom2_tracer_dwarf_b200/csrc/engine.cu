@@ -197,6 +197,7 @@ Engine::Engine(const MeshHost &mesh, Precision prec) : p_(new EngineImpl) {
   // level stride: 32-byte aligned columns for FP64, 16-byte aligned ones (or
   // better) for the 4- and 2-byte types
   P.S = prec == Precision::FP64 ? (M.nl + 3) / 4 * 4 : (M.nl + 7) / 8 * 8;
+  CK(cudaGetDevice(&P.device));
   CK(cudaStreamCreateWithFlags(&P.stream, cudaStreamNonBlocking));
   // slot order: edges sorted by their smaller node id (stable in edge id)
   std::vector<int> slot_edge(E), edge_slot(E);
@@ -244,6 +245,7 @@ int Engine::cells_per_block() const { return p_->cells_per_block; }
 int Engine::level_stride() const { return p_->S; }
 Precision Engine::precision() const { return p_->prec; }
 void *Engine::stream() const { return (void *)p_->stream; }
+int Engine::device() const { return p_->device; }
 void Engine::synchronize() const { CK(cudaStreamSynchronize(p_->stream)); }
 size_t Engine::device_bytes() const { return p_->bytes; }
 int Engine::num_tracers() const { return (int)p_->tr.size(); }

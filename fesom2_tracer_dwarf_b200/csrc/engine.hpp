@@ -97,6 +97,8 @@ class Engine {
   void step_tracer(int id, double dt, bool refresh_ab);
   // Device pointers / stream for benchmarking and tests.
   void *stream() const;
+  // CUDA device the engine was created on (current device at construction)
+  int device() const;
   void synchronize() const;
   // Kernel launches issued by one step() of every tracer.
   int launches_per_step() const;

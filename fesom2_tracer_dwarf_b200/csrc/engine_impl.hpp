@@ -54,6 +54,7 @@ struct EngineImpl {
   size_t ts_bytes = 8;  // tracer storage element
   size_t r_bytes = 8;   // compute / geometry / work element
   cudaStream_t stream = nullptr;
+  int device = 0;  // current CUDA device when the engine was created
   std::vector<void *> allocs;
   size_t bytes = 0;
   DMeshT<double> dm64{};

@@ -233,9 +233,13 @@ int tracer_selftest_sround(int fmt, long long n, int draws, uint32_t seed, long 
  * (tracer_mesh_dims()[5]) of doubles.  Work space comes from a 64 MiB
  * static device array (tracer_noalloc_scratch_bytes()) shared by every call:
  * meshes needing more are rejected with -1; calls that overlap on the GPU
- * race.  The device state must exist (tracer_init_for_advection); the first
- * call on a device looks up the array's device address and should come
- * before any stream capture.  Returns after the step has finished. */
+ * race.  The device state must exist (tracer_init_for_advection, which also
+ * commits the static array on the engine's device and looks up its address,
+ * so it should come before the host reserves its memory pool and before any
+ * stream capture).  The step runs on the engine's device whatever the
+ * calling thread's current device, and first waits for all work already
+ * queued on that device (so inputs written asynchronously by the caller are
+ * complete).  Returns after the step has finished. */
 int tracer_advect_device_noalloc(int tracer_id, const double *T_dev, const double *TAB_dev,
                                  double *T_out_dev, double dt);
 /* Size in bytes of the static work array of tracer_advect_device_noalloc. */
