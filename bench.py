@@ -20,7 +20,9 @@ Arms:
   --impl reference   the reference algorithm on the host cores: the CPU
                      oracle (a C restatement of the reference's Fortran, which
                      cannot be compiled here: no Fortran compiler), OpenMP over
-                     all host threads, on a bounded sample of the same workload.
+                     all host threads, on the same full-size workload, with
+                     inputs built by the oracle's own restatement of the
+                     seeded generators (the product library is not loaded).
 
 Multi-GPU (torchrun): every rank advects its own replica of the workload on
 its own GPU with no data-path collective (weak scaling); a barrier brackets
@@ -73,6 +75,15 @@ def parse():
 def workload_name(nx, nl):
     return (f"periodic {nx}x{nx}x{nl} (left-oriented edges), smooth bathymetry U[3,{nl}] seed 0, "
             "divergence-free layered flow CFL 0.5, MUSCL+PPM+FCT, 2 tracers")
+
+
+def workload_config(nx, nl, cells, dt, gpus):
+    """The workload description both arms print (identical for the same
+    workload): per-step algorithmic FP64 traffic against the L2 size."""
+    step_gb = BYTES_PER_CELL["fp64"] * cells * 2 / 1e9
+    return {"workload": workload_name(nx, nl), "wet_cells": cells, "tracers": 2, "dt_s": dt,
+            "parallelism": f"replicas x{gpus}",
+            "l2": f"inputs larger than L2 ({step_gb:.2f} GB of FP64 fields per step vs {L2_BYTES / 1e9:.2f} GB L2)"}
 
 
 def make_inputs(api, nx, nl):
@@ -161,28 +172,26 @@ def committed_traffic(args):
 
 
 # ---------------------------------------------------------------------------
-# CPU arm: the oracle on a bounded sample
+# CPU arm: the oracle (a C restatement of the reference's Fortran) on the same
+# workload.  Its inputs are built by the oracle's own restatement of the
+# seeded generators (bit-identical to the library's, tests/test_synth_oracle.py),
+# so this arm never loads the product library.
 # ---------------------------------------------------------------------------
-def cpu_rate(nx_sample, nl, steps, warmup=1, serial=False):
-    """Cell-updates/s of the oracle (OpenMP on every host thread, or the
-    serial build) on a periodic nx_sample^2 x nl mesh drawn like the GPU
-    workload.  Returns (rate, threads, sample text, per-step seconds)."""
+def cpu_run(nx, nl, steps, warmup=1, serial=False):
+    """Runs the oracle (OpenMP on every host thread, or the serial build) on
+    the periodic nx^2 x nl layered-flow workload, 2 tracers, MUSCL+PPM+FCT,
+    valuesAB := values.  Returns (rate, threads, sample text, per-step
+    seconds)."""
     sys.path.insert(0, str(ROOT / "oracle"))
     import pyoracle
-    from fesom2_tracer_dwarf_b200 import FESOMTracerAdvection
-    api = FESOMTracerAdvection()
-    api.cleanup()
-    K, uv, w, T, S, dt, cells = make_inputs(api, nx_sample, nl)
-    api.cleanup()
     o = pyoracle.Oracle(openmp=not serial)
     if not serial:
         o.set_threads(os.cpu_count() or 1)
-    m = pyoracle.OracleMesh(o, nx_sample, nx_sample, nl, periodic=True, full_rings=True, node_K=K,
-                            left_oriented=True)
-    N = m.nod2D
+    m, K, uv, w, T, S, dt, cells = pyoracle.layered_flow_case(o, nx, nl, seed=0)
     vals = np.ascontiguousarray(np.stack([T.T, S.T]))  # (2, nod2D, nl-1): each tracer a Fortran (nl-1, nod2D) block
     ab = vals.copy()
-    m.run(vals, ab, uv, w, dt, warmup, "MUSCL", "PPM", "FCT", refresh_ab=True)
+    if warmup:
+        m.run(vals, ab, uv, w, dt, warmup, "MUSCL", "PPM", "FCT", refresh_ab=True)
     per = []
     for _ in range(steps):
         t0 = time.perf_counter()
@@ -190,24 +199,26 @@ def cpu_rate(nx_sample, nl, steps, warmup=1, serial=False):
         per.append(time.perf_counter() - t0)
     sec = statistics.median(per)
     rate = 2 * cells / sec
-    sample = (f"periodic {nx_sample}x{nx_sample}x{nl} ({N} nodes, {cells} wet cells), same bathymetry/flow/tracer "
-              f"distributions, 2 tracers, median of {steps} steps after {warmup} warm-up")
-    return rate, (1 if serial else o.threads()), sample, per
+    what = "the full workload" if nx == 1000 and nl == 64 else "a sample"
+    sample = (f"{what}: periodic {nx}x{nx}x{nl} ({m.nod2D} nodes, {cells} wet cells), inputs from the oracle's "
+              f"restatement of the seeded generators, 2 tracers, median of {steps} steps after {warmup} warm-up")
+    return rate, (1 if serial else o.threads()), sample, per, cells, dt
 
 
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    nx_sample = min(args.nx, 300)
     steps = max(1, args.steps)
-    rate, threads, sample, per = cpu_rate(nx_sample, args.nl, steps, warmup=max(1, min(args.warmup, 2)))
+    warmup = max(1, min(args.warmup, 2))
+    rate, threads, sample, per, cells, dt = cpu_run(args.nx, args.nl, steps, warmup=warmup)
     sec = statistics.median(per)
     line = {
         "metric": "tracer cell-updates/s", "value": rate, "unit": "cell-updates/s", "impl": "reference",
-        "n_gpus": args.gpus, "steps": steps, "warmup": args.warmup, "ms_per_step": sec * 1e3,
+        "n_gpus": args.gpus, "steps": steps, "warmup": warmup, "ms_per_step": sec * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": workload_name(args.nx, args.nl), "sample": sample},
+        "config": workload_config(args.nx, args.nl, cells, dt, args.gpus),
+        "sample": sample,
         "cpu_baseline": {"value": rate, "unit": "cell-updates/s", "cores": threads, "kind": "port",
                          "sample": sample},
         "e2e": {"value": rate, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -314,11 +325,10 @@ def run_ours(args):
             "metric": "tracer cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": DTYPE[args.precision], "data": "synthetic",
-            "config": {"workload": workload_name(args.nx, args.nl) + (", learned antidiffusive flux (MLP on "
-                                                                       "tcgen05) ahead of FCT" if args.learned else ""),
-                       "wet_cells": cells, "tracers": 2,
-                       "dt_s": dt, "parallelism": f"replicas x{world}",
-                       "l2": f"inputs larger than L2 ({dev_bytes / 1e9:.1f} GB resident vs 0.13 GB L2)"},
+            "config": workload_config(args.nx, args.nl, cells, dt, world),
+            "device_bytes": dev_bytes,
+            "precision": args.precision + (", learned antidiffusive flux (MLP on tcgen05) ahead of FCT"
+                                           if args.learned else ""),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
                          "kernel": f"full step (all kernels of one step, {BYTES_PER_CELL[args.precision]} B/cell algorithmic)",
@@ -335,11 +345,14 @@ def run_ours(args):
     ranks.close()
     api.cleanup()
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        rate, threads, sample, _ = cpu_rate(min(args.nx, 300), args.nl, 3)
+        # the same workload at full size, a few steps (about 10-30 s of CPU work)
+        rate, threads, sample, _, _, _ = cpu_run(args.nx, args.nl, 3)
         result["cpu_baseline"] = {"value": rate, "unit": "cell-updates/s", "cores": threads, "kind": "port",
                                   "sample": sample}
-        # the reference's own build is serial: the same oracle on one thread
-        rate1, _, sample1, _ = cpu_rate(min(args.nx, 150), args.nl, 3, serial=True)
+        # the reference's own build is serial: the same oracle on one thread,
+        # on a smaller mesh of the same recipe (a full-size serial step takes
+        # about a minute)
+        rate1, _, sample1, _, _, _ = cpu_run(min(args.nx, 150), args.nl, 3, serial=True)
         result["cpu_baseline_serial"] = {"value": rate1, "unit": "cell-updates/s", "cores": 1, "kind": "port",
                                          "sample": sample1}
     if rank == 0:

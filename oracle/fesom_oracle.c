@@ -1836,3 +1836,226 @@ void om_stats(const om_mesh *m, const double *values, double *out) {
   }
   out[0] = mn; out[1] = mx; out[2] = sm; out[3] = nan;
 }
+
+/* ------------------------------------------------------------------------ */
+/* Seeded synthetic inputs of the benchmark workloads, restated here so that  */
+/* the CPU baseline builds its inputs without the product library.  They are  */
+/* the same functions of the same seeds as the library's generators: a CPU    */
+/* test checks the two bit for bit.                                           */
+/* ------------------------------------------------------------------------ */
+
+/* MT19937-64 (Matsumoto & Nishimura, "Mersenne Twister 64-bit", 2004): the
+ * published recurrence, tempering and seeding, which are also those of the
+ * C++ std::mt19937_64 engine. */
+typedef struct { uint64_t s[312]; int i; } mt64;
+static void mt64_seed(mt64 *g, uint64_t seed) {
+  g->s[0] = seed;
+  for (int i = 1; i < 312; i++) g->s[i] = 6364136223846793005ULL * (g->s[i - 1] ^ (g->s[i - 1] >> 62)) + (uint64_t)i;
+  g->i = 312;
+}
+static uint64_t mt64_next(mt64 *g) {
+  if (g->i >= 312) {
+    const uint64_t UM = 0xFFFFFFFF80000000ULL, LM = 0x7FFFFFFFULL, A = 0xB5026F5AA96619E9ULL;
+    for (int k = 0; k < 312; k++) {
+      const uint64_t x = (g->s[k] & UM) | (g->s[(k + 1) % 312] & LM);
+      g->s[k] = g->s[(k + 156) % 312] ^ (x >> 1) ^ ((x & 1ULL) ? A : 0ULL);
+    }
+    g->i = 0;
+  }
+  uint64_t x = g->s[g->i++];
+  x ^= (x >> 29) & 0x5555555555555555ULL;
+  x ^= (x << 17) & 0x71D67FFFEDA60000ULL;
+  x ^= (x << 37) & 0xFFF7EEE000000000ULL;
+  x ^= x >> 43;
+  return x;
+}
+static double mt64_uni(mt64 *g) { return (double)(mt64_next(g) >> 11) * 0x1.0p-53; } /* [0, 1) */
+static double mt64_normal(mt64 *g) { /* Box-Muller, first variate */
+  double u1 = mt64_uni(g), u2 = mt64_uni(g);
+  if (u1 < 1e-300) u1 = 1e-300;
+  return sqrt(-2.0 * log(u1)) * cos(2.0 * PI_F * u2);
+}
+
+/* six Fourier modes with integer wave numbers, periodic on [0,Lx) x [0,Ly) */
+typedef struct { int kx[6], ky[6]; double amp[6], ph[6]; } om_modes;
+static void modes_draw(om_modes *md, mt64 *g) {
+  for (int q = 0; q < 6; q++) {
+    md->kx[q] = 1 + (int)(mt64_next(g) % 4);
+    md->ky[q] = 1 + (int)(mt64_next(g) % 4);
+    md->amp[q] = 0.5 + mt64_uni(g);
+    md->ph[q] = 2.0 * PI_F * mt64_uni(g);
+  }
+}
+static double modes_eval(const om_modes *md, double x, double y, double Lx, double Ly) {
+  double s = 0.0;
+  for (int q = 0; q < 6; q++) s += md->amp[q] * sin(2.0 * PI_F * (md->kx[q] * x / Lx + md->ky[q] * y / Ly) + md->ph[q]);
+  return s;
+}
+
+void om_synth_bathymetry_smooth(int nx, int ny, int periodic, int nl, double corr_cells, unsigned long long seed, int *K) {
+  mt64 g;
+  mt64_seed(&g, seed);
+  enum { NM = 48 };
+  double kx[NM], ky[NM], ph[NM];
+  const double cmax = (double)(nx > ny ? nx : ny);
+  const double cc = corr_cells > 1.0 ? corr_cells : 1.0;
+  const double kmax = fmax(1.0, cmax / cc);
+  for (int q = 0; q < NM; q++) {
+    double a, b;
+    do {
+      a = floor((2.0 * mt64_uni(&g) - 1.0) * (kmax + 1.0));
+      b = floor((2.0 * mt64_uni(&g) - 1.0) * (kmax + 1.0));
+    } while (a == 0.0 && b == 0.0);
+    kx[q] = a; ky[q] = b;
+    ph[q] = 2.0 * PI_F * mt64_uni(&g);
+  }
+  const int ni = periodic ? nx - 1 : nx, nj = periodic ? ny - 1 : ny;
+  const double norm = sqrt(2.0 / NM);
+  for (int j = 0; j < nj; j++)
+    for (int i = 0; i < ni; i++) {
+      const double x = (double)i / (double)(nx - 1), y = (double)j / (double)(ny - 1);
+      double gg = 0.0;
+      for (int q = 0; q < NM; q++) gg += cos(2.0 * PI_F * (kx[q] * x + ky[q] * y) + ph[q]);
+      gg *= norm;
+      const double u = 0.5 * erfc(-gg / sqrt(2.0));
+      int k = 3 + (int)(u * (double)(nl - 2));
+      K[(size_t)j * ni + i] = imin2(nl, imax2(3, k));
+    }
+}
+
+void om_synth_velocity(const om_mesh *m, unsigned long long seed, double umax, double mode1_frac, double mode2_frac,
+                       double baro_frac, double *uv, double *W) {
+  const int N = m->nod2D, T = m->elem2D, E = m->edge2D, nl = m->nl, L = nl - 1;
+  mt64 g;
+  mt64_seed(&g, seed);
+  double *xm = malloc(sizeof(double) * N), *ym = malloc(sizeof(double) * N);
+  for (int n = 0; n < N; n++) {
+    xm[n] = A2(m->coord, 1, n + 1, 2) * R_EARTH;
+    ym[n] = A2(m->coord, 2, n + 1, 2) * R_EARTH;
+  }
+  om_modes p1, p2, chi, p0;
+  modes_draw(&p1, &g);
+  modes_draw(&p2, &g);
+  modes_draw(&chi, &g);
+  if (baro_frac != 0.0) modes_draw(&p0, &g);
+  double *f1 = malloc(sizeof(double) * N), *f2 = malloc(sizeof(double) * N), *f3 = malloc(sizeof(double) * N);
+  for (int n = 0; n < N; n++) {
+    f1[n] = modes_eval(&p1, xm[n], ym[n], m->Lx, m->Ly);
+    f2[n] = modes_eval(&p2, xm[n], ym[n], m->Lx, m->Ly);
+    f3[n] = modes_eval(&chi, xm[n], ym[n], m->Lx, m->Ly);
+  }
+  const size_t nuv = (size_t)2 * L * T;
+  memset(uv, 0, nuv * sizeof(double));
+  /* barotropic part curl(psi0), psi0 zero at nodes of an element dry at the
+   * level and on walls */
+  if (baro_frac != 0.0) {
+    int *shallowest = malloc(sizeof(int) * N);
+    char *wall = calloc(N, 1);
+    double *f0 = malloc(sizeof(double) * N);
+    for (int n = 0; n < N; n++) shallowest[n] = nl;
+    for (int e = 0; e < T; e++)
+      for (int q = 0; q < 3; q++) {
+        const int nd = m->elem2D_nodes[3 * e + q] - 1;
+        shallowest[nd] = imin2(shallowest[nd], m->nlevels[e]);
+      }
+    for (int e = 0; e < E; e++)
+      if (m->edge_tri[2 * e + 1] <= 0) { wall[m->edges[2 * e] - 1] = 1; wall[m->edges[2 * e + 1] - 1] = 1; }
+    for (int n = 0; n < N; n++) f0[n] = wall[n] ? 0.0 : baro_frac * modes_eval(&p0, xm[n], ym[n], m->Lx, m->Ly);
+    for (int e = 0; e < T; e++) {
+      const int *en = &m->elem2D_nodes[3 * e];
+      const double *gs = &m->gradient_sca[6 * e];
+      for (int k = 0; k < m->nlevels[e] - 1; k++) {
+        double psi[3];
+        for (int q = 0; q < 3; q++) psi[q] = (k + 1) > shallowest[en[q] - 1] - 1 ? 0.0 : f0[en[q] - 1];
+        uv[2 * ((size_t)e * L + k)] += -(gs[3] * psi[0] + gs[4] * psi[1] + gs[5] * psi[2]);
+        uv[2 * ((size_t)e * L + k) + 1] += gs[0] * psi[0] + gs[1] * psi[1] + gs[2] * psi[2];
+      }
+    }
+    free(shallowest); free(wall); free(f0);
+  }
+  double *c1 = malloc(sizeof(double) * (L > 0 ? L : 1)), *c2 = malloc(sizeof(double) * (L > 0 ? L : 1));
+  for (int e = 0; e < T; e++) {
+    const int a0 = m->elem2D_nodes[3 * e] - 1, a1 = m->elem2D_nodes[3 * e + 1] - 1, a2 = m->elem2D_nodes[3 * e + 2] - 1;
+    const double *gs = &m->gradient_sca[6 * e];
+#define GX(f) (gs[0] * (f)[a0] + gs[1] * (f)[a1] + gs[2] * (f)[a2])
+#define GY(f) (gs[3] * (f)[a0] + gs[4] * (f)[a1] + gs[5] * (f)[a2])
+    const double u1 = -GY(f1), v1 = GX(f1);
+    const double u2 = -GY(f2) + GX(f3), v2 = GX(f2) + GY(f3);
+#undef GX
+#undef GY
+    const int M = m->nlevels[e] - 1;
+    const double *h = &m->helem[(size_t)e * L];
+    double s1 = 0.0, s2 = 0.0, hs = 0.0;
+    for (int k = 0; k < M; k++) {
+      c1[k] = cos(PI_F * ((double)k + 0.5) / (double)M);
+      c2[k] = cos(2.0 * PI_F * ((double)k + 0.5) / (double)M);
+      s1 += c1[k] * h[k];
+      s2 += c2[k] * h[k];
+      hs += h[k];
+    }
+    s1 /= hs;
+    s2 /= hs;
+    for (int k = 0; k < M; k++) {
+      const double b1 = mode1_frac * (c1[k] - s1), b2 = mode2_frac * (c2[k] - s2);
+      uv[2 * ((size_t)e * L + k)] += b1 * u1 + b2 * u2;
+      uv[2 * ((size_t)e * L + k) + 1] += b1 * v1 + b2 * v2;
+    }
+  }
+  double vmax = 0.0;
+  for (size_t i = 0; i < nuv / 2; i++) vmax = fmax(vmax, hypot(uv[2 * i], uv[2 * i + 1]));
+  const double scale = umax < 0.0 ? -umax : (vmax > 0.0 ? umax / vmax : 0.0);
+  for (size_t i = 0; i < nuv; i++) uv[i] *= scale;
+  /* horizontal divergence of the edge volume fluxes, then W from the bottom up */
+  double *D = calloc((size_t)L * N, sizeof(double));
+  for (int e = 0; e < E; e++) {
+    const int n1 = m->edges[2 * e] - 1, n2 = m->edges[2 * e + 1] - 1;
+    const int t1 = m->edge_tri[2 * e] - 1, t2 = m->edge_tri[2 * e + 1] - 1;
+    const int nl1 = m->nlevels[t1] - 1, nl2 = t2 >= 0 ? m->nlevels[t2] - 1 : 0;
+    const double *c = &m->edge_cross_dxdy[4 * e];
+    for (int k = 0; k < imax2(nl1, nl2); k++) {
+      double v = 0.0;
+      if (k < nl1) v += (-uv[2 * ((size_t)t1 * L + k) + 1] * c[0] + uv[2 * ((size_t)t1 * L + k)] * c[1]) * m->helem[(size_t)t1 * L + k];
+      if (k < nl2) v += (uv[2 * ((size_t)t2 * L + k) + 1] * c[2] - uv[2 * ((size_t)t2 * L + k)] * c[3]) * m->helem[(size_t)t2 * L + k];
+      D[(size_t)n1 * L + k] += v;
+      D[(size_t)n2 * L + k] -= v;
+    }
+  }
+  memset(W, 0, (size_t)nl * N * sizeof(double));
+  for (int n = 0; n < N; n++) {
+    const int nlev = m->nlevels_nod2D[n];
+    for (int i = nlev - 1; i >= 2; i--) {
+      const double Ai = m->area[(size_t)n * nl + i - 1], Ai1 = m->area[(size_t)n * nl + i];
+      const double flux_below = W[(size_t)n * nl + i] * Ai1;
+      W[(size_t)n * nl + i - 1] = Ai > 0.0 ? (flux_below - D[(size_t)n * L + i - 1]) / Ai : 0.0;
+    }
+    W[(size_t)n * nl + 0] = 0.0;
+  }
+  free(D); free(c1); free(c2); free(f1); free(f2); free(f3); free(xm); free(ym);
+}
+
+void om_synth_tracer(const om_mesh *m, unsigned long long seed, int kind, double *T) {
+  const int N = m->nod2D, L = m->nl - 1;
+  mt64 g;
+  mt64_seed(&g, seed);
+  memset(T, 0, (size_t)L * N * sizeof(double));
+  if (kind == 0) {
+    double bx[8], by[8], bs[8], ba[8];
+    for (int b = 0; b < 8; b++) {
+      bx[b] = mt64_uni(&g) * m->Lx; by[b] = mt64_uni(&g) * m->Ly;
+      bs[b] = (0.03 + 0.07 * mt64_uni(&g)) * m->Lx; ba[b] = 5.0 + 10.0 * mt64_uni(&g);
+    }
+    for (int n = 0; n < N; n++) {
+      const double x = A2(m->coord, 1, n + 1, 2) * R_EARTH, y = A2(m->coord, 2, n + 1, 2) * R_EARTH;
+      double blob = 0.0;
+      for (int b = 0; b < 8; b++) {
+        double dx = fabs(x - bx[b]), dy = fabs(y - by[b]);
+        if (m->periodic) { dx = fmin(dx, m->Lx - dx); dy = fmin(dy, m->Ly - dy); }
+        blob += ba[b] * exp(-(dx * dx + dy * dy) / (bs[b] * bs[b]));
+      }
+      for (int k = 0; k < m->nlevels_nod2D[n] - 1; k++) T[(size_t)n * L + k] = 20.0 * mt64_uni(&g) + blob;
+    }
+  } else {
+    for (int n = 0; n < N; n++)
+      for (int k = 0; k < m->nlevels_nod2D[n] - 1; k++) T[(size_t)n * L + k] = 35.0 + 0.5 * mt64_normal(&g);
+  }
+}

@@ -104,6 +104,19 @@ int om_run(const om_mesh *m, int hor, int ver, int lim, double ph, double pv,
  * (src/fesom_analytic.F90:441-446). */
 void om_stats(const om_mesh *m, const double *values, double *out4);
 
+/* Seeded synthetic inputs of the benchmark workloads (the same functions of
+ * the same seeds as the library's generators, restated so that the CPU
+ * baseline does not load the product): a smooth bottom-level field K (per
+ * analytic grid node, uniform marginal on [3, nl]); a layered flow uv
+ * (2, nl-1, elem2D) and w (nl, nod2D) that is discretely divergence-free;
+ * tracer fields (nl-1, nod2D): kind 0 temperature-like U[0,20] + blobs,
+ * kind 1 salinity-like 35 + N(0, 0.5). */
+void om_synth_bathymetry_smooth(int nx, int ny, int periodic, int nl, double corr_cells,
+                                unsigned long long seed, int *K);
+void om_synth_velocity(const om_mesh *m, unsigned long long seed, double umax, double mode1_frac,
+                       double mode2_frac, double baro_frac, double *uv, double *w);
+void om_synth_tracer(const om_mesh *m, unsigned long long seed, int kind, double *T);
+
 /* Threads used by the OpenMP build (no-op in the serial build). */
 void om_set_threads(int n);
 int om_get_threads(void);

@@ -57,6 +57,10 @@ class Oracle:
         lib.om_tracer_step.argtypes = [vp, ci, ci, ci, cd, cd, cd] + [vp] * 7
         lib.om_run.argtypes = [vp, ci, ci, ci, cd, cd, cd, vp, vp, ci, ci, vp, vp, ci]
         lib.om_stats.argtypes = [vp, vp, vp]
+        u64 = ctypes.c_ulonglong
+        lib.om_synth_bathymetry_smooth.argtypes = [ci, ci, ci, ci, cd, u64, vp]
+        lib.om_synth_velocity.argtypes = [vp, u64, cd, cd, cd, cd, vp, vp]
+        lib.om_synth_tracer.argtypes = [vp, u64, ci, vp]
         lib.om_set_threads.argtypes = [ci]
         lib.om_get_threads.restype = ci
         self.lib = lib
@@ -181,7 +185,59 @@ class OracleMesh:
         self.o.lib.om_run(self.h, HOR[hor], VER[ver], LIM[lim], ph, pv, dt, _p(uv), _p(w), ntr, nsteps,
                           _p(values), _p(values_ab), int(refresh_ab))
 
+    def synth_velocity(self, seed=0, umax=1.0, mode2=0.5, baro=0.0, mode1=1.0):
+        """Seeded layered flow: uv (2, nl-1, elem2D), w (nl, nod2D)."""
+        uv = np.zeros((2, self.nl - 1, self.elem2D), order="F")
+        w = np.zeros((self.nl, self.nod2D), order="F")
+        self.o.lib.om_synth_velocity(self.h, seed, umax, mode1, mode2, baro, _p(uv), _p(w))
+        return uv, w
+
+    def synth_tracer(self, seed=0, kind=0):
+        v = np.zeros((self.nl - 1, self.nod2D), order="F")
+        self.o.lib.om_synth_tracer(self.h, seed, kind, _p(v))
+        return v
+
     def stats(self, values):
         s = np.zeros(4)
         self.o.lib.om_stats(self.h, _p(np.asfortranarray(values)), _p(s))
         return s
+
+
+def synth_bathymetry_smooth(oracle: Oracle, nx, ny, nl, periodic=True, corr_cells=40.0, seed=0):
+    """Smooth seeded bottom level index per analytic grid node (uniform on [3, nl])."""
+    n = (nx - 1) * (ny - 1) if periodic else nx * ny
+    K = np.zeros(n, dtype=np.int32)
+    oracle.lib.om_synth_bathymetry_smooth(nx, ny, int(periodic), nl, corr_cells, seed, _p(K))
+    return K
+
+
+LX = LY = 1.0e5
+MAX_DEPTH = 1000.0
+
+
+def cfl_dt(nx, ny, nl, uv, w, cfl=0.5):
+    """dt at CFL `cfl` of the faster of the horizontal and vertical crossings
+    on the uniform analytic grid."""
+    dx = min(LX / (nx - 1), LY / (ny - 1))
+    dz = MAX_DEPTH / (nl - 1)
+    umax = float(np.sqrt(uv[0] ** 2 + uv[1] ** 2).max())
+    wmax = float(np.abs(w).max())
+    rate = max(umax / dx, wmax / dz)
+    return cfl / rate if rate > 0.0 else 1.0
+
+
+def layered_flow_case(oracle: Oracle, nx, nl, seed=0, periodic=True):
+    """The benchmark's plain-method-at-scale inputs built by the oracle alone:
+    the same mesh, bathymetry, flow, tracers and dt as the library's
+    workloads.layered_flow_case for the same arguments.  Returns
+    (mesh, K, uv, w, T, S, dt, wet_cells)."""
+    corr = max(4.0, nx / 25.0)
+    K = synth_bathymetry_smooth(oracle, nx, nx, nl, periodic=periodic, corr_cells=corr, seed=seed)
+    m = OracleMesh(oracle, nx, nx, nl, Lx=LX, Ly=LY, max_depth=MAX_DEPTH, periodic=periodic, full_rings=True,
+                   node_K=K, left_oriented=True)
+    uv, w = m.synth_velocity(seed=seed + 1, umax=1.0, mode2=0.5, baro=1.0)
+    T = m.synth_tracer(seed=seed + 2, kind=0)
+    S = m.synth_tracer(seed=seed + 3, kind=1)
+    nlev = m.array("nlevels_nod2D")[: m.nod2D]
+    wet = int(np.maximum(nlev - 1, 0).sum())
+    return m, K, uv, w, T, S, cfl_dt(nx, nx, nl, uv, w), wet
