@@ -59,6 +59,10 @@ SIGNATURES = {
     "tracer_set_ab_refresh": (ctypes.c_int, [ctypes.c_int]),
     "tracer_set_precision": (ctypes.c_int, [ctypes.c_int]),
     "tracer_set_rounding": (ctypes.c_int, [ctypes.c_int]),
+    "tracer_set_step_path": (ctypes.c_int, [ctypes.c_int]),
+    "tracer_step_info": (ctypes.c_int, [_vp]),
+    "tracer_set_patch_size": (ctypes.c_int, [ctypes.c_int]),
+    "tracer_tile_plan_check": (ctypes.c_int, [ctypes.c_int, _vp]),
     "tracer_host_register": (ctypes.c_int, [_vp, ctypes.c_longlong]),
     "tracer_host_unregister": (ctypes.c_int, [_vp]),
     "tracer_storage_offset": (ctypes.c_int, [ctypes.c_int, _vp]),

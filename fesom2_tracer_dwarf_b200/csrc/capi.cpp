@@ -16,6 +16,7 @@
 #include "engine.hpp"
 #include "output.hpp"
 #include "partition.hpp"
+#include "tile.hpp"
 
 using namespace fesom;
 
@@ -38,6 +39,8 @@ struct State {
   bool pend_vel = false;
   Precision prec = Precision::FP64;
   int sround = 0;  // rounding of 16-bit stores (tracer_set_rounding)
+  int step_path = 0;  // tracer_set_step_path
+  int patch_size = 0;  // tracer_set_patch_size (0: the default)
 };
 State g;
 std::unique_ptr<Decomposition> g_dd;  // domain-decomposed runner (tracer_dd_*)
@@ -67,6 +70,8 @@ void ensure_engine() {
   if (!g.mesh) throw std::runtime_error("no mesh connectivity: use tracer_init_analytic or tracer_set_mesh_arrays");
   g.eng.reset(new Engine(*g.mesh, g.prec));
   g.eng->set_rounding(g.sround);
+  g.eng->set_step_path(g.step_path);
+  if (g.patch_size > 0) g.eng->set_patch_size(g.patch_size);
   if (g.ntr > 0) {
     g.eng->allocate_tracers(g.ntr);
     for (int i = 0; i < g.ntr; i++) {
@@ -458,6 +463,54 @@ int tracer_set_rounding(int mode) {
   g.sround = mode;
   if (g.eng) g.eng->set_rounding(mode);
   return 0;
+}
+
+int tracer_set_step_path(int path) {
+  return guarded([&] {
+    if (path < 0 || path > 1) return fail("step path must be 0 (fused where possible) or 1 (five kernels)");
+    g.step_path = path;
+    if (g.eng) g.eng->set_step_path(path);
+    return 0;
+  });
+}
+
+int tracer_tile_plan_check(int max_owned, double *out8) {
+  return guarded([&] {
+    if (!out8) return fail("null output");
+    if (!g.mesh) return fail("no mesh");
+    if (max_owned < 1) return fail("max_owned must be positive");
+    const std::vector<int> slot = edge_slot_order(*g.mesh);
+    const TilePlanHost P = build_tile_plan(*g.mesh, slot, max_owned);
+    const std::string bad = check_tile_plan(*g.mesh, P, slot);
+    if (!bad.empty()) return fail("tile plan: " + bad);
+    int mn = 1 << 30;
+    for (const TileCounts &c : P.cnt) mn = std::min(mn, c.n0);
+    out8[0] = P.np; out8[1] = mn; out8[2] = P.max_n2; out8[3] = P.max_n3;
+    out8[4] = P.max_e2; out8[5] = P.max_el; out8[6] = P.node_ratio; out8[7] = P.edge_ratio;
+    return 0;
+  });
+}
+
+int tracer_set_patch_size(int owned) {
+  return guarded([&] {
+    if (owned < 0) return fail("patch size must be >= 0 (0: the default)");
+    g.patch_size = owned;
+    if (g.eng) g.eng->set_patch_size(owned > 0 ? owned : kTileOwned);
+    return 0;
+  });
+}
+
+int tracer_step_info(double *out4) {
+  return guarded([&] {
+    if (!out4) return fail("null output");
+    if (check_ready()) return -1;
+    ensure_engine();
+    out4[0] = g.eng->step_path();
+    out4[1] = (g.ntr > 0 && g.eng->num_tracers() > 0) ? (g.eng->fused(0) ? 1.0 : 0.0) : 0.0;
+    out4[2] = g.eng->tile_count();
+    out4[3] = g.eng->tile_node_ratio();
+    return 0;
+  });
 }
 
 int tracer_storage_offset(int tracer_id, double *off) {

@@ -182,7 +182,57 @@ void build_dmesh(EngineImpl &P, DMeshT<R> &d, const std::vector<int> &slot_edge,
   build_schedules(P, d, kCellsPerBlock);
 }
 
+// Patch plan of the fused step kernel: built on the host, uploaded, host
+// lists released (the maxima stay for the shared-memory layout).
+void build_tiles(EngineImpl &P, const std::vector<int> &edge_slot, int owned) {
+  for (const void *q : {(const void *)P.tiles.cnt, (const void *)P.tiles.node_gid, (const void *)P.tiles.node_info,
+                        (const void *)P.tiles.inc_ptr, (const void *)P.tiles.inc, (const void *)P.tiles.edge_slot,
+                        (const void *)P.tiles.edge_nn, (const void *)P.tiles.edge_ud, (const void *)P.tiles.elem_gid,
+                        (const void *)P.tiles.elem_nn, (const void *)P.tiles.ring_ptr, (const void *)P.tiles.ring})
+    P.dfree(const_cast<void *>(q));
+  P.tiles = DTiles{};
+  P.tplan = TilePlanHost();
+  if (P.mesh.nod2D <= 0 || P.mesh.nl > kTileMaxLevels) return;
+  TilePlanHost &t = P.tplan;
+  try {
+    t = build_tile_plan(P.mesh, edge_slot, owned);
+  } catch (const std::runtime_error &) {
+    t = TilePlanHost();  // no plan: the five-kernel path runs every scheme
+    return;
+  }
+  DTiles &d = P.tiles;
+  d.cnt = P.upload(t.cnt);
+  d.node_gid = P.upload(t.node_gid);
+  d.node_info = P.upload(t.node_info);
+  d.inc_ptr = P.upload(t.inc_ptr);
+  d.inc = P.upload(t.inc);
+  d.edge_slot = P.upload(t.edge_slot);
+  d.edge_nn = P.upload(t.edge_nn);
+  d.edge_ud = P.upload(t.edge_ud);
+  d.elem_gid = P.upload(t.elem_gid);
+  d.elem_nn = P.upload(t.elem_nn);
+  d.ring_ptr = P.upload(t.ring_ptr);
+  d.ring = P.upload(t.ring);
+  d.np = t.np;
+  for (auto *v : {&t.node_gid, &t.inc_ptr, &t.edge_slot, &t.elem_gid, &t.ring_ptr}) std::vector<int>().swap(*v);
+  for (auto *v : {&t.node_info, &t.inc, &t.edge_nn, &t.edge_ud, &t.elem_nn}) std::vector<uint32_t>().swap(*v);
+  std::vector<uint16_t>().swap(t.ring);
+  std::vector<TileCounts>().swap(t.cnt);
+}
+
 }  // namespace
+
+std::vector<int> edge_slot_order(const MeshHost &M) {
+  // slot order: edges sorted by their smaller node id (stable in edge id)
+  const int E = M.edge2D;
+  std::vector<int> slot_edge(E), edge_slot(E);
+  for (int e = 0; e < E; e++) slot_edge[e] = e;
+  std::stable_sort(slot_edge.begin(), slot_edge.end(), [&](int a, int b) {
+    return std::min(M.edge_nodes[2 * a], M.edge_nodes[2 * a + 1]) < std::min(M.edge_nodes[2 * b], M.edge_nodes[2 * b + 1]);
+  });
+  for (int s = 0; s < E; s++) edge_slot[slot_edge[s]] = s;
+  return edge_slot;
+}
 
 Engine::Engine(const MeshHost &mesh, Precision prec) : p_(new EngineImpl) {
   EngineImpl &P = *p_;
@@ -199,13 +249,9 @@ Engine::Engine(const MeshHost &mesh, Precision prec) : p_(new EngineImpl) {
   P.S = prec == Precision::FP64 ? (M.nl + 3) / 4 * 4 : (M.nl + 7) / 8 * 8;
   CK(cudaGetDevice(&P.device));
   CK(cudaStreamCreateWithFlags(&P.stream, cudaStreamNonBlocking));
-  // slot order: edges sorted by their smaller node id (stable in edge id)
-  std::vector<int> slot_edge(E), edge_slot(E);
-  for (int e = 0; e < E; e++) slot_edge[e] = e;
-  std::stable_sort(slot_edge.begin(), slot_edge.end(), [&](int a, int b) {
-    return std::min(M.edge_nodes[2 * a], M.edge_nodes[2 * a + 1]) < std::min(M.edge_nodes[2 * b], M.edge_nodes[2 * b + 1]);
-  });
-  for (int s = 0; s < E; s++) edge_slot[slot_edge[s]] = s;
+  const std::vector<int> edge_slot = edge_slot_order(M);
+  std::vector<int> slot_edge(E);
+  for (int e = 0; e < E; e++) slot_edge[edge_slot[e]] = e;
   P.slot_edge = slot_edge;
   if (prec == Precision::FP64) {
     build_dmesh<double>(P, P.dm64, slot_edge, edge_slot);
@@ -214,6 +260,7 @@ Engine::Engine(const MeshHost &mesh, Precision prec) : p_(new EngineImpl) {
     build_dmesh<float>(P, P.dm32, slot_edge, edge_slot);
     build_rcp_f32(P);
   }
+  build_tiles(P, edge_slot, kTileOwned);
   P.vel = P.dalloc_bytes((size_t)2 * M.elem2D * P.S * P.r_bytes);
   P.W = P.dalloc_bytes((size_t)M.nod2D * P.S * P.r_bytes);
   CK(cudaStreamSynchronize(P.stream));
@@ -397,6 +444,14 @@ static void ensure_slots(EngineImpl &P, int n) {
   P.slots = n;
 }
 
+bool fused_step(const EngineImpl &P, const TracerScheme &sc, bool learned) {
+  if (P.step_path != 0 || P.tiles.np <= 0 || learned) return false;
+  if (P.prec != Precision::FP64 && P.prec != Precision::FP32) return false;
+  if (sc.ver != 0 && sc.ver != 1) return false;  // QR4C and CDIFF: five-kernel path
+  const TileLayout L = tile_layout(P.tplan, (unsigned)P.r_bytes, false, sc.hor != 0, sc.lim == 1);
+  return L.bytes <= (unsigned)kTileSmemMax;
+}
+
 static void dispatch(EngineImpl &P, const TracerScheme &sc, int nt, const BatchPtrs &b, double dt) {
   if (P.mesh.nod2D <= 0) return;
   if (P.prec == Precision::FP64) launch_batch_f64(P, sc, nt, b, dt);
@@ -453,11 +508,30 @@ int Engine::launches_per_step() const {
   int n = 0;
   for (int i = 0; i < (int)P.tr.size();) {
     const int nt = batch_size(P, i);
-    n += (P.tr[i].sch.lim == 1 ? 4 : 3) + (P.tr[i].sch.hor != 0 ? 1 : 0);
+    if (fused_step(P, P.tr[i].sch, learned_active(P) && P.tr[i].sch.hor == 1)) n += nt;
+    else n += (P.tr[i].sch.lim == 1 ? 4 : 3) + (P.tr[i].sch.hor != 0 ? 1 : 0);
     i += nt;
   }
   return n;
 }
+
+void Engine::set_step_path(int path) {
+  if (path < 0 || path > 1) throw std::invalid_argument("step path must be 0 (fused where possible) or 1 (five kernels)");
+  p_->step_path = path;
+}
+int Engine::step_path() const { return p_->step_path; }
+bool Engine::fused(int id) const {
+  check_id(*p_, id);
+  return fused_step(*p_, p_->tr[id].sch, learned_active(*p_) && p_->tr[id].sch.hor == 1);
+}
+int Engine::tile_count() const { return p_->tiles.np; }
+void Engine::set_patch_size(int owned) {
+  if (owned < 1) throw std::invalid_argument("patch size must be at least one owned node");
+  CK(cudaStreamSynchronize(p_->stream));
+  build_tiles(*p_, edge_slot_order(p_->mesh), owned);
+  CK(cudaStreamSynchronize(p_->stream));
+}
+double Engine::tile_node_ratio() const { return p_->tplan.node_ratio; }
 
 void Engine::step_tracer(int id, double dt, bool refresh_ab) {
   check_id(*p_, id);
@@ -503,7 +577,7 @@ void Engine::step_with_scratch(int id, const double *T, const double *TAB, doubl
 }
 
 const char *const *Engine::kernel_kind_names(int *n) {
-  static const char *const names[KK_COUNT] = {"k_edge", "k_col1", "k_col2", "k_col3", "k_grad"};
+  static const char *const names[KK_COUNT] = {"k_edge", "k_col1", "k_col2", "k_col3", "k_grad", "k_tile", "k_vflux"};
   *n = KK_COUNT;
   return names;
 }

@@ -29,6 +29,10 @@ enum class Precision { FP64 = 0, FP32 = 1, BF16 = 2, FP16 = 3 };
 
 struct EngineImpl;
 
+// Storage slot of every edge in the engine's edge arrays (edges sorted by
+// their smaller node id, stable in edge id).
+std::vector<int> edge_slot_order(const MeshHost &m);
+
 // Page-lock a host range for single-DMA tracer transfers (transfer.cu);
 // 0 on success.
 int host_register(void *p, size_t bytes);
@@ -99,6 +103,18 @@ class Engine {
   void *stream() const;
   // CUDA device the engine was created on (current device at construction)
   int device() const;
+  // Step kernels: 0 = the fused patch kernel wherever the scheme allows it
+  // (FP64 or FP32 storage, PPM or UPW1 vertical, no learned flux), else the
+  // five-kernel path; 1 = always the five-kernel path.  Both give the same
+  // bits.
+  void set_step_path(int path);
+  int step_path() const;
+  bool fused(int id) const;      // whether tracer id's steps run the fused kernel
+  int tile_count() const;        // patches of the fused kernel's plan (0: none)
+  // Rebuilds the fused kernel's plan with patches of about `owned` owned
+  // nodes (default kTileOwned); any size gives the same results.
+  void set_patch_size(int owned);
+  double tile_node_ratio() const;  // LO-solution nodes computed per node (halo redundancy)
   void synchronize() const;
   // Kernel launches issued by one step() of every tracer.
   int launches_per_step() const;

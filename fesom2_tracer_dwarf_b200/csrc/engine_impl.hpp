@@ -10,6 +10,7 @@
 
 #include "dmesh.hpp"
 #include "engine.hpp"
+#include "tile.hpp"
 
 namespace fesom {
 
@@ -78,6 +79,12 @@ struct EngineImpl {
   int slots = 0;
   void *vflux = nullptr;
   bool vflux_valid = false;  // vflux holds the edge volume fluxes of the current velocity
+  // fused patch kernel (tile.cuh): the plan's maxima (host lists released
+  // after upload) and its device copy; step_path 0 runs it wherever the
+  // scheme allows, 1 always runs the five-kernel path
+  TilePlanHost tplan;
+  DTiles tiles{};
+  int step_path = 0;
   void *adfh[kBatchMax] = {}, *adfv[kBatchMax] = {}, *lo[kBatchMax] = {}, *rp[kBatchMax] = {}, *rm[kBatchMax] = {};
   void *gradn[kBatchMax] = {};
 
@@ -147,11 +154,14 @@ struct EngineImpl {
 };
 
 // Kernel kinds reported by profile_steps.
-enum { KK_EDGE = 0, KK_COL1, KK_COL2, KK_COL3, KK_GRAD, KK_COUNT };
+enum { KK_EDGE = 0, KK_COL1, KK_COL2, KK_COL3, KK_GRAD, KK_TILE, KK_VFLUX, KK_COUNT };
 
 // Launch one batch of nt tracers (kernels in step_f64.cu / step_f32.cu).
 void launch_batch_f64(EngineImpl &P, const TracerScheme &sc, int nt, const BatchPtrs &b, double dt);
 void launch_batch_f32(EngineImpl &P, const TracerScheme &sc, int nt, const BatchPtrs &b, double dt);
+// Whether the fused patch kernel runs a batch of this scheme (precision,
+// storage type, vertical scheme, learned flux and plan permitting).
+bool fused_step(const EngineImpl &P, const TracerScheme &sc, bool learned);
 // Geometry reciprocals of k_col3 (step_f64.cu / step_f32.cu).
 void build_rcp_f64(EngineImpl &P);
 void build_rcp_f32(EngineImpl &P);

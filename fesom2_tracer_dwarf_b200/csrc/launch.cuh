@@ -6,6 +6,7 @@
 
 #include "advect_fused.cuh"
 #include "engine_impl.hpp"
+#include "tile.cuh"
 
 namespace fesom {
 
@@ -102,8 +103,64 @@ void build_rcp_planes_t(EngineImpl &P, DMeshT<R> &d) {
   d.rcp_plane = plane;
 }
 
+// Edge volume fluxes of every edge level (the values k_edge computes and
+// stores), for the fused kernel, which reads them.
+template <typename R>
+__global__ void __launch_bounds__(256) k_vflux(DMeshT<R> m, const R *vel, R *vflux) {
+  const size_t n = (size_t)m.E * m.S;
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
+    const int s = (int)(q / m.S), k = (int)(q - (size_t)s * m.S);
+    if (k >= m.edge_lev[s].y) continue;
+    vflux[q] = edge_vflux(m, edge_ctx(m, s), vel, k);
+  }
+}
+
+template <typename R, int LIM, bool AB>
+void launch_tile(EngineImpl &P, const TileArgs<R> &a, const TileLayout &L) {
+  set_smem(k_tile<R, LIM, AB>, L.bytes);
+  k_tile<R, LIM, AB><<<P.tiles.np, kTileThreads, L.bytes, P.stream>>>(dmesh<R>(P), a, P.tiles, L);
+}
+
+// One batch through the fused patch kernel: the edge volume fluxes first
+// when the batch does not find them stored, then one launch per tracer.
+template <typename R>
+void run_tiles(EngineImpl &P, const TracerScheme &sc, int nt, const BatchPtrs &b, double dt) {
+  const DMeshT<R> &m = dmesh<R>(P);
+  if (b.vflux_mode != 2) {
+    const size_t n = (size_t)m.E * m.S;
+    const int grid = (int)std::max<size_t>(1, std::min<size_t>((n + 255) / 256, (size_t)148 * 16));
+    P.mark_begin(KK_VFLUX);
+    k_vflux<R><<<grid, 256, 0, P.stream>>>(m, (const R *)P.vel, (R *)b.vflux);
+    P.mark_end();
+  }
+  for (int t = 0; t < nt; t++) {
+    TileArgs<R> a{};
+    a.T = (const R *)b.T[t];
+    a.TAB = (const R *)b.TAB[t];
+    a.T_out = (R *)b.T_out[t];
+    a.vflux = (const R *)b.vflux;
+    a.W = (const R *)P.W;
+    a.dt = (R)dt;
+    a.ph = (R)sc.ph;
+    a.hor = sc.hor;
+    a.ver = sc.ver;
+    const bool ab = b.TAB[t] == b.T[t];
+    const TileLayout L = tile_layout(P.tplan, (unsigned)sizeof(R), ab, sc.hor != 0, sc.lim == 1);
+    P.mark_begin(KK_TILE);
+    if (sc.lim == 1) ab ? launch_tile<R, LIM_FCT, true>(P, a, L) : launch_tile<R, LIM_FCT, false>(P, a, L);
+    else ab ? launch_tile<R, LIM_NONE, true>(P, a, L) : launch_tile<R, LIM_NONE, false>(P, a, L);
+    P.mark_end();
+  }
+}
+
 template <typename R, typename TS>
 void launch_batch_t(EngineImpl &P, const TracerScheme &sc, int nt, const BatchPtrs &b, double dt) {
+  if constexpr (std::is_same<R, TS>::value) {
+    if (fused_step(P, sc, b.feat[0] != nullptr)) {
+      run_tiles<R>(P, sc, nt, b, dt);
+      return;
+    }
+  }
   FusedArgs<R, TS> a{};
   for (int t = 0; t < nt; t++) {
     a.T[t] = (const TS *)b.T[t];

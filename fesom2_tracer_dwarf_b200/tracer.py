@@ -165,6 +165,20 @@ class FESOMTracerAdvection:
         _lib.check(self.lib, self.lib.tracer_volume_sum(tracer_id, _lib.ptr(out)), "tracer_volume_sum")
         return float(out[0]), float(out[1])
 
+    def set_step_path(self, path):
+        """'fused' (default: one patch kernel per tracer where the scheme allows it) or 'five' (five kernels)."""
+        _lib.check(self.lib, self.lib.tracer_set_step_path({"fused": 0, "five": 1}[path]), "tracer_set_step_path")
+
+    def set_patch_size(self, owned):
+        """Owned nodes per patch of the fused kernel (0: the default)."""
+        _lib.check(self.lib, self.lib.tracer_set_patch_size(int(owned)), "tracer_set_patch_size")
+
+    def step_info(self):
+        """dict(path, fused, patches, node_ratio) of the device state (tracer_step_info)."""
+        out = np.zeros(4)
+        _lib.check(self.lib, self.lib.tracer_step_info(_lib.ptr(out)), "tracer_step_info")
+        return {"path": int(out[0]), "fused": bool(out[1]), "patches": int(out[2]), "node_ratio": float(out[3])}
+
     def set_ab_refresh(self, on):
         self.lib.tracer_set_ab_refresh(int(bool(on)))
 

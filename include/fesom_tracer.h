@@ -157,6 +157,29 @@ int tracer_set_precision(int mode);
  * latest full upload (tracer_set_values); tracer_storage_offset returns it
  * (0 in modes 0, 1). */
 int tracer_set_rounding(int mode);
+/* Step kernels (no counterpart in the reference): 0 (default) = one fused
+ * kernel per tracer, a thread block per mesh patch that keeps the patch and
+ * three halo rings on chip and writes only the new values, wherever the
+ * scheme allows it (FP64 or FP32 modes, PPM or UPW1 vertical, no learned
+ * flux); 1 = always the five-kernel path (gradients, edges, LO solution, FCT
+ * ratios, update) with the intermediates in device memory.  Both paths give
+ * bit-identical results.  tracer_step_info reports out4[0] = the path,
+ * out4[1] = 1 when tracer 1 runs the fused kernel, out4[2] = patches of the
+ * fused kernel's plan, out4[3] = the plan's LO-solution nodes per mesh node
+ * (its halo redundancy). */
+int tracer_set_step_path(int path);
+int tracer_step_info(double *out4);
+/* Owned nodes per patch of the fused kernel's plan (0 = the default, 225);
+ * every size gives the same results, small ones recompute more halo. */
+int tracer_set_patch_size(int owned);
+/* Builds the fused kernel's patch plan for the loaded mesh on the host (no
+ * device needed) with patches of about max_owned owned nodes, checks it
+ * against the mesh (every node owned once, three halo rings, incidence lists
+ * in ascending edge id, up/down triangles, rings) and returns out8 =
+ * {patches, smallest owned count, largest N2 and N3 region, largest edge and
+ * element counts, LO-solution nodes per mesh node, edges per mesh edge};
+ * -1 with a message when a check fails. */
+int tracer_tile_plan_check(int max_owned, double *out8);
 /* Page-lock a host range (cudaHostRegister) so that tracer_set_values*,
  * tracer_get_values* and tracer_advect_* transfers from / to arrays inside it
  * take one DMA each way instead of going through the library's pinned
