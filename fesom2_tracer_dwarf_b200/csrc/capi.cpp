@@ -16,6 +16,7 @@
 #include "engine.hpp"
 #include "output.hpp"
 #include "partition.hpp"
+#include "restart.hpp"
 #include "tile.hpp"
 
 using namespace fesom;
@@ -41,6 +42,7 @@ struct State {
   int sround = 0;  // rounding of 16-bit stores (tracer_set_rounding)
   int step_path = 0;  // tracer_set_step_path
   int patch_size = 0;  // tracer_set_patch_size (0: the default)
+  std::vector<int> ids;  // tracer IDs read from a restart
 };
 State g;
 std::unique_ptr<Decomposition> g_dd;  // domain-decomposed runner (tracer_dd_*)
@@ -136,15 +138,87 @@ extern "C" {
 int tracer_init_mpi(int) { return 0; }
 int tracer_finalize_mpi(void) { return 0; }
 
+// Installs a restart's mesh, and its tracers and flow when read.
+static void install_restart(RestartData &&d) {
+  install_mesh(std::move(d.mesh));
+  g.ntr = (int)d.values.size();
+  g.schemes = d.schemes;
+  g.pend_values = std::move(d.values);
+  g.pend_ab = std::move(d.values_ab);
+  g.ids = d.ids;
+  if (!d.uv.empty()) {
+    g.pend_uv = std::move(d.uv);
+    g.pend_w = std::move(d.w);
+    g.pend_vel = true;
+  }
+  g.ab_refresh = false;  // valuesAB as stored, like the reference's drivers
+  g.initialized = true;
+}
+
 int tracer_init(const char *restart_dir) {
-  return fail(std::string("binary restart input is not supported by this build (") + (restart_dir ? restart_dir : "") + ")");
+  return guarded([&] {
+    if (!restart_dir) return fail("tracer_init: null restart_dir");
+    install_restart(read_restart(restart_dir, true, true));
+    std::printf("Tracer initialized from: %s/np1\n", restart_dir);
+    return 0;
+  });
 }
+
 int tracer_finalize(const char *output_dir) {
-  return fail(std::string("binary restart output is not supported by this build (") + (output_dir ? output_dir : "") + ")");
+  return guarded([&] {
+    if (!g.initialized) return fail("tracer not initialized.");
+    if (!output_dir) return fail("tracer_finalize: null output_dir");
+    if (!g.mesh) return fail("tracer_finalize: no mesh connectivity to write");
+    RestartData d;
+    d.mesh = *g.mesh;
+    const size_t LN = (size_t)(g.nl - 1) * g.nod2D;
+    for (int t = 0; t < g.ntr; t++) {
+      std::vector<double> v(LN), ab(LN);
+      if (g.eng) {
+        g.eng->get_values(t, v.data());
+        if (g.ab_refresh) ab = v;
+        else g.eng->get_values_ab(t, ab.data());
+      } else {
+        v = g.pend_values[t].empty() ? std::vector<double>(LN, 0.0) : g.pend_values[t];
+        ab = (g.ab_refresh || g.pend_ab[t].empty()) ? v : g.pend_ab[t];
+      }
+      d.values.push_back(std::move(v));
+      d.values_ab.push_back(std::move(ab));
+      d.schemes.push_back(g.schemes[t]);
+      d.ids.push_back(t < (int)g.ids.size() ? g.ids[t] : t + 1);
+    }
+    if (g.pend_vel) {
+      d.uv = g.pend_uv;
+      d.w = g.pend_w;
+    }
+    write_restart(output_dir, d);
+    std::printf("Restart files written to: %s/np1\n", output_dir);
+    g.initialized = false;  // as the reference's tracer_finalize
+    return 0;
+  });
 }
-int tracer_run_workflow(const char *restart_dir, int, double) { return tracer_init(restart_dir); }
+
+int tracer_run_workflow(const char *restart_dir, int nsteps, double dt) {
+  int status = tracer_init(restart_dir);
+  if (status) return status;
+  for (int step = 1; step <= nsteps; step++) {
+    if ((status = tracer_advect_step(dt))) return status;
+    double mn = 0, mx = 0, sm = 0;
+    if ((status = tracer_get_stats(&mn, &mx, &sm))) return status;
+    std::printf("Step %3d: min/max/sum = %15.6E%15.6E%15.6E\n", step, mn, mx, sm);
+  }
+  return tracer_finalize(restart_dir);
+}
+
 int tracer_load_mesh_partition(const char *restart_dir) {
-  return fail(std::string("binary restart input is not supported by this build (") + (restart_dir ? restart_dir : "") + ")");
+  return guarded([&] {
+    if (!restart_dir) return fail("tracer_load_mesh_partition: null restart_dir");
+    RestartData d = read_restart(restart_dir, false, true);
+    const int nl = d.mesh.nl, N = d.mesh.nod2D, E = d.mesh.edge2D;
+    install_restart(std::move(d));
+    std::printf("Loaded mesh partition from: %s/np1\n  Mesh: nl=%8d, nod2D=%8d, edge2D=%8d\n", restart_dir, nl, N, E);
+    return 0;
+  });
 }
 int tracer_load_mesh_from_files_opts(const char *mesh_path, int rotate, double alpha, double beta, double gamma,
                                      double angle_scale, double cyclic_length) {
@@ -225,6 +299,7 @@ int tracer_allocate_tracers(int num_tracers, int nl, int nod2D, int AB_order) {
     if (nl != g.nl || nod2D != g.nod2D) return fail("tracer_allocate_tracers: dimensions do not match");
     if (AB_order < 1) return fail("AB_order < 1");
     g.ntr = num_tracers;
+    g.ids.clear();
     g.schemes.assign(num_tracers, TracerScheme());
     g.pend_values.assign(num_tracers, std::vector<double>((size_t)(nl - 1) * nod2D, 0.0));
     g.pend_ab.assign(num_tracers, std::vector<double>());

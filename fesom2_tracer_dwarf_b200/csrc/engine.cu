@@ -398,6 +398,14 @@ void Engine::get_values(int id, double *out) const {
   stage_download(P, out);
 }
 
+void Engine::get_values_ab(int id, double *out) const {
+  EngineImpl &P = *p_;
+  check_id(P, id);
+  CK(cudaStreamSynchronize(P.stream));
+  stage_unpack(P, P.tr[id].TAB ? P.tr[id].TAB : P.tr[id].T, P.tr[id].off);
+  stage_download(P, out);
+}
+
 void Engine::set_rounding(int mode) {
   if (mode < 0 || mode > 1) throw std::invalid_argument("rounding mode must be 0 (nearest) or 1 (stochastic)");
   p_->sround = mode;

@@ -93,6 +93,8 @@ class Engine {
   void set_values(int id, const double *v, bool also_ab);
   void set_values_ab(int id, const double *v);
   void get_values(int id, double *out) const;
+  // valuesAB of tracer id (its own array, or the values when it has none)
+  void get_values_ab(int id, double *out) const;
   void set_scheme(int id, const TracerScheme &s);
   TracerScheme scheme(int id) const;
   // Advance every tracer one step.  refresh_ab: valuesAB := values first.

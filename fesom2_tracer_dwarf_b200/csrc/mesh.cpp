@@ -361,7 +361,9 @@ MeshHost build_analytic_mesh(int nx, int ny, int nl, double Lx, double Ly, doubl
   return m;
 }
 
-void MeshHost::finalize_tables() {
+void MeshHost::finalize_tables() { finalize_tables(true); }
+
+void MeshHost::finalize_tables(bool muscl_tables) {
   const int N = nod2D, E = edge2D;
   // nlevels_nod2D_min over the rings (lib/oce_mesh.F90:1522-1560)
   nlev_node_min.assign(N, 0);
@@ -377,6 +379,21 @@ void MeshHost::finalize_tables() {
     if (edge_tri[2 * e + 1] >= 0) a = 0.5 * (a + kREarth * elem_cos[edge_tri[2 * e + 1]]);
     edge_a[e] = a;
   }
+  if (muscl_tables) build_muscl_tables();
+  // node -> incident edges, ascending edge id
+  node_edge_ptr.assign(N + 1, 0);
+  for (int e = 0; e < E; e++) { node_edge_ptr[edge_nodes[2 * e] + 1]++; node_edge_ptr[edge_nodes[2 * e + 1] + 1]++; }
+  std::partial_sum(node_edge_ptr.begin(), node_edge_ptr.end(), node_edge_ptr.begin());
+  node_edge.resize(node_edge_ptr[N]);
+  std::vector<int> fill(node_edge_ptr.begin(), node_edge_ptr.end() - 1);
+  for (int e = 0; e < E; e++) {
+    node_edge[fill[edge_nodes[2 * e]]++] = (e << 1);
+    node_edge[fill[edge_nodes[2 * e + 1]]++] = (e << 1) | 1;
+  }
+}
+
+void MeshHost::build_muscl_tables() {
+  const int E = edge2D;
   // up/down-wind triangles (lib/oce_muscl_adv.F90:245-338) with a
   // minimum-image wrap on periodic meshes; the last matching ring element wins
   up_dn_tri.assign(2 * E, -1);
@@ -411,6 +428,11 @@ void MeshHost::finalize_tables() {
       }
     }
   }
+  build_nboundary_lay();
+}
+
+void MeshHost::build_nboundary_lay() {
+  const int N = nod2D, E = edge2D;
   // nboundary_lay (lib/oce_muscl_adv.F90:96-161)
   nboundary_lay.assign(N, nl - 1);
   for (int e = 0; e < E; e++) {
@@ -424,16 +446,6 @@ void MeshHost::finalize_tables() {
       nboundary_lay[n1] = std::min(nboundary_lay[n1], mn);
       nboundary_lay[n2] = std::min(nboundary_lay[n2], mn);
     }
-  }
-  // node -> incident edges, ascending edge id
-  node_edge_ptr.assign(N + 1, 0);
-  for (int e = 0; e < E; e++) { node_edge_ptr[edge_nodes[2 * e] + 1]++; node_edge_ptr[edge_nodes[2 * e + 1] + 1]++; }
-  std::partial_sum(node_edge_ptr.begin(), node_edge_ptr.end(), node_edge_ptr.begin());
-  node_edge.resize(node_edge_ptr[N]);
-  std::vector<int> fill(node_edge_ptr.begin(), node_edge_ptr.end() - 1);
-  for (int e = 0; e < E; e++) {
-    node_edge[fill[edge_nodes[2 * e]]++] = (e << 1);
-    node_edge[fill[edge_nodes[2 * e + 1]]++] = (e << 1) | 1;
   }
 }
 

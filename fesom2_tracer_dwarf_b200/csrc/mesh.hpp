@@ -87,8 +87,12 @@ struct MeshHost {
   // Number of wet (node, layer) cells.
   long long wet_cells() const;
   // Finish the derived tables (rings must exist): nlev_node_min, edge_a,
-  // up/down triangles, nboundary_lay, node->edge lists.
+  // up/down triangles, nboundary_lay, node->edge lists.  muscl_tables =
+  // false keeps up_dn_tri and nboundary_lay as given (read from a restart).
   void finalize_tables();
+  void finalize_tables(bool muscl_tables);
+  void build_muscl_tables();  // up/down triangles (from coord) and nboundary_lay
+  void build_nboundary_lay();
   std::string validate() const;  // "" when consistent
 };
 

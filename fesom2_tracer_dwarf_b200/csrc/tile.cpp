@@ -84,7 +84,40 @@ TilePlanHost build_tile_plan(const MeshHost &m, const std::vector<int> &edge_slo
   std::iota(ids.begin(), ids.end(), 0);
   std::vector<std::pair<int, int>> parts;
   const int target = std::max(1, max_owned);
-  bisect(m, ids, 0, N, (N + target - 1) / target, parts);
+  bool flat = true;  // no coordinates (a mesh read from a restart record)
+  for (int n = 1; n < N && flat; n++)
+    flat = m.coord[2 * n] == m.coord[0] && m.coord[2 * n + 1] == m.coord[1];
+  if (flat && N > 1) {
+    // breadth-first parts: from the lowest unassigned node, collect target
+    // nodes over the edge graph
+    std::vector<char> used(N, 0);
+    std::vector<int> order, queue;
+    order.reserve(N);
+    for (int s = 0; s < N; s++) {
+      if (used[s]) continue;
+      size_t head = 0;
+      queue.assign(1, s);
+      used[s] = 1;
+      const int begin = (int)order.size();
+      while (head < queue.size() && (int)order.size() - begin < target) {
+        const int n = queue[head++];
+        order.push_back(n);
+        for (int p = m.node_edge_ptr[n]; p < m.node_edge_ptr[n + 1]; p++) {
+          const int e = m.node_edge[p] >> 1;
+          const int o = m.edge_nodes[2 * e] == n ? m.edge_nodes[2 * e + 1] : m.edge_nodes[2 * e];
+          if (!used[o]) {
+            used[o] = 1;
+            queue.push_back(o);
+          }
+        }
+      }
+      for (size_t q = head; q < queue.size(); q++) used[queue[q]] = 0;  // not taken
+      parts.push_back({begin, (int)order.size()});
+    }
+    ids = order;
+  } else {
+    bisect(m, ids, 0, N, (N + target - 1) / target, parts);
+  }
 
   // which elements hold every node (the ring lists may be incomplete)
   std::vector<int> holds(N, 0);

@@ -21,8 +21,10 @@
  *    ELEMENTS, the mesh entity velocity lives on; the reference allocated it
  *    by edges and the kernels then read it as (2, nl-1, elem) (:694-725).
  * Restart files (tracer_init, tracer_finalize, tracer_run_workflow,
- * tracer_load_mesh_partition) are not provided by this build: they return
- * -1 with a message.  Meshes come from tracer_init_analytic,
+ * tracer_load_mesh_partition) use the reference's derived-type binary
+ * format (lib/io_restart_derivedtype.F90:33-199) for one process:
+ * <dir>/np1/t_mesh.0, t_partit.0, t_tracer.0, t_dynamics.0 and
+ * <dir>/meta.time.  Meshes also come from tracer_init_analytic,
  * tracer_set_mesh_arrays or the ASCII mesh files
  * (tracer_load_mesh_from_files, one process, no partition files).
  */
@@ -40,7 +42,11 @@ extern "C" {
 int tracer_init_mpi(int mpi_comm);
 /* :89 tracer_finalize_mpi -- always 0. */
 int tracer_finalize_mpi(void);
-/* :113 tracer_init -- binary restarts are not supported: -1. */
+/* :113 tracer_init -- mesh, tracers (values, valuesAB, schemes) and flow
+ * (uv, w) from the restart in restart_dir/np1; valuesAB is kept as read
+ * (not refreshed per step), as in the reference's drivers.  -1 with a
+ * message naming the file and field when a record does not parse, the
+ * partition is not one process's, or ulevels /= 1. */
 int tracer_init(const char *restart_dir);
 /* :163 tracer_advect_step -- one step of every tracer. */
 int tracer_advect_step(double dt);
@@ -50,9 +56,12 @@ int tracer_get_stats(double *tmin, double *tmax, double *tsum);
 int tracer_get_size(int *nz, int *nn);
 /* :280 tracer_get_values -- tracer 1 into values(nz, nn). */
 int tracer_get_values(double *values, int nz, int nn);
-/* :308 tracer_finalize -- restart output is not supported: -1. */
+/* :308 tracer_finalize -- writes the restart of the current state into
+ * output_dir/np1 and output_dir/meta.time; the state is then no longer
+ * initialised (as in the reference). */
 int tracer_finalize(const char *output_dir);
-/* :356 tracer_run_workflow -- needs restart input: -1. */
+/* :356 tracer_run_workflow -- tracer_init, nsteps steps each followed by
+ * tracer_get_stats (printed), tracer_finalize into the same directory. */
 int tracer_run_workflow(const char *restart_dir, int nsteps, double dt);
 /* :391 tracer_cleanup -- releases every host and device resource. */
 int tracer_cleanup(void);
@@ -74,7 +83,8 @@ int tracer_set_velocity_zero(int nl, int nod2D, int edge2D);
 int tracer_set_velocity(const double *uv, const double *w, int nl, int nod2D, int nelem);
 /* :749 tracer_init_complete */
 int tracer_init_complete(void);
-/* :769 tracer_load_mesh_partition -- binary restarts are not supported: -1. */
+/* :769 tracer_load_mesh_partition -- mesh and flow from a restart directory
+ * (its tracer record, when present, supplies only the MUSCL tables). */
 int tracer_load_mesh_partition(const char *restart_dir);
 /* :830 tracer_load_mesh_from_files -- reads the mesh directory's nod2d.out,
  * elem2d.out, aux3d.out, edgenum.out, edges.out, edge_tri.out, elvls.out and
