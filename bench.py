@@ -48,8 +48,9 @@ sys.path.insert(0, str(ROOT))
 
 # 14 words per wet cell and tracer at storage precision: 3 tracer words
 # (T read, T_AB read, T write) + 11 geometry / flow words
-BYTES_PER_CELL = {"fp64": 112, "fp32": 56, "bf16": 3 * 2 + 11 * 4, "fp16": 3 * 2 + 11 * 4}
-DTYPE = {"fp64": "f64", "fp32": "f32", "bf16": "bf16 storage / f32 compute", "fp16": "f16 storage / f32 compute"}
+BYTES_PER_CELL = {"fp64": 112, "fp64fma": 112, "fp32": 56, "bf16": 3 * 2 + 11 * 4, "fp16": 3 * 2 + 11 * 4}
+DTYPE = {"fp64": "f64", "fp64fma": "f64 (FMA-contracted kernels)", "fp32": "f32",
+         "bf16": "bf16 storage / f32 compute", "fp16": "f16 storage / f32 compute"}
 L2_BYTES = 126 * 2**20
 
 
@@ -63,7 +64,9 @@ def parse():
     p.add_argument("--nl", type=int, default=64)
     p.add_argument("--e2e-steps", type=int, default=5)
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--precision", default="fp64", choices=["fp64", "fp32", "bf16", "fp16"])
+    p.add_argument("--precision", default="fp64", choices=["fp64", "fp64fma", "fp32", "bf16", "fp16"])
+    p.add_argument("--step-path", default="fused", choices=["fused", "five"],
+                   help="fused patch kernel (default) or the five-kernel path")
     p.add_argument("--learned", action="store_true",
                    help="FP32 with the learned antidiffusive flux (shipped parameters) ahead of FCT")
     a = p.parse_args()
@@ -242,6 +245,7 @@ def run_ours(args):
         raise RuntimeError(api.lib.tracer_last_error().decode())
     K, uv, w, T, S, dt, cells = make_inputs(api, args.nx, args.nl)
     api.set_precision(args.precision)
+    api.set_step_path(args.step_path)
     api.allocate_tracers(2)
     api.set_values(1, T)
     api.set_values(2, S)

@@ -28,6 +28,7 @@
 #include "advect_ops.cuh"
 
 namespace fesom {
+FESOM_VARIANT_BEGIN
 
 constexpr int NTMAX = 4;
 constexpr int kThreads = 256;
@@ -902,4 +903,5 @@ constexpr size_t smem_col_staged(int nt, int arrays) {
   return smem_col<R>(nt, arrays) + smem_stage();
 }
 
+FESOM_VARIANT_END
 }  // namespace fesom

@@ -15,7 +15,23 @@
 
 #include "dmesh.hpp"
 
+// The FP64 kernels are compiled twice: without FMA contraction (bit-identical
+// to the reference's arithmetic) and, in a translation unit that defines
+// FESOM_KERNEL_VARIANT, with it (step_f64fma.cu).  The variant's kernels and
+// their launch templates live in an inline namespace of that name, so the two
+// builds of the same templates do not collide at link time.
+#ifndef FESOM_VARIANT_BEGIN
+#ifdef FESOM_KERNEL_VARIANT
+#define FESOM_VARIANT_BEGIN inline namespace FESOM_KERNEL_VARIANT {
+#define FESOM_VARIANT_END }
+#else
+#define FESOM_VARIANT_BEGIN
+#define FESOM_VARIANT_END
+#endif
+#endif
+
 namespace fesom {
+FESOM_VARIANT_BEGIN
 
 // Fortran MAX/MIN as evaluated by the oracle: the first argument wins ties.
 template <typename R> __device__ __forceinline__ R fmax2(R a, R b) { return (b > a) ? b : a; }
@@ -207,4 +223,5 @@ __device__ __forceinline__ R ver_cdiff(const Col<R, TS> &c, int i, R v) {
   return -(tv * c.W[i - 1] * c.A[i - 1]) - v;
 }
 
+FESOM_VARIANT_END
 }  // namespace fesom

@@ -41,6 +41,7 @@ struct State {
   Precision prec = Precision::FP64;
   int sround = 0;  // rounding of 16-bit stores (tracer_set_rounding)
   int step_path = 0;  // tracer_set_step_path
+  bool fma64 = false;  // precision mode 4: FP64 with FMA-contracted kernels
   int patch_size = 0;  // tracer_set_patch_size (0: the default)
   std::vector<int> ids;  // tracer IDs read from a restart
 };
@@ -73,6 +74,7 @@ void ensure_engine() {
   g.eng.reset(new Engine(*g.mesh, g.prec));
   g.eng->set_rounding(g.sround);
   g.eng->set_step_path(g.step_path);
+  g.eng->set_fma64(g.fma64);
   if (g.patch_size > 0) g.eng->set_patch_size(g.patch_size);
   if (g.ntr > 0) {
     g.eng->allocate_tracers(g.ntr);
@@ -505,8 +507,11 @@ int tracer_set_scheme(int tracer_id, const char *hor, const char *ver, const cha
 }
 
 int tracer_set_precision(int mode) {
-  if (mode < 0 || mode > 3) return fail("precision mode must be 0 (FP64), 1 (FP32), 2 (BF16 storage) or 3 (FP16 storage)");
-  const Precision p = (Precision)mode;
+  if (mode < 0 || mode > 4)
+    return fail("precision mode must be 0 (FP64), 1 (FP32), 2 (BF16 storage), 3 (FP16 storage) or 4 (FP64 with FMA)");
+  const Precision p = mode == 4 ? Precision::FP64 : (Precision)mode;
+  g.fma64 = mode == 4;
+  if (g.eng && g.eng->precision() == p) g.eng->set_fma64(g.fma64);
   if (g.eng && g.eng->precision() != p) {
     // rebuild the device state in the new mode, keeping the tracer values
     std::vector<std::vector<double>> keep(g.ntr);

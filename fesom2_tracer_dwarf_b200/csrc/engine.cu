@@ -293,6 +293,8 @@ int Engine::level_stride() const { return p_->S; }
 Precision Engine::precision() const { return p_->prec; }
 void *Engine::stream() const { return (void *)p_->stream; }
 int Engine::device() const { return p_->device; }
+void Engine::set_fma64(bool on) { p_->fma64 = on; }
+bool Engine::fma64() const { return p_->fma64; }
 void Engine::synchronize() const { CK(cudaStreamSynchronize(p_->stream)); }
 size_t Engine::device_bytes() const { return p_->bytes; }
 int Engine::num_tracers() const { return (int)p_->tr.size(); }
@@ -462,7 +464,7 @@ bool fused_step(const EngineImpl &P, const TracerScheme &sc, bool learned) {
 
 static void dispatch(EngineImpl &P, const TracerScheme &sc, int nt, const BatchPtrs &b, double dt) {
   if (P.mesh.nod2D <= 0) return;
-  if (P.prec == Precision::FP64) launch_batch_f64(P, sc, nt, b, dt);
+  if (P.prec == Precision::FP64) (P.fma64 ? launch_batch_f64fma : launch_batch_f64)(P, sc, nt, b, dt);
   else launch_batch_f32(P, sc, nt, b, dt);
   CK(cudaGetLastError());
 }
@@ -622,17 +624,10 @@ void Engine::volume_sum(int id, double out[2]) const {
 }
 
 void Engine::stats(int id, double out[4]) const {
-  const int L = p_->mesh.nl - 1, N = p_->mesh.nod2D;
-  std::vector<double> v((size_t)L * N);
-  get_values(id, v.data());
-  double mn = v.empty() ? 0.0 : v[0], mx = mn, sm = 0.0, nan = 0.0;
-  for (double x : v) {
-    if (x < mn) mn = x;
-    if (x > mx) mx = x;
-    sm += x;
-    if (x != x) nan += 1.0;
-  }
-  out[0] = mn; out[1] = mx; out[2] = sm; out[3] = nan;
+  EngineImpl &P = *p_;
+  check_id(P, id);
+  CK(cudaStreamSynchronize(P.stream));
+  tracer_stats(P, P.tr[id].T, P.tr[id].off, out);
 }
 
 }  // namespace fesom

@@ -105,6 +105,10 @@ class Engine {
   void *stream() const;
   // CUDA device the engine was created on (current device at construction)
   int device() const;
+  // FP64 engines: true runs the kernels built with FMA contraction (about
+  // 1e-13 relative to the bit-exact ones, fewer FP64 instructions)
+  void set_fma64(bool on);
+  bool fma64() const;
   // Step kernels: 0 = the fused patch kernel wherever the scheme allows it
   // (FP64 or FP32 storage, PPM or UPW1 vertical, no learned flux), else the
   // five-kernel path; 1 = always the five-kernel path.  Both give the same

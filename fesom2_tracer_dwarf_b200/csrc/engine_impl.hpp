@@ -52,6 +52,7 @@ struct EngineImpl {
   int cells_per_block = 512;   // schedule tile
   int S = 0;
   Precision prec = Precision::FP64;
+  bool fma64 = false;    // FP64 mode with FMA-contracted kernels (step_f64fma.cu)
   size_t ts_bytes = 8;  // tracer storage element
   size_t r_bytes = 8;   // compute / geometry / work element
   cudaStream_t stream = nullptr;
@@ -73,6 +74,7 @@ struct EngineImpl {
   // (nl-1, nod2D) FP64 layout, and a ring of pinned host slots
   static constexpr int kRing = 4;
   double *stage_d = nullptr;
+  double *stats_d = nullptr;  // per-block partial statistics (tracer_stats)
   void *ring[kRing] = {};
   cudaEvent_t ring_ev[kRing] = {};
   std::vector<Tracer> tr;
@@ -159,6 +161,8 @@ enum { KK_EDGE = 0, KK_COL1, KK_COL2, KK_COL3, KK_GRAD, KK_TILE, KK_VFLUX, KK_CO
 // Launch one batch of nt tracers (kernels in step_f64.cu / step_f32.cu).
 void launch_batch_f64(EngineImpl &P, const TracerScheme &sc, int nt, const BatchPtrs &b, double dt);
 void launch_batch_f32(EngineImpl &P, const TracerScheme &sc, int nt, const BatchPtrs &b, double dt);
+// The FP64 kernels built with FMA contraction (step_f64fma.cu).
+void launch_batch_f64fma(EngineImpl &P, const TracerScheme &sc, int nt, const BatchPtrs &b, double dt);
 // Whether the fused patch kernel runs a batch of this scheme (precision,
 // storage type, vertical scheme, learned flux and plan permitting).
 bool fused_step(const EngineImpl &P, const TracerScheme &sc, bool learned);
@@ -181,6 +185,9 @@ double stage_wet_mean(EngineImpl &P);
 void stage_pack(EngineImpl &P, double off, void *d0, void *d1, void *d2);
 void stage_unpack(EngineImpl &P, const void *s, double off);
 void storage_reoffset(EngineImpl &P, void *s, double off_old, double off_new);
+// min, max, sum and NaN count of a tracer over the (nl-1, nod2D) values the
+// host reads back, reduced on the device (transfer.cu)
+void tracer_stats(EngineImpl &P, const void *s, double off, double out[4]);
 void release_ring(EngineImpl &P);
 
 // Learned flux (mlp.cu): after the edge kernel wrote features and scales,

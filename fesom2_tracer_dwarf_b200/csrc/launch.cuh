@@ -4,11 +4,13 @@
 #include <mutex>
 #include <unordered_map>
 
-#include "advect_fused.cuh"
+// engine_impl.hpp first: its declarations name the non-variant FusedArgs
 #include "engine_impl.hpp"
+#include "advect_fused.cuh"
 #include "tile.cuh"
 
 namespace fesom {
+FESOM_VARIANT_BEGIN
 
 template <typename R>
 const DMeshT<R> &dmesh(const EngineImpl &P);
@@ -264,4 +266,5 @@ void volume_sum_t(EngineImpl &P, const void *T, double off, double res[2]) {
   res[1] = s1 + c1;
 }
 
+FESOM_VARIANT_END
 }  // namespace fesom

@@ -35,6 +35,7 @@
 #include "tile.hpp"
 
 namespace fesom {
+FESOM_VARIANT_BEGIN
 
 template <typename R>
 struct TileArgs {
@@ -596,4 +597,5 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_tile(DMeshT<R> m, TileArgs<
   cp_async_wait_all();
 }
 
+FESOM_VARIANT_END
 }  // namespace fesom

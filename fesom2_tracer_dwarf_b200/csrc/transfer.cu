@@ -215,6 +215,53 @@ __global__ void k_wet_sum(const double *__restrict__ src, const int *__restrict_
 
 constexpr int kGrid = 148 * 8, kBlock = 256;
 
+// Statistics of one tracer over the (nl-1, nod2D) values the host would read
+// back (wet cells T = storage + off, dry cells the storage itself): per block
+// the minimum and maximum of the non-NaN values, the NaN count and a
+// Neumaier-compensated sum, in a fixed assignment of cells to threads and a
+// fixed reduction order, so the result does not depend on scheduling.
+constexpr int kStatBlocks = 296, kStatThreads = 256;
+template <typename TS>
+__global__ void __launch_bounds__(kStatThreads) k_stats(const TS *__restrict__ s, const int *__restrict__ nlev,
+                                                        int L, int S, long long N, double off, double *out) {
+  double mn = INFINITY, mx = -INFINITY, nan = 0.0, sm = 0.0, c = 0.0;
+  const long long total = N * L;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+       i += (long long)gridDim.x * blockDim.x) {
+    const long long n = i / L;
+    const int k = (int)(i - n * L);
+    const double raw = from_ts<TS>(s[n * S + k]);
+    const double v = k < nlev[n] - 1 ? raw + off : raw;
+    if (v != v) {
+      nan += 1.0;
+      continue;
+    }
+    mn = fmin(mn, v);
+    mx = fmax(mx, v);
+    double t, e;
+    two_sum_d(sm, v, t, e);
+    sm = t;
+    c += e;
+  }
+  __shared__ double sh[5][kStatThreads];
+  const int tid = threadIdx.x;
+  sh[0][tid] = mn; sh[1][tid] = mx; sh[2][tid] = nan; sh[3][tid] = sm; sh[4][tid] = c;
+  __syncthreads();
+  for (int w = kStatThreads / 2; w > 0; w >>= 1) {
+    if (tid < w) {
+      sh[0][tid] = fmin(sh[0][tid], sh[0][tid + w]);
+      sh[1][tid] = fmax(sh[1][tid], sh[1][tid + w]);
+      sh[2][tid] += sh[2][tid + w];
+      double t, e;
+      two_sum_d(sh[3][tid], sh[3][tid + w], t, e);
+      sh[3][tid] = t;
+      sh[4][tid] += sh[4][tid + w] + e;
+    }
+    __syncthreads();
+  }
+  if (tid < 5) out[5 * blockIdx.x + tid] = sh[tid][0];
+}
+
 template <typename TS>
 void pack_t(EngineImpl &P, double off, void *d0, void *d1, void *d2) {
   k_pack<TS><<<kGrid, kBlock, 0, P.stream>>>(P.stage_d, nlev_dev(P), P.mesh.nl - 1, P.S, P.mesh.nod2D, off,
@@ -318,6 +365,60 @@ void stage_unpack(EngineImpl &P, const void *s, double off) {
     case Precision::BF16: unpack_t<__nv_bfloat16>(P, s, off); break;
     case Precision::FP16: unpack_t<__half>(P, s, off); break;
   }
+}
+
+void tracer_stats(EngineImpl &P, const void *s, double off, double out[4]) {
+  if (!P.stats_d) P.stats_d = P.dalloc<double>(5 * kStatBlocks + 1);
+  const int L = P.mesh.nl - 1;
+  const long long N = P.mesh.nod2D;
+  switch (P.prec) {
+    case Precision::FP32:
+      k_stats<float><<<kStatBlocks, kStatThreads, 0, P.stream>>>((const float *)s, nlev_dev(P), L, P.S, N, off, P.stats_d);
+      break;
+    case Precision::BF16:
+      k_stats<__nv_bfloat16><<<kStatBlocks, kStatThreads, 0, P.stream>>>((const __nv_bfloat16 *)s, nlev_dev(P), L, P.S,
+                                                                        N, off, P.stats_d);
+      break;
+    case Precision::FP16:
+      k_stats<__half><<<kStatBlocks, kStatThreads, 0, P.stream>>>((const __half *)s, nlev_dev(P), L, P.S, N, off,
+                                                                 P.stats_d);
+      break;
+    default:
+      k_stats<double><<<kStatBlocks, kStatThreads, 0, P.stream>>>((const double *)s, nlev_dev(P), L, P.S, N, off,
+                                                                 P.stats_d);
+      break;
+  }
+  CK(cudaGetLastError());
+  // the first cell as the host reads it: a NaN there makes min and max NaN,
+  // like a host loop seeded with the first value
+  std::vector<double> h(5 * kStatBlocks);
+  P.d2h(h.data(), P.stats_d, h.size() * sizeof(double));
+  double first = 0.0;
+  if (L > 0 && N > 0) {
+    double raw = 0.0;
+    switch (P.prec) {
+      case Precision::FP32: { float f; P.d2h(&f, s, 4); raw = f; break; }
+      case Precision::BF16: { __nv_bfloat16 b; P.d2h(&b, s, 2); raw = (double)__bfloat162float(b); break; }
+      case Precision::FP16: { __half b; P.d2h(&b, s, 2); raw = (double)__half2float(b); break; }
+      default: P.d2h(&raw, s, 8); break;
+    }
+    first = (P.mesh.nlev_node[0] - 1 > 0) ? raw + off : raw;
+  }
+  double mn = INFINITY, mx = -INFINITY, nan = 0.0, sm = 0.0, c = 0.0;
+  for (int b = 0; b < kStatBlocks; b++) {
+    mn = std::fmin(mn, h[5 * b]);
+    mx = std::fmax(mx, h[5 * b + 1]);
+    nan += h[5 * b + 2];
+    const double x = h[5 * b + 3], t = sm + x;
+    c += (std::fabs(sm) >= std::fabs(x)) ? (sm - t) + x : (x - t) + sm;
+    sm = t;
+    c += h[5 * b + 4];
+  }
+  if (first != first || (L > 0 && N > 0 && nan == (double)L * N)) mn = mx = first;
+  out[0] = (L > 0 && N > 0) ? mn : 0.0;
+  out[1] = (L > 0 && N > 0) ? mx : 0.0;
+  out[2] = sm + c;
+  out[3] = nan;
 }
 
 void storage_reoffset(EngineImpl &P, void *s, double off_old, double off_new) {

@@ -131,7 +131,7 @@ class FESOMTracerAdvection:
         rc = self.lib.tracer_set_velocity_elem(_lib.ptr(u), _lib.ptr(ww), d["nl"], d["nod2D"], d["elem2D"])
         _lib.check(self.lib, rc, "tracer_set_velocity_elem")
 
-    PRECISIONS = {"fp64": 0, "fp32": 1, "bf16": 2, "fp16": 3}
+    PRECISIONS = {"fp64": 0, "fp32": 1, "bf16": 2, "fp16": 3, "fp64fma": 4}
 
     def set_precision(self, mode):
         """'fp64' (bit-exact), 'fp32', 'bf16' or 'fp16' (16-bit tracer storage, FP32 arithmetic)."""

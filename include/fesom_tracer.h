@@ -155,9 +155,11 @@ int tracer_set_values_ab(int tracer_id, const double *values, int nl, int nod2D)
 int tracer_set_ab_refresh(int on);
 /* Arithmetic mode of the device state: 0 FP64 (default, bit-identical to the
  * reference algorithm), 1 FP32, 2 BF16 tracer storage with FP32 arithmetic, 3
- * FP16 tracer storage with FP32 arithmetic; in modes 1-3 the FCT ratio
- * denominators are formed in FP64.  Changing it rebuilds the device state and
- * keeps the tracer values. */
+ * FP16 tracer storage with FP32 arithmetic, 4 FP64 with the kernels built
+ * with FMA contraction (each a*b+c the compiler fuses rounds once: results
+ * within about 1e-13 relative of mode 0, fewer FP64 instructions); in modes
+ * 1-3 the FCT ratio denominators are formed in FP64.  Changing it rebuilds
+ * the device state and keeps the tracer values. */
 int tracer_set_precision(int mode);
 /* Rounding of new tracer values into 16-bit storage (modes 2, 3):
  * 0 = to nearest (default), 1 = stochastic (round up with probability equal

@@ -1,0 +1,50 @@
+"""tracer_get_stats / tracer_get_stats_id reduce on the device: min and max
+bit-identical to the host's view of the field (nl-1 x nod2D, dry cells
+included), the NaN count exact, the sum within a few ulps of an exact sum
+(compensated, in a fixed order: the same bits on every call)."""
+import math
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _case(api, prec="fp64"):
+    from fesom2_tracer_dwarf_b200 import synth_bathymetry
+    K = synth_bathymetry(api.lib.tracer_analytic_nodes(40, 33, 1), 17, 9)
+    api.init_analytic(40, 33, 17, periodic=True, full_rings=True, node_K=K)
+    api.set_precision(prec)
+    T = api.synth_tracer(seed=2, kind=0)
+    api.allocate_tracers(2)
+    api.set_values(1, T)
+    api.set_values(2, api.synth_tracer(seed=3, kind=1))
+    return T
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32", "bf16"])
+def test_device_stats_match_the_host_view(api, prec):
+    _case(api, prec)
+    for t in (1, 2):
+        v = api.get_tracer_values(t)
+        st = api.get_statistics(t)
+        assert st["min"] == v.min() and st["max"] == v.max() and st["nan"] == 0
+        exact = math.fsum(v.ravel())
+        assert abs(st["sum"] - exact) <= 4 * np.spacing(abs(exact))
+        assert api.get_statistics(t) == st  # deterministic
+
+
+def test_device_stats_count_nans(api):
+    T = _case(api)
+    T = T.copy(order="F")
+    T[3, 7] = np.nan
+    T[0, 100] = np.nan
+    api.set_values(1, T)
+    st = api.get_statistics(1)
+    assert st["nan"] == 2
+    ok = T[~np.isnan(T)]
+    assert st["min"] == ok.min() and st["max"] == ok.max()
+    T[0, 0] = np.nan  # the host loop seeds min and max with the first value
+    api.set_values(1, T)
+    st = api.get_statistics(1)
+    assert st["nan"] == 3 and math.isnan(st["min"]) and math.isnan(st["max"])
