@@ -69,6 +69,11 @@ def parse():
                    help="fused patch kernel (default) or the five-kernel path")
     p.add_argument("--learned", action="store_true",
                    help="FP32 with the learned antidiffusive flux (shipped parameters) ahead of FCT")
+    p.add_argument("--config", default="c2", choices=["c2", "c3", "c4", "dd"],
+                   help="c2: the plain method at scale (default); c3: 48 tracers x 8 uneven members, one "
+                        "persistent launch per step; c4: BF16/FP16/FP32 storage against FP64 at 2000x2000x48; "
+                        "dd: the 1000x1000x64 step cut into strips on one GPU")
+    p.add_argument("--parts", type=int, nargs="+", default=[2, 4, 8], help="dd: strip counts")
     a = p.parse_args()
     if a.learned:
         a.precision = "fp32"
@@ -364,10 +369,159 @@ def run_ours(args):
     return 0
 
 
+# ---------------------------------------------------------------------------
+# further configurations (one GPU; each prints one JSON line with the clocks
+# sampled while it was timed)
+# ---------------------------------------------------------------------------
+def timed(gpu, fn):
+    """Runs fn() with the clock sampler on; returns (fn's result, clocks)."""
+    clock = ClockSampler(gpu)
+    clock.start()
+    try:
+        out = fn()
+    finally:
+        clocks = clock.stop()
+    return out, clocks
+
+
+def run_c3(args):
+    """48 tracers x 8 ensemble members on seeded analytic meshes of uneven
+    size (nx = ny in [100, 800], nl in [20, 80], periodic and closed mixed),
+    FP32 MUSCL+PPM+FCT: the persistent one-launch step (autotuned tile,
+    replayed from a CUDA graph) against the per-member separate launches."""
+    from fesom2_tracer_dwarf_b200 import FESOMTracerAdvection
+    from fesom2_tracer_dwarf_b200.batch import TracerBatch
+    from fesom2_tracer_dwarf_b200.workloads import build_ensemble, ensemble_specs
+    specs = ensemble_specs(8, 0, (100, 800), (20, 80))
+    api = FESOMTracerAdvection()
+    batch = TracerBatch()
+    dts = build_ensemble(batch, api, specs, 48)
+    batch.configure(dts, "MUSCL", "PPM", "FCT")
+    info = batch.info()
+    batch.autotune(2)
+    tile = batch.tile()
+    batch.steps(max(args.warmup, 3), graph=True)
+    steps = max(args.steps, 1)
+    ms_graph, clocks = timed(0, lambda: batch.time_steps(steps, graph=True) / steps)
+    ms_plain = batch.time_steps(steps, graph=False) / steps
+    ms_sep = batch.time_separate(steps) / steps
+    ms_sep_graph = batch.time_separate(steps, graph=True) / steps
+    cells = info["cell_tracers"]
+    batch.close()
+    api.cleanup()
+    line = {"metric": "tracer cell-updates/s", "value": cells / (ms_graph / 1e3), "unit": "cell-updates/s",
+            "n_gpus": 1, "steps": steps, "warmup": args.warmup, "ms_per_step": ms_graph, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "48 tracers x 8 members, nx=ny in [100,800], nl in [20,80], periodic/closed "
+                                   "mixed, seeds 0..7, MUSCL+PPM+FCT, one persistent launch per step in a CUDA graph",
+                       "members": specs, "cell_tracers": cells, "tile": tile},
+            "paths_ms_per_step": {"persistent_graph": ms_graph, "persistent_no_graph": ms_plain,
+                                  "separate_launches": ms_sep, "separate_launches_graph": ms_sep_graph},
+            "clocks": clocks}
+    print(json.dumps(line))
+    return 0
+
+
+def run_c4(args):
+    """2000x2000x48 (or --nx/--nl), 200 steps by default: every storage mode
+    against the bit-exact FP64 path on identical seeded inputs -- time per
+    step (clocks sampled per mode), relative L2 and max-abs error over wet
+    cells, content drift."""
+    from fesom2_tracer_dwarf_b200 import FESOMTracerAdvection
+    from fesom2_tracer_dwarf_b200.precision import compare, run_mode
+    from fesom2_tracer_dwarf_b200.workloads import layered_flow_case
+    nx = args.nx if args.nx != 1000 else 2000
+    nl = args.nl if args.nl != 64 else 48
+    steps = args.steps if args.steps != 100 else 200
+    api = FESOMTracerAdvection()
+    api.cleanup()
+    api.lib.tracer_set_device(0)
+    c = layered_flow_case(api, nx, nl, seed=0)
+    ref, clk = timed(0, lambda: run_mode(api, c, "fp64", steps))
+    modes = {"fp64": {"ms_per_step": ref["ms_per_step"], "clocks": clk,
+                      "cell_updates_per_s": 2 * c.wet_cells / (ref["ms_per_step"] / 1e3)}}
+    for m in ("fp64fma", "fp32", "bf16", "bf16+sr", "fp16", "fp16+sr"):
+        res, clk = timed(0, lambda: run_mode(api, c, m, steps))
+        modes[m] = {"ms_per_step": res["ms_per_step"], "clocks": clk,
+                    "cell_updates_per_s": 2 * c.wet_cells / (res["ms_per_step"] / 1e3),
+                    "errors": compare(ref, res)}
+    api.cleanup()
+    best = modes["bf16+sr"]
+    line = {"metric": "tracer cell-updates/s", "value": best["cell_updates_per_s"], "unit": "cell-updates/s",
+            "n_gpus": 1, "steps": steps, "warmup": 0, "ms_per_step": best["ms_per_step"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "bf16 storage / f32 compute (value); every mode listed",
+            "data": "synthetic",
+            "config": {"workload": f"periodic {nx}x{nx}x{nl}, smooth bathymetry, layered flow CFL 0.5, "
+                                   "MUSCL+PPM+FCT, 2 tracers", "wet_cells": c.wet_cells, "steps": steps},
+            "modes": modes, "clocks": best["clocks"]}
+    print(json.dumps(line))
+    return 0
+
+
+def run_dd(args):
+    """The 1000x1000x64 FP64 step cut into P index strips, every part on
+    this GPU with the halo exchange after each step, against the whole mesh:
+    redundant halo work, halo bytes per step, time per step of all parts."""
+    from fesom2_tracer_dwarf_b200 import FESOMTracerAdvection
+    from fesom2_tracer_dwarf_b200.decomp import DomainDecomposition, partition_by_index
+    from fesom2_tracer_dwarf_b200.workloads import layered_flow_case
+    api = FESOMTracerAdvection()
+    api.cleanup()
+    c = layered_flow_case(api, args.nx, args.nl)
+    N = api.mesh_dims()["nod2D"]
+    api.allocate_tracers(2)
+    api.set_values(1, c.T)
+    api.set_values(2, c.S)
+    for t in (1, 2):
+        api.set_scheme(t, "MUSCL", "PPM", "FCT")
+    api.set_velocity(c.uv, c.w)
+    api.set_ab_refresh(True)
+    api.advect_steps(max(args.warmup, 3), c.dt)
+    steps = max(args.steps, 1)
+    whole, clocks = timed(0, lambda: api.time_steps(steps, c.dt) / steps)
+    parts = []
+    for P in args.parts:
+        dd = DomainDecomposition(api, partition_by_index(N, P), P)
+        dd.allocate_tracers(2)
+        for t in (1, 2):
+            dd.set_scheme(t, "MUSCL", "PPM", "FCT")
+        dd.set_velocity(c.uv, c.w)
+        dd.set_values(1, c.T)
+        dd.set_values(2, c.S)
+        halo = sum(dd.transfer_nodes(i, p, False) for i in range(P) for p in range(P) if p != i)
+        local = sum(dd.part_info(i)["nodes"] for i in range(P))
+        dd.steps(3, c.dt)
+        t0 = time.perf_counter()
+        dd.steps(steps, c.dt, exchange=True)
+        t1 = time.perf_counter()
+        dd.steps(steps, c.dt, exchange=False)
+        t2 = time.perf_counter()
+        dd.destroy()
+        parts.append({"parts": P, "local_over_owned_nodes": local / N,
+                      "halo_bytes_per_step": halo * (args.nl - 1) * 2 * 8,
+                      "ms_per_step_all_parts": (t1 - t0) * 1e3 / steps,
+                      "ms_per_step_all_parts_no_exchange": (t2 - t1) * 1e3 / steps})
+    api.cleanup()
+    line = {"metric": "tracer cell-updates/s", "value": 2 * c.wet_cells / (whole / 1e3), "unit": "cell-updates/s",
+            "n_gpus": 1, "steps": steps, "warmup": args.warmup, "ms_per_step": whole, "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": workload_name(args.nx, args.nl) + ", whole mesh (value) and P strips on one GPU "
+                                                                     "(host-timed, exchange included)"},
+            "parts": parts, "clocks": clocks}
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.config == "c3":
+        return run_c3(args)
+    if args.config == "c4":
+        return run_c4(args)
+    if args.config == "dd":
+        return run_dd(args)
     return run_ours(args)
 
 

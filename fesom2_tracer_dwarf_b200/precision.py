@@ -1,25 +1,18 @@
-"""Precision study: FP32, BF16-storage and FP16-storage runs of the tracer
-step (16-bit stores rounded to nearest or stochastically) against the FP64
-path on identical seeded inputs.
+"""Error of a reduced-precision mode against the FP64 path: FP32,
+BF16-storage and FP16-storage runs of the tracer step (16-bit stores rounded
+to nearest or stochastically) on identical seeded inputs.
 
 The FP64 path is bit-identical to the CPU oracle (tests/test_gpu_parity.py
 checks it at every size up to 1000x1000x64), so it serves as the FP64
 reference at sizes where a CPU run would take hours.  Reported per mode and
 tracer: relative L2 and max-abs error of the final field over wet cells, the
 drift of the conserved content Sum(T*areasvol*hnode_new) (compensated FP64
-sum on the device), and device time per step.
-
-    python -m fesom2_tracer_dwarf_b200.precision_study --nx 2000 --nl 48 --steps 200
+sum on the device), and device time per step.  bench.py --config c4 runs the
+2000x2000x48 configuration through these functions.
 """
 from __future__ import annotations
 
-import argparse
-import json
-
 import numpy as np
-
-from .tracer import FESOMTracerAdvection
-from .workloads import layered_flow_case
 
 
 def run_mode(api, c, mode, steps, hor="MUSCL", ver="PPM", lim="FCT"):
@@ -60,34 +53,3 @@ def compare(ref, res):
             "content_drift_rel_fp64": float((ref["v1"][t] - ref["v0"][t]) / ref["v0"][t]),
         })
     return rows
-
-
-def study(nx, nl, steps, modes=("fp32", "bf16", "bf16+sr", "fp16", "fp16+sr"), seed=0):
-    api = FESOMTracerAdvection()
-    api.cleanup()
-    c = layered_flow_case(api, nx, nl, seed=seed)
-    ref = run_mode(api, c, "fp64", steps)
-    out = {"config": {"nx": nx, "nl": nl, "steps": steps, "wet_cells": ref["cells"], "seed": seed,
-                      "dt_s": ref["dt"]},
-           "fp64_ms_per_step": ref["ms_per_step"], "modes": {}}
-    for m in modes:
-        res = run_mode(api, c, m, steps)
-        out["modes"][m] = {"ms_per_step": res["ms_per_step"], "storage_offsets": res["offsets"],
-                           "cell_updates_per_s": 2 * res["cells"] / (res["ms_per_step"] / 1e3),
-                           "errors": compare(ref, res)}
-    out["fp64_cell_updates_per_s"] = 2 * ref["cells"] / (ref["ms_per_step"] / 1e3)
-    api.cleanup()
-    return out
-
-
-def main():
-    p = argparse.ArgumentParser()
-    p.add_argument("--nx", type=int, default=2000)
-    p.add_argument("--nl", type=int, default=48)
-    p.add_argument("--steps", type=int, default=200)
-    a = p.parse_args()
-    print(json.dumps(study(a.nx, a.nl, a.steps), indent=1))
-
-
-if __name__ == "__main__":
-    main()

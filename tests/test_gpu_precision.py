@@ -81,8 +81,19 @@ def test_stochastic_rounding_is_reproducible(api, mode):
 
 @pytest.fixture(scope="module")
 def study():
-    from fesom2_tracer_dwarf_b200.precision_study import study as run
-    return run(160, 24, 40)
+    """Every mode against the FP64 path on the 160x160x24 case, 40 steps."""
+    from fesom2_tracer_dwarf_b200 import FESOMTracerAdvection
+    from fesom2_tracer_dwarf_b200.precision import compare, run_mode
+    from fesom2_tracer_dwarf_b200.workloads import layered_flow_case
+    api = FESOMTracerAdvection()
+    api.cleanup()
+    c = layered_flow_case(api, 160, 24)
+    ref = run_mode(api, c, "fp64", 40)
+    out = {"modes": {}}
+    for m in ("fp32", "bf16", "bf16+sr", "fp16", "fp16+sr"):
+        out["modes"][m] = {"errors": compare(ref, run_mode(api, c, m, 40))}
+    api.cleanup()
+    return out
 
 
 def test_fp32_error(study):
