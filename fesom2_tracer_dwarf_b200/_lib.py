@@ -62,6 +62,8 @@ SIGNATURES = {
     "tracer_set_step_path": (ctypes.c_int, [ctypes.c_int]),
     "tracer_step_info": (ctypes.c_int, [_vp]),
     "tracer_set_patch_size": (ctypes.c_int, [ctypes.c_int]),
+    "tracer_set_nan_check": (ctypes.c_int, [ctypes.c_int]),
+    "tracer_step_status": (ctypes.c_int, [_vp]),
     "tracer_tile_plan_check": (ctypes.c_int, [ctypes.c_int, _vp]),
     "tracer_host_register": (ctypes.c_int, [_vp, ctypes.c_longlong]),
     "tracer_host_unregister": (ctypes.c_int, [_vp]),

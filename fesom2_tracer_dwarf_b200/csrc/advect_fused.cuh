@@ -173,6 +173,8 @@ struct FusedArgs {
   // limiter needs them), 1 computed and stored, 2 loaded from vflux (stored
   // by an earlier launch with the same velocity)
   int vflux_mode;
+  // failure detection: count of non-finite new values (nullptr: not counted)
+  unsigned long long *nonfinite;
 };
 
 // ---------------------------------------------------------------------------
@@ -881,6 +883,7 @@ __device__ __forceinline__ void col3_block(const DMeshT<R> &m, const FusedArgs<R
       const R del = R(0) + dh[t] + dv[t];
       const R tnew = ldT(a.T[t], o, a.off[t]) + div_rcp(del, hn, yhn);
       a.T_out[t][o] = stT<R, TS>(tnew, a.off[t], a.sround != 0, a.sround ? mix32(a.seed[t] ^ mix32((uint32_t)o)) : 0u);
+      if (a.nonfinite && !isfinite(tnew)) atomicAdd(a.nonfinite, 1ull);
     }
   }
 }

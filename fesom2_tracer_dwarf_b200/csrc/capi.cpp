@@ -42,6 +42,7 @@ struct State {
   int sround = 0;  // rounding of 16-bit stores (tracer_set_rounding)
   int step_path = 0;  // tracer_set_step_path
   bool fma64 = false;  // precision mode 4: FP64 with FMA-contracted kernels
+  bool nan_check = false;  // tracer_set_nan_check
   int patch_size = 0;  // tracer_set_patch_size (0: the default)
   std::vector<int> ids;  // tracer IDs read from a restart
 };
@@ -580,6 +581,19 @@ int tracer_set_patch_size(int owned) {
   });
 }
 
+int tracer_set_nan_check(int on) {
+  g.nan_check = on != 0;
+  return 0;
+}
+
+int tracer_step_status(long long *nonfinite) {
+  return guarded([&] {
+    if (!nonfinite) return fail("null output");
+    *nonfinite = g.eng ? g.eng->nonfinite_values(true) : 0;
+    return 0;
+  });
+}
+
 int tracer_step_info(double *out4) {
   return guarded([&] {
     if (!out4) return fail("null output");
@@ -628,6 +642,10 @@ int tracer_advect_steps(int nsteps, double dt) {
     ensure_engine();
     for (int s = 0; s < nsteps; s++) g.eng->step(dt, g.ab_refresh);
     g.eng->synchronize();
+    if (g.nan_check) {
+      const long long bad = g.eng->nonfinite_values(true);
+      if (bad) return fail("tracer_advect_step: " + std::to_string(bad) + " non-finite new values");
+    }
     return 0;
   });
 }

@@ -261,6 +261,7 @@ Engine::Engine(const MeshHost &mesh, Precision prec) : p_(new EngineImpl) {
     build_rcp_f32(P);
   }
   build_tiles(P, edge_slot, kTileOwned);
+  P.nonfinite_d = P.dalloc<unsigned long long>(1);
   P.vel = P.dalloc_bytes((size_t)2 * M.elem2D * P.S * P.r_bytes);
   P.W = P.dalloc_bytes((size_t)M.nod2D * P.S * P.r_bytes);
   CK(cudaStreamSynchronize(P.stream));
@@ -294,6 +295,16 @@ Precision Engine::precision() const { return p_->prec; }
 void *Engine::stream() const { return (void *)p_->stream; }
 int Engine::device() const { return p_->device; }
 void Engine::set_fma64(bool on) { p_->fma64 = on; }
+long long Engine::nonfinite_values(bool reset) {
+  EngineImpl &P = *p_;
+  unsigned long long n = 0;
+  P.d2h(&n, P.nonfinite_d, sizeof(n));
+  if (reset && n) {
+    CK(cudaMemsetAsync(P.nonfinite_d, 0, sizeof(n), P.stream));
+    CK(cudaStreamSynchronize(P.stream));
+  }
+  return (long long)n;
+}
 bool Engine::fma64() const { return p_->fma64; }
 void Engine::synchronize() const { CK(cudaStreamSynchronize(p_->stream)); }
 size_t Engine::device_bytes() const { return p_->bytes; }

@@ -109,6 +109,9 @@ class Engine {
   // 1e-13 relative to the bit-exact ones, fewer FP64 instructions)
   void set_fma64(bool on);
   bool fma64() const;
+  // Non-finite new values the steps have written since the last reset
+  // (counted on the device by the update kernels); reset = true zeroes it.
+  long long nonfinite_values(bool reset);
   // Step kernels: 0 = the fused patch kernel wherever the scheme allows it
   // (FP64 or FP32 storage, PPM or UPW1 vertical, no learned flux), else the
   // five-kernel path; 1 = always the five-kernel path.  Both give the same

@@ -75,6 +75,7 @@ struct EngineImpl {
   static constexpr int kRing = 4;
   double *stage_d = nullptr;
   double *stats_d = nullptr;  // per-block partial statistics (tracer_stats)
+  unsigned long long *nonfinite_d = nullptr;  // non-finite new values written by the steps
   void *ring[kRing] = {};
   cudaEvent_t ring_ev[kRing] = {};
   std::vector<Tracer> tr;

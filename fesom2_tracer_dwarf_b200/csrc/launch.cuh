@@ -146,6 +146,7 @@ void run_tiles(EngineImpl &P, const TracerScheme &sc, int nt, const BatchPtrs &b
     a.ph = (R)sc.ph;
     a.hor = sc.hor;
     a.ver = sc.ver;
+    a.nonfinite = P.nonfinite_d;
     const bool ab = b.TAB[t] == b.T[t];
     const TileLayout L = tile_layout(P.tplan, (unsigned)sizeof(R), ab, sc.hor != 0, sc.lim == 1);
     P.mark_begin(KK_TILE);
@@ -189,6 +190,7 @@ void launch_batch_t(EngineImpl &P, const TracerScheme &sc, int nt, const BatchPt
   }
   a.sround = b.sround;
   a.vflux_mode = b.vflux_mode;
+  a.nonfinite = P.nonfinite_d;
   const bool fct = sc.lim == 1;
   if (nt == 4) fct ? run_group<R, TS, 4, LIM_FCT>(P, sc, a) : run_group<R, TS, 4, LIM_NONE>(P, sc, a);
   else if (nt == 2) fct ? run_group<R, TS, 2, LIM_FCT>(P, sc, a) : run_group<R, TS, 2, LIM_NONE>(P, sc, a);

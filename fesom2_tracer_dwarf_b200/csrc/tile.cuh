@@ -47,6 +47,7 @@ struct TileArgs {
   R dt, ph;
   int hor;         // HOR_UPW1 / HOR_MUSCL / HOR_MFCT
   int ver;         // VER_UPW1 / VER_PPM
+  unsigned long long *nonfinite;  // count of non-finite new values (nullptr: not counted)
 };
 
 // asynchronous global -> shared copies of one element (4 or 8 bytes)
@@ -589,7 +590,9 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_tile(DMeshT<R> m, TileArgs<
           dh = second ? dh - term : dh + term;
         }
         const R del = R(0) + dh + dv;
-        a.T_out[o] = T_m2 + div_rcp(del, hn, yhn);
+        const R tnew = T_m2 + div_rcp(del, hn, yhn);
+        a.T_out[o] = tnew;
+        if (a.nonfinite && !isfinite(tnew)) atomicAdd(a.nonfinite, 1ull);
       }
     }
     (void)AS_0; (void)YA_0; (void)YH_0; (void)HN_m1; (void)sl_0; (void)mn_m2;

@@ -184,6 +184,13 @@ int tracer_step_info(double *out4);
 /* Owned nodes per patch of the fused kernel's plan (0 = the default, 225);
  * every size gives the same results, small ones recompute more halo. */
 int tracer_set_patch_size(int owned);
+/* Failure detection (no counterpart in the reference): the update kernels
+ * count, on the device, every new tracer value that is not finite.
+ * tracer_step_status returns that count since its last call (and resets
+ * it); with tracer_set_nan_check(1), tracer_advect_step / _steps return -1
+ * with a message when the steps of the call produced any. */
+int tracer_set_nan_check(int on);
+int tracer_step_status(long long *nonfinite);
 /* Builds the fused kernel's patch plan for the loaded mesh on the host (no
  * device needed) with patches of about max_owned owned nodes, checks it
  * against the mesh (every node owned once, three halo rings, incidence lists

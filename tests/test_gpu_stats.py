@@ -48,3 +48,33 @@ def test_device_stats_count_nans(api):
     api.set_values(1, T)
     st = api.get_statistics(1)
     assert st["nan"] == 3 and math.isnan(st["min"]) and math.isnan(st["max"])
+
+
+@pytest.mark.parametrize("path", ["fused", "five"])
+def test_nonfinite_new_values_are_flagged_on_the_device(api, path):
+    """The update kernels count non-finite new values: none on a clean run;
+    a NaN planted in one wet cell spreads to its neighbours within a step
+    and is reported by tracer_step_status, and with the check on by
+    tracer_advect_step itself (-1 and a message)."""
+    import ctypes
+    from fesom2_tracer_dwarf_b200.workloads import layered_flow_case
+    c = layered_flow_case(api, 40, 12, seed=1)
+    api.set_step_path(path)
+    api.allocate_tracers(1)
+    api.set_values(1, c.T)
+    api.set_scheme(1, "MUSCL", "PPM", "FCT")
+    api.set_velocity(c.uv, c.w)
+    api.set_ab_refresh(True)
+    n = ctypes.c_longlong(-1)
+    api.advect_steps(2, c.dt)
+    assert api.lib.tracer_step_status(ctypes.byref(n)) == 0 and n.value == 0
+    T = c.T.copy(order="F")
+    T[2, 300] = np.nan
+    api.set_values(1, T)
+    api.advect_steps(1, c.dt)
+    assert api.lib.tracer_step_status(ctypes.byref(n)) == 0 and n.value >= 1
+    assert api.lib.tracer_step_status(ctypes.byref(n)) == 0 and n.value == 0  # reset by the read
+    assert api.lib.tracer_set_nan_check(1) == 0
+    assert api.lib.tracer_advect_step(c.dt) == -1
+    assert b"non-finite" in api.lib.tracer_last_error()
+    api.lib.tracer_set_nan_check(0)
