@@ -65,8 +65,8 @@ def parse():
     p.add_argument("--e2e-steps", type=int, default=5)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--precision", default="fp64", choices=["fp64", "fp64fma", "fp32", "bf16", "fp16"])
-    p.add_argument("--step-path", default="fused", choices=["fused", "five"],
-                   help="fused patch kernel (default) or the five-kernel path")
+    p.add_argument("--step-path", default="five", choices=["fused", "five"],
+                   help="the five-kernel path (default) or the fused patch kernel")
     p.add_argument("--learned", action="store_true",
                    help="FP32 with the learned antidiffusive flux (shipped parameters) ahead of FCT")
     p.add_argument("--config", default="c2", choices=["c2", "c3", "c4", "dd"],

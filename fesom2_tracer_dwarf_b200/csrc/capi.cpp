@@ -40,7 +40,7 @@ struct State {
   bool pend_vel = false;
   Precision prec = Precision::FP64;
   int sround = 0;  // rounding of 16-bit stores (tracer_set_rounding)
-  int step_path = 0;  // tracer_set_step_path
+  int step_path = 1;  // tracer_set_step_path (1: five kernels, the default)
   bool fma64 = false;  // precision mode 4: FP64 with FMA-contracted kernels
   bool nan_check = false;  // tracer_set_nan_check
   int patch_size = 0;  // tracer_set_patch_size (0: the default)

@@ -196,7 +196,7 @@ void build_tiles(EngineImpl &P, const std::vector<int> &edge_slot, int owned) {
   TilePlanHost &t = P.tplan;
   try {
     t = build_tile_plan(P.mesh, edge_slot, owned);
-  } catch (const std::runtime_error &) {
+  } catch (const std::exception &) {
     t = TilePlanHost();  // no plan: the five-kernel path runs every scheme
     return;
   }

@@ -114,8 +114,8 @@ class Engine {
   long long nonfinite_values(bool reset);
   // Step kernels: 0 = the fused patch kernel wherever the scheme allows it
   // (FP64 or FP32 storage, PPM or UPW1 vertical, no learned flux), else the
-  // five-kernel path; 1 = always the five-kernel path.  Both give the same
-  // bits.
+  // five-kernel path; 1 (default) = always the five-kernel path.  Both give
+  // the same bits in FP64.
   void set_step_path(int path);
   int step_path() const;
   bool fused(int id) const;      // whether tracer id's steps run the fused kernel

@@ -84,10 +84,10 @@ struct EngineImpl {
   bool vflux_valid = false;  // vflux holds the edge volume fluxes of the current velocity
   // fused patch kernel (tile.cuh): the plan's maxima (host lists released
   // after upload) and its device copy; step_path 0 runs it wherever the
-  // scheme allows, 1 always runs the five-kernel path
+  // scheme allows, 1 (the default, faster on B200) the five-kernel path
   TilePlanHost tplan;
   DTiles tiles{};
-  int step_path = 0;
+  int step_path = 1;
   void *adfh[kBatchMax] = {}, *adfv[kBatchMax] = {}, *lo[kBatchMax] = {}, *rp[kBatchMax] = {}, *rm[kBatchMax] = {};
   void *gradn[kBatchMax] = {};
 

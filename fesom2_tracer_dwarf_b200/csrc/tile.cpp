@@ -41,8 +41,12 @@ struct Region {
   int n0 = 0, n1 = 0, n2 = 0, n3 = 0;
 };
 
-// Owned nodes plus three rings over the edge graph, each ring ascending.
-Region grow(const MeshHost &m, std::vector<int> owned, std::vector<int> &mark, int stamp) {
+// Owned nodes plus three rings, each ring ascending.  Two nodes are
+// neighbours when an edge or an element joins them (the same on a whole
+// mesh; on the local mesh of a domain-decomposition part an element may be
+// kept while one of its edges is not).
+Region grow(const MeshHost &m, const std::vector<int> &nel_ptr, const std::vector<int> &nel,
+            std::vector<int> owned, std::vector<int> &mark, int stamp) {
   Region r;
   std::sort(owned.begin(), owned.end());
   r.nodes = owned;
@@ -63,6 +67,14 @@ Region grow(const MeshHost &m, std::vector<int> owned, std::vector<int> &mark, i
           ring.push_back(o);
         }
       }
+      for (int p = nel_ptr[n]; p < nel_ptr[n + 1]; p++)
+        for (int q = 0; q < 3; q++) {
+          const int o = m.elem_nodes[3 * nel[p] + q];
+          if (mark[o] != stamp) {
+            mark[o] = stamp;
+            ring.push_back(o);
+          }
+        }
     }
     std::sort(ring.begin(), ring.end());
     r.nodes.insert(r.nodes.end(), ring.begin(), ring.end());
@@ -144,7 +156,7 @@ TilePlanHost build_tile_plan(const MeshHost &m, const std::vector<int> &edge_slo
   while (!todo.empty()) {
     std::vector<int> owned = std::move(todo.back());
     todo.pop_back();
-    Region r = grow(m, owned, mark, stamp++);
+    Region r = grow(m, node_elems_ptr, node_elems, owned, mark, stamp++);
     // edges: E1 (an end in N1), then E2 \ E1 (an end in N2)
     std::vector<int> e1, e2;
     for (int i = 0; i < r.n2; i++) loc[r.nodes[i]] = i;

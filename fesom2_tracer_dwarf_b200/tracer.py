@@ -166,7 +166,7 @@ class FESOMTracerAdvection:
         return float(out[0]), float(out[1])
 
     def set_step_path(self, path):
-        """'fused' (default: one patch kernel per tracer where the scheme allows it) or 'five' (five kernels)."""
+        """'five' (default: five kernels) or 'fused' (one patch kernel per tracer where the scheme allows it)."""
         _lib.check(self.lib, self.lib.tracer_set_step_path({"fused": 0, "five": 1}[path]), "tracer_set_step_path")
 
     def set_patch_size(self, owned):

@@ -169,13 +169,15 @@ int tracer_set_precision(int mode);
  * latest full upload (tracer_set_values); tracer_storage_offset returns it
  * (0 in modes 0, 1). */
 int tracer_set_rounding(int mode);
-/* Step kernels (no counterpart in the reference): 0 (default) = one fused
- * kernel per tracer, a thread block per mesh patch that keeps the patch and
- * three halo rings on chip and writes only the new values, wherever the
- * scheme allows it (FP64 or FP32 modes, PPM or UPW1 vertical, no learned
- * flux); 1 = always the five-kernel path (gradients, edges, LO solution, FCT
- * ratios, update) with the intermediates in device memory.  Both paths give
- * bit-identical results.  tracer_step_info reports out4[0] = the path,
+/* Step kernels (no counterpart in the reference): 1 (default) = the
+ * five-kernel path (gradients, edges, LO solution, FCT ratios, update) with
+ * the intermediates in device memory; 0 = one fused kernel per tracer, a
+ * thread block per mesh patch that keeps the patch and three halo rings on
+ * chip and writes only the new values, wherever the scheme allows it (FP64
+ * or FP32 modes, PPM or UPW1 vertical, no learned flux) -- it moves about a
+ * third of the DRAM bytes but runs slower on B200 (one 12-warp block per SM,
+ * five block barriers per level).  Both paths give bit-identical FP64
+ * results.  tracer_step_info reports out4[0] = the path,
  * out4[1] = 1 when tracer 1 runs the fused kernel, out4[2] = patches of the
  * fused kernel's plan, out4[3] = the plan's LO-solution nodes per mesh node
  * (its halo redundancy). */

@@ -18,6 +18,14 @@ pytestmark = pytest.mark.gpu
 SCHEMES = [(h, v, l) for l in ("FCT", "NONE") for h in ("MUSCL", "MFCT", "UPW1") for v in ("PPM", "UPW1")]
 
 
+@pytest.fixture(autouse=True)
+def fused_path(api):
+    """These tests run the fused kernel (the engine's default is the
+    five-kernel path)."""
+    api.set_step_path("fused")
+    yield
+
+
 def _info(api):
     return api.step_info()
 
