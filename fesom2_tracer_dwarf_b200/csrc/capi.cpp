@@ -652,6 +652,26 @@ int tracer_advect_steps(int nsteps, double dt) {
 
 int tracer_advect_step(double dt) { return tracer_advect_steps(1, dt); }
 
+int tracer_advect_step_io(double dt, const double *const *values_in, double *const *values_out, int ntracers) {
+  return guarded([&] {
+    if (check_ready()) return -1;
+    if (g.ntr < 1) return fail("no tracers allocated");
+    if (ntracers != g.ntr) return fail("tracer_advect_step_io: ntracers must equal the allocated tracers");
+    if (!(dt > 0.0)) return fail("dt must be positive");
+    ensure_engine();
+    if (g.eng->step_io(dt, g.ab_refresh, values_in, values_out)) return 0;
+    // not page-locked (or 16-bit storage): the same operations one by one
+    const size_t LN = (size_t)(g.nl - 1) * g.nod2D;
+    (void)LN;
+    for (int t = 0; t < g.ntr; t++)
+      if (values_in && values_in[t]) g.eng->set_values(t, values_in[t], true);
+    g.eng->step(dt, g.ab_refresh);
+    for (int t = 0; t < g.ntr; t++)
+      if (values_out && values_out[t]) g.eng->get_values(t, values_out[t]);
+    return 0;
+  });
+}
+
 int tracer_get_values_id(int tracer_id, double *values, int nz, int nn) {
   return guarded([&] {
     if (check_ready()) return -1;

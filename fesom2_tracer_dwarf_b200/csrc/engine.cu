@@ -270,6 +270,14 @@ Engine::Engine(const MeshHost &mesh, Precision prec) : p_(new EngineImpl) {
 Engine::~Engine() {
   if (!p_) return;
   cudaStreamSynchronize(p_->stream);
+  if (p_->io_h2d) {
+    cudaStreamSynchronize(p_->io_h2d);
+    cudaStreamSynchronize(p_->io_d2h);
+    cudaStreamDestroy(p_->io_h2d);
+    cudaStreamDestroy(p_->io_d2h);
+  }
+  for (cudaEvent_t e : p_->io_ev_in) cudaEventDestroy(e);
+  for (cudaEvent_t e : p_->io_ev_out) cudaEventDestroy(e);
   release_ring(*p_);
   learned_release(*p_);
   for (void *a : p_->allocs) cudaFree(a);
@@ -553,6 +561,58 @@ void Engine::set_patch_size(int owned) {
   CK(cudaStreamSynchronize(p_->stream));
 }
 double Engine::tile_node_ratio() const { return p_->tplan.node_ratio; }
+
+bool Engine::step_io(double dt, bool refresh_ab, const double *const *in, double *const *out) {
+  EngineImpl &P = *p_;
+  const int ntr = (int)P.tr.size();
+  const size_t bytes = sizeof(double) * (size_t)(P.mesh.nl - 1) * P.mesh.nod2D;
+  if (P.prec != Precision::FP64 && P.prec != Precision::FP32) return false;
+  for (int t = 0; t < ntr; t++) {
+    if (in && in[t] && !host_range_pinned(in[t], bytes)) return false;
+    if (out && out[t] && !host_range_pinned(out[t], bytes)) return false;
+    if (!refresh_ab && !P.tr[t].TAB) return false;
+  }
+  CK(cudaStreamSynchronize(P.stream));
+  if (!P.io_h2d) {
+    CK(cudaStreamCreateWithFlags(&P.io_h2d, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&P.io_d2h, cudaStreamNonBlocking));
+  }
+  while ((int)P.io_in.size() < ntr) {
+    P.io_in.push_back(P.dalloc<double>(bytes / sizeof(double)));
+    P.io_out.push_back(P.dalloc<double>(bytes / sizeof(double)));
+    cudaEvent_t a, b;
+    CK(cudaEventCreateWithFlags(&a, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&b, cudaEventDisableTiming));
+    P.io_ev_in.push_back(a);
+    P.io_ev_out.push_back(b);
+  }
+  // every input copy is queued at once on the H2D stream; the compute stream
+  // takes each tracer as soon as its copy lands, and the D2H stream takes
+  // each new field as soon as its step is done
+  for (int t = 0; t < ntr; t++)
+    if (in && in[t]) {
+      CK(cudaMemcpyAsync(P.io_in[t], in[t], bytes, cudaMemcpyHostToDevice, P.io_h2d));
+      CK(cudaEventRecord(P.io_ev_in[t], P.io_h2d));
+    }
+  for (int t = 0; t < ntr; t++) {
+    auto &tr = P.tr[t];
+    if (in && in[t]) {
+      CK(cudaStreamWaitEvent(P.stream, P.io_ev_in[t], 0));
+      pack_from(P, P.io_in[t], P.stream, tr.T, tr.TAB, tr.Tout);
+    }
+    run_batch(P, t, 1, dt, refresh_ab);
+    if (out && out[t]) {
+      unpack_to(P, tr.T, P.io_out[t], P.stream);
+      CK(cudaEventRecord(P.io_ev_out[t], P.stream));
+      CK(cudaStreamWaitEvent(P.io_d2h, P.io_ev_out[t], 0));
+      CK(cudaMemcpyAsync(out[t], P.io_out[t], bytes, cudaMemcpyDeviceToHost, P.io_d2h));
+    }
+  }
+  CK(cudaStreamSynchronize(P.stream));
+  CK(cudaStreamSynchronize(P.io_d2h));
+  CK(cudaStreamSynchronize(P.io_h2d));
+  return true;
+}
 
 void Engine::step_tracer(int id, double dt, bool refresh_ab) {
   check_id(*p_, id);

@@ -99,6 +99,14 @@ class Engine {
   TracerScheme scheme(int id) const;
   // Advance every tracer one step.  refresh_ab: valuesAB := values first.
   void step(double dt, bool refresh_ab);
+  // One step with host I/O, pipelined per tracer: in[t] (nullable) becomes
+  // tracer t's values (and valuesAB), every tracer is advanced, out[t]
+  // (nullable) receives its new values.  Each tracer's upload, step and
+  // download run on their own streams so that tracer t+1's upload and
+  // tracer t-1's download overlap tracer t's step.  Needs page-locked host
+  // arrays (tracer_host_register) and FP64 or FP32 storage; returns false
+  // (nothing done) otherwise.
+  bool step_io(double dt, bool refresh_ab, const double *const *in, double *const *out);
   // Advance one tracer one step (the reference's tracer_advect_step on id).
   void step_tracer(int id, double dt, bool refresh_ab);
   // Device pointers / stream for benchmarking and tests.

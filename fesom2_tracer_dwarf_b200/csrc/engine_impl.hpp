@@ -75,6 +75,11 @@ struct EngineImpl {
   static constexpr int kRing = 4;
   double *stage_d = nullptr;
   double *stats_d = nullptr;  // per-block partial statistics (tracer_stats)
+  // pipelined host-I/O step (Engine::step_io): per-tracer device buffers of
+  // the host layout, the two copy streams and their events
+  std::vector<double *> io_in, io_out;
+  cudaStream_t io_h2d = nullptr, io_d2h = nullptr;
+  std::vector<cudaEvent_t> io_ev_in, io_ev_out;
   unsigned long long *nonfinite_d = nullptr;  // non-finite new values written by the steps
   void *ring[kRing] = {};
   cudaEvent_t ring_ev[kRing] = {};
@@ -186,6 +191,12 @@ double stage_wet_mean(EngineImpl &P);
 void stage_pack(EngineImpl &P, double off, void *d0, void *d1, void *d2);
 void stage_unpack(EngineImpl &P, const void *s, double off);
 void storage_reoffset(EngineImpl &P, void *s, double off_old, double off_new);
+// Host-I/O step helpers (FP64 / FP32 storage): whether a host range lies in
+// page-locked memory; (nl-1, nod2D) doubles -> storage arrays and back, on a
+// given stream with explicit device buffers.
+bool host_range_pinned(const void *p, size_t bytes);
+void pack_from(EngineImpl &P, const double *src, cudaStream_t st, void *d0, void *d1, void *d2);
+void unpack_to(EngineImpl &P, const void *s, double *dst, cudaStream_t st);
 // min, max, sum and NaN count of a tracer over the (nl-1, nod2D) values the
 // host reads back, reduced on the device (transfer.cu)
 void tracer_stats(EngineImpl &P, const void *s, double off, double out[4]);

@@ -421,6 +421,28 @@ void tracer_stats(EngineImpl &P, const void *s, double off, double out[4]) {
   out[3] = nan;
 }
 
+bool host_range_pinned(const void *p, size_t bytes) { return range_pinned(p, bytes); }
+
+void pack_from(EngineImpl &P, const double *src, cudaStream_t st, void *d0, void *d1, void *d2) {
+  const int L = P.mesh.nl - 1;
+  const long long N = P.mesh.nod2D;
+  if (P.prec == Precision::FP64)
+    k_pack<double><<<kGrid, kBlock, 0, st>>>(src, nlev_dev(P), L, P.S, N, 0.0, (double *)d0, (double *)d1, (double *)d2);
+  else
+    k_pack<float><<<kGrid, kBlock, 0, st>>>(src, nlev_dev(P), L, P.S, N, 0.0, (float *)d0, (float *)d1, (float *)d2);
+  CK(cudaGetLastError());
+}
+
+void unpack_to(EngineImpl &P, const void *s, double *dst, cudaStream_t st) {
+  const int L = P.mesh.nl - 1;
+  const long long N = P.mesh.nod2D;
+  if (P.prec == Precision::FP64)
+    k_unpack<double><<<kGrid, kBlock, 0, st>>>((const double *)s, nlev_dev(P), L, P.S, N, 0.0, dst);
+  else
+    k_unpack<float><<<kGrid, kBlock, 0, st>>>((const float *)s, nlev_dev(P), L, P.S, N, 0.0, dst);
+  CK(cudaGetLastError());
+}
+
 void storage_reoffset(EngineImpl &P, void *s, double off_old, double off_new) {
   if (P.prec == Precision::BF16) reoffset_t<__nv_bfloat16>(P, s, off_old, off_new);
   else if (P.prec == Precision::FP16) reoffset_t<__half>(P, s, off_old, off_new);

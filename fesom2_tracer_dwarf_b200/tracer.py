@@ -165,6 +165,18 @@ class FESOMTracerAdvection:
         _lib.check(self.lib, self.lib.tracer_volume_sum(tracer_id, _lib.ptr(out)), "tracer_volume_sum")
         return float(out[0]), float(out[1])
 
+    def advect_step_io(self, dt, values_in, values_out):
+        """One step with host I/O (tracer_advect_step_io): values_in[t] (or None)
+        become tracer t+1's values, values_out[t] (or None) receive the new
+        values; pipelined across tracers when every array is page-locked
+        (pin)."""
+        n = len(values_in)
+        vin = (ctypes.c_void_p * n)(*[None if a is None else a.ctypes.data for a in values_in])
+        vout = (ctypes.c_void_p * n)(*[None if a is None else a.ctypes.data for a in values_out])
+        _lib.check(self.lib, self.lib.tracer_advect_step_io(dt, ctypes.cast(vin, ctypes.c_void_p),
+                                                            ctypes.cast(vout, ctypes.c_void_p), n),
+                   "tracer_advect_step_io")
+
     def set_step_path(self, path):
         """'five' (default: five kernels) or 'fused' (one patch kernel per tracer where the scheme allows it)."""
         _lib.check(self.lib, self.lib.tracer_set_step_path({"fused": 0, "five": 1}[path]), "tracer_set_step_path")

@@ -192,6 +192,15 @@ int tracer_set_patch_size(int owned);
  * it); with tracer_set_nan_check(1), tracer_advect_step / _steps return -1
  * with a message when the steps of the call produced any. */
 int tracer_set_nan_check(int on);
+/* One step with host I/O (no counterpart in the reference): values_in[t]
+ * (nullable) becomes tracer t+1's values (and valuesAB), every tracer is
+ * advanced once, values_out[t] (nullable) receives its new values; arrays
+ * (nl-1, nod2D).  When every array is page-locked (tracer_host_register)
+ * and the storage is FP64 or FP32, the uploads, the per-tracer steps and the
+ * downloads are pipelined on three streams (tracer t+1 uploads and tracer
+ * t-1 downloads while tracer t steps); otherwise the same operations run one
+ * after the other.  ntracers must equal the allocated tracers. */
+int tracer_advect_step_io(double dt, const double *const *values_in, double *const *values_out, int ntracers);
 int tracer_step_status(long long *nonfinite);
 /* Builds the fused kernel's patch plan for the loaded mesh on the host (no
  * device needed) with patches of about max_owned owned nodes, checks it

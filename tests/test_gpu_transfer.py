@@ -65,3 +65,41 @@ def test_transfer_larger_than_the_staging_ring(api):
         api.unpin(V)
         api.unpin(out)
     assert np.array_equal(out, V)
+
+
+@pytest.mark.parametrize("pinned", [True, False])
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_step_io_matches_the_separate_calls(api, pinned, prec):
+    """tracer_advect_step_io (pipelined when the host arrays are page-locked)
+    gives the bits of set_values / advect_step / get_values, two steps in a
+    row, with valuesAB refreshed and frozen."""
+    from fesom2_tracer_dwarf_b200.workloads import layered_flow_case
+    c = layered_flow_case(api, 60, 14, seed=2)
+    L, N = c.T.shape
+    for refresh in (True, False):
+        api.set_precision(prec)
+        api.allocate_tracers(2)
+        for t, v in ((1, c.T), (2, c.S)):
+            api.set_values(t, v)
+            api.set_scheme(t, "MUSCL", "PPM", "FCT")
+        api.set_velocity(c.uv, c.w)
+        api.set_ab_refresh(refresh)
+        ins = [np.asfortranarray(c.T + 0.5), np.asfortranarray(c.S - 0.25)]
+        outs = [np.zeros((L, N), order="F"), np.zeros((L, N), order="F")]
+        if pinned:
+            for a in ins + outs:
+                api.pin(a)
+        for step in range(2):
+            api.advect_step_io(c.dt, ins, outs)
+            got = [o.copy() for o in outs]
+            api.set_values(1, ins[0])
+            api.set_values(2, ins[1])
+            api.advect_steps(1, c.dt)
+            ref = [api.get_tracer_values(1), api.get_tracer_values(2)]
+            for g, r in zip(got, ref):
+                assert np.array_equal(g.view(np.uint64), r.view(np.uint64)), (step, refresh)
+            for a, g in zip(ins, got):
+                a[...] = g  # the next step starts from this one's result
+        if pinned:
+            for a in ins + outs:
+                api.unpin(a)
