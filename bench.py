@@ -168,7 +168,8 @@ def committed_traffic(args):
     'dram_bytes_per_step_scaled: X'); None for any other workload or
     precision, which that capture does not cover."""
     p = ROOT / "profiles" / "step_c2_fp64.md"
-    if args.precision != "fp64" or args.learned or args.nx != 1000 or args.nl != 64 or not p.exists():
+    if (args.precision != "fp64" or args.learned or args.nx != 1000 or args.nl != 64 or args.step_path != "five"
+            or not p.exists()):
         return None
     for line in p.read_text().splitlines():
         if line.strip().startswith("dram_bytes_per_step_scaled:"):
@@ -322,6 +323,21 @@ def run_ours(args):
             api.advect_step_io(dt, [Th, Sh], [outT, outS])
         return ranks.max((time.perf_counter() - t0) / args.e2e_steps)
 
+    def ref_loop():
+        """The reference harness's loop (src/fesom_analytic.F90:385-449):
+        one step, then min / max / sum of tracer 1 read back, every step."""
+        st = np.zeros(4)
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.e2e_steps):
+            if api.advect_step(dt) != 0:
+                raise RuntimeError(api.lib.tracer_last_error().decode())
+            api.lib.tracer_get_stats_id(1, st.ctypes.data_as(ctypes.c_void_p))
+        return ranks.max((time.perf_counter() - t0) / args.e2e_steps)
+
+    ref_loop()
+    ref_loop_sec = ref_loop()
+
     host = [np.asfortranarray(api.get_tracer_values(1)), np.asfortranarray(api.get_tracer_values(2)),
             np.zeros((L, N), order="F"), np.zeros((L, N), order="F")]
     e2e_pageable_sec = e2e_loop(host)
@@ -352,6 +368,10 @@ def run_ours(args):
                                            if args.learned else ""),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
+                         "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum of the five step "
+                                            "kernels of one step on the 300x300x64 case of this workload, scaled by "
+                                            "wet cells (x11.17) to this size; profiles/step_c2_fp64.md"
+                                            if traffic else None),
                          "kernel": f"full step (all kernels of one step, {BYTES_PER_CELL[args.precision]} B/cell algorithmic)",
                          "peak_source": f"{peak_kind} hbm_gbs"},
             "kernel_ms_per_step": kernel_ms,
@@ -364,6 +384,10 @@ def run_ours(args):
                            "ms_per_step": e2e_serial_sec * 1e3},
             "e2e_pageable": {"value": world * 2 * cells / e2e_pageable_sec, "unit": "cell-updates/s",
                              "ms_per_step": e2e_pageable_sec * 1e3},
+            "reference_loop": {"value": world * 2 * cells / ref_loop_sec, "unit": "cell-updates/s",
+                               "what": "tracer_advect_step + tracer_get_stats every step (the reference "
+                                       "harness's loop; state stays on the device)",
+                               "ms_per_step": ref_loop_sec * 1e3},
             "gpu_launches": launches_per_step * args.steps,
             "clocks": clocks,
         }
