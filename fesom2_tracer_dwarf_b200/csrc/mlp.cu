@@ -104,6 +104,34 @@ __device__ __forceinline__ float gelu_grad(float z) {
   return 0.5f * (1.0f + t) + 0.5f * z * (1.0f - t * t) * kGeluC * (1.0f + 3.0f * kGeluA * z * z);
 }
 
+// The inference epilogues evaluate GELU on packed FP16 pairs (two values per
+// instruction, hardware tanh.approx.f16x2): the activations are stored as
+// BF16 anyway, whose 8-bit mantissa is coarser than FP16's 11 bits, and the
+// output layer still accumulates in FP32.  Training keeps the FP32 form.
+__device__ __forceinline__ __half2 tanh_fast2(__half2 x) {
+  uint32_t y, xi = *reinterpret_cast<uint32_t *>(&x);
+  asm("tanh.approx.f16x2 %0, %1;" : "=r"(y) : "r"(xi));
+  return *reinterpret_cast<__half2 *>(&y);
+}
+__device__ __forceinline__ __half2 gelu2(__half2 z) {
+  const __half2 c = __float2half2_rn(kGeluC), ca = __float2half2_rn(kGeluC * kGeluA), h = __float2half2_rn(0.5f);
+  const __half2 z2 = __hmul2(z, z);
+  const __half2 u = __hmul2(z, __hfma2(ca, z2, c));  // c z + c a z^3
+  const __half2 hz = __hmul2(h, z);
+  return __hfma2(hz, tanh_fast2(u), hz);             // z/2 (1 + tanh u)
+}
+// 16 FP32 pre-activations (bias added) -> GELU -> 16 BF16 in two 16-byte stores
+__device__ __forceinline__ void gelu_store16(unsigned char *base, uint32_t off_lo, uint32_t off_hi, const float *v,
+                                             const float *bias) {
+  __align__(16) __nv_bfloat162 o[8];
+  for (int i = 0; i < 8; i++) {
+    const __half2 g = gelu2(__floats2half2_rn(v[2 * i] + bias[2 * i], v[2 * i + 1] + bias[2 * i + 1]));
+    o[i] = __float22bfloat162_rn(__half22float2(g));
+  }
+  *reinterpret_cast<uint4 *>(base + off_lo) = *reinterpret_cast<const uint4 *>(o);
+  *reinterpret_cast<uint4 *>(base + off_hi) = *reinterpret_cast<const uint4 *>(o + 4);
+}
+
 struct MlpDev {
   const __nv_bfloat16 *W1b, *W2b;  // [64][16], [64][64] BF16
   const float *p;                  // FP32 packed parameters
@@ -221,9 +249,7 @@ __global__ void __launch_bounds__(128, 1)
     for (int c = 0; c < kH; c += 16) {
       float v[16];
       umma::tmem_ld16(D1 + lane + c, v);
-      for (int i = 0; i < 16; i++) v[i] = gelu(v[i] + sb1[c + i]);
-      st_bf16x8(sm + FwdSmem::H1, umma::kmajor_offset(tid, c, kH), v);
-      st_bf16x8(sm + FwdSmem::H1, umma::kmajor_offset(tid, c + 8, kH), v + 8);
+      gelu_store16(sm + FwdSmem::H1, umma::kmajor_offset(tid, c, kH), umma::kmajor_offset(tid, c + 8, kH), v, sb1 + c);
     }
     smem_to_tc();
     if (tid == 0) {
@@ -235,7 +261,11 @@ __global__ void __launch_bounds__(128, 1)
     for (int c = 0; c < kH; c += 16) {
       float v[16];
       umma::tmem_ld16(D2 + lane + c, v);
-      for (int i = 0; i < 16; i++) acc += gelu(v[i] + sb2[c + i]) * sw3[c + i];
+      for (int i = 0; i < 16; i += 2) {
+        const float2 g = __half22float2(gelu2(__floats2half2_rn(v[i] + sb2[c + i], v[i + 1] + sb2[c + i + 1])));
+        acc += g.x * sw3[c + i];
+        acc += g.y * sw3[c + i + 1];
+      }
     }
     if (sample < S) y[sample] = acc + b3;
     umma::tc_fence_before();
