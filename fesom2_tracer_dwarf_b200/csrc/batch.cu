@@ -133,7 +133,9 @@ BatchKernel pick_kernel_b(const TracerScheme &s) {
 
 // the register budget follows the resident threads per SM the tile asks for
 BatchKernel pick_kernel(const TracerScheme &s, int threads = 256, int blocks_per_sm = 2) {
-  const int minb = std::max(2, std::min(5, (threads * blocks_per_sm + 255) / 256));
+  const int minb = std::max(2, std::min(7, (threads * blocks_per_sm + 255) / 256));
+  if (minb == 7) return pick_kernel_b<7>(s);
+  if (minb == 6) return pick_kernel_b<6>(s);
   if (minb == 5) return pick_kernel_b<5>(s);
   if (minb == 4) return pick_kernel_b<4>(s);
   if (minb == 3) return pick_kernel_b<3>(s);
