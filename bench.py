@@ -427,8 +427,11 @@ def timed(gpu, fn):
 def run_c3(args):
     """48 tracers x 8 ensemble members on seeded analytic meshes of uneven
     size (nx = ny in [100, 800], nl in [20, 80], periodic and closed mixed),
-    FP32 MUSCL+PPM+FCT: the persistent one-launch step (autotuned tile,
-    replayed from a CUDA graph) against the per-member separate launches."""
+    FP32 MUSCL+PPM+FCT: the batched step on the path and tile the autotuner
+    picks (one persistent launch per phase and wave, or one cooperative launch
+    per step), replayed from a CUDA graph, against the per-member separate
+    launches; both batched paths are timed at the chosen tile."""
+    import re
     from fesom2_tracer_dwarf_b200 import FESOMTracerAdvection
     from fesom2_tracer_dwarf_b200.batch import TracerBatch
     from fesom2_tracer_dwarf_b200.workloads import build_ensemble, ensemble_specs
@@ -438,14 +441,27 @@ def run_c3(args):
     dts = build_ensemble(batch, api, specs, 48)
     batch.configure(dts, "MUSCL", "PPM", "FCT")
     info = batch.info()
-    batch.autotune(2)
+    log = batch.autotune(2)
+    tuned = {}
+    for ln in log.splitlines():
+        mt = re.match(r"path=(\w+) .*ms_per_step=([0-9.eE+-]+)", ln)
+        if mt:
+            tuned[mt.group(1)] = min(tuned.get(mt.group(1), 1e30), float(mt.group(2)))
     tile = batch.tile()
-    batch.steps(max(args.warmup, 3), graph=True)
+    chosen = batch.path()
     steps = max(args.steps, 1)
-    ms_graph, clocks = timed(0, lambda: batch.time_steps(steps, graph=True) / steps)
-    ms_plain = batch.time_steps(steps, graph=False) / steps
-    ms_sep = batch.time_separate(steps) / steps
-    ms_sep_graph = batch.time_separate(steps, graph=True) / steps
+    paths = {}
+    for path in ("phases", "cooperative"):
+        batch.set_path(path)
+        batch.steps(max(args.warmup, 3), graph=True)
+        ms_g, clk = timed(0, lambda: batch.time_steps(steps, graph=True) / steps)
+        paths[f"{path}_graph"] = ms_g
+        paths[f"{path}_no_graph"] = batch.time_steps(steps, graph=False) / steps
+        if path == chosen:
+            ms_graph, clocks = ms_g, clk
+    batch.set_path(chosen)
+    paths["separate_launches"] = batch.time_separate(steps) / steps
+    paths["separate_launches_graph"] = batch.time_separate(steps, graph=True) / steps
     cells = info["cell_tracers"]
     batch.close()
     api.cleanup()
@@ -453,10 +469,9 @@ def run_c3(args):
             "n_gpus": 1, "steps": steps, "warmup": args.warmup, "ms_per_step": ms_graph, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": "48 tracers x 8 members, nx=ny in [100,800], nl in [20,80], periodic/closed "
-                                   "mixed, seeds 0..7, MUSCL+PPM+FCT, one persistent launch per step in a CUDA graph",
-                       "members": specs, "cell_tracers": cells, "tile": tile},
-            "paths_ms_per_step": {"persistent_graph": ms_graph, "persistent_no_graph": ms_plain,
-                                  "separate_launches": ms_sep, "separate_launches_graph": ms_sep_graph},
+                                   f"mixed, seeds 0..7, MUSCL+PPM+FCT, batched path '{chosen}' in a CUDA graph",
+                       "members": specs, "cell_tracers": cells, "tile": tile, "path": chosen},
+            "paths_ms_per_step": paths, "autotune_best_ms_per_step": tuned,
             "clocks": clocks}
     print(json.dumps(line))
     return 0

@@ -106,6 +106,8 @@ SIGNATURES = {
     "tracer_batch_set_tile": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     "tracer_batch_get_tile": (ctypes.c_int, [_vp]),
     "tracer_batch_autotune": (ctypes.c_int, [ctypes.c_int, ctypes.c_char_p, ctypes.c_int]),
+    "tracer_batch_set_path": (ctypes.c_int, [ctypes.c_int]),
+    "tracer_batch_get_path": (ctypes.c_int, []),
     "tracer_batch_steps": (ctypes.c_int, [ctypes.c_int, ctypes.c_int]),
     "tracer_batch_time_steps": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),
     "tracer_batch_steps_separate": (ctypes.c_int, [ctypes.c_int, ctypes.c_int]),

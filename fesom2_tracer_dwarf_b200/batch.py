@@ -81,6 +81,18 @@ class TracerBatch:
         _lib.check(self.lib, self.lib.tracer_batch_autotune(steps_per_candidate, buf, len(buf)), "tracer_batch_autotune")
         return buf.value.decode()
 
+    PATHS = {"cooperative": 0, "phases": 1}
+
+    def set_path(self, path):
+        """'phases' (default): one persistent launch per phase and wave;
+        'cooperative': the whole step as one cooperative launch."""
+        _lib.check(self.lib, self.lib.tracer_batch_set_path(self.PATHS[path]), "tracer_batch_set_path")
+
+    def path(self):
+        rc = self.lib.tracer_batch_get_path()
+        _lib.check(self.lib, min(rc, 0), "tracer_batch_get_path")
+        return {v: k for k, v in self.PATHS.items()}[rc]
+
     def steps(self, n, graph=True):
         _lib.check(self.lib, self.lib.tracer_batch_steps(n, int(bool(graph))), "tracer_batch_steps")
 

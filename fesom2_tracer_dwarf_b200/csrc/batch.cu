@@ -142,6 +142,98 @@ BatchKernel pick_kernel(const TracerScheme &s, int threads = 256, int blocks_per
   return pick_kernel_b<2>(s);
 }
 
+// One persistent launch per phase: the launch walks the blocks of every task
+// of a wave for one phase (grid = SMs x resident blocks of that kernel), so
+// each phase keeps the register budget of its standalone kernel and the task
+// descriptors sit in the kernel's parameter space (constant bank) instead of
+// shared memory.  Kernel boundaries order the phases.
+constexpr int kPackTasks = 16;
+struct PhasePack {
+  int ntasks;
+  int prefix[kPackTasks + 1];  // running totals of the tasks' blocks of this phase
+  BatchTask t[kPackTasks];
+};
+static_assert(sizeof(PhasePack) <= 32000, "phase pack must fit the kernel parameter space");
+
+template <int PH>
+struct PhaseBudget {
+  static constexpr int v = PH == PH_GRAD   ? MinBlocks<float>::grad
+                           : PH == PH_EDGE ? MinBlocks<float>::edge
+                           : PH == PH_COL1 ? MinBlocks<float>::col1
+                           : PH == PH_COL2 ? MinBlocks<float>::col2
+                                           : MinBlocks<float>::col3;
+};
+
+template <int PH, int HOR, int VER, int LIM>
+__global__ void __launch_bounds__(kThreads, PhaseBudget<PH>::v) k_batch_phase(const __grid_constant__ PhasePack p) {
+  extern __shared__ __align__(16) int smem[];
+  const int total = p.prefix[p.ntasks];
+  int task = 0;
+  for (int g = blockIdx.x; g < total; g += gridDim.x) {
+    while (p.prefix[task + 1] <= g) task++;
+    if (g != (int)blockIdx.x) __syncthreads();  // the previous item is done with shared memory
+    const int vblk = g - p.prefix[task];
+    const BatchTask &st = p.t[task];
+    if (PH == PH_GRAD) grad_block<float, float, kNT>(st.m, st.a, vblk, smem);
+    else if (PH == PH_EDGE) edge_block<float, float, kNT, HOR, LIM>(st.m, st.a, vblk, smem);
+    else if (PH == PH_COL1) col1_block<float, float, kNT, VER, LIM>(st.m, st.a, vblk, smem);
+    else if (PH == PH_COL2) col2_block<float, float, kNT>(st.m, st.a, vblk, smem);
+    else col3_block<float, float, kNT, LIM>(st.m, st.a, vblk, smem);
+  }
+}
+
+// dynamic shared memory of each phase: that of its standalone kernel
+size_t phase_smem(int ph) {
+  switch (ph) {
+    case PH_GRAD:
+    case PH_EDGE: return smem_edge();
+    case PH_COL1: return StageIncidence<float>::col1 ? smem_col_staged<float>(kNT, 2) : smem_col<float>(kNT, 2);
+    case PH_COL2: return StageIncidence<float>::col2 ? smem_col_staged<float>(kNT, 2) : smem_col<float>(kNT, 2);
+    default: return StageIncidence<float>::col3 ? smem_col_staged<float>(kNT, 0) : smem_col<float>(kNT, 0);
+  }
+}
+
+struct PhaseKernel {
+  const void *fn = nullptr;
+  void (*launch)(const PhasePack &, int, size_t, cudaStream_t) = nullptr;
+};
+
+template <int PH, int HOR, int VER, int LIM>
+void launch_phase(const PhasePack &p, int grid, size_t smem, cudaStream_t st) {
+  k_batch_phase<PH, HOR, VER, LIM><<<grid, kThreads, smem, st>>>(p);
+}
+
+template <int HOR, int VER, int LIM>
+void phase_kernels_t(PhaseKernel *k) {
+  k[PH_GRAD] = {(const void *)k_batch_phase<PH_GRAD, HOR, VER, LIM>, launch_phase<PH_GRAD, HOR, VER, LIM>};
+  k[PH_EDGE] = {(const void *)k_batch_phase<PH_EDGE, HOR, VER, LIM>, launch_phase<PH_EDGE, HOR, VER, LIM>};
+  k[PH_COL1] = {(const void *)k_batch_phase<PH_COL1, HOR, VER, LIM>, launch_phase<PH_COL1, HOR, VER, LIM>};
+  if (LIM == LIM_FCT)
+    k[PH_COL2] = {(const void *)k_batch_phase<PH_COL2, HOR, VER, LIM>, launch_phase<PH_COL2, HOR, VER, LIM>};
+  k[PH_COL3] = {(const void *)k_batch_phase<PH_COL3, HOR, VER, LIM>, launch_phase<PH_COL3, HOR, VER, LIM>};
+}
+
+bool phase_kernels(const TracerScheme &s, PhaseKernel *k) {
+  for (int ph = 0; ph < PH_COUNT; ph++) k[ph] = PhaseKernel{};
+  if (s.hor == HOR_MUSCL && s.ver == VER_PPM && s.lim == LIM_FCT) phase_kernels_t<HOR_MUSCL, VER_PPM, LIM_FCT>(k);
+  else if (s.hor == HOR_MUSCL && s.ver == VER_PPM && s.lim == LIM_NONE) phase_kernels_t<HOR_MUSCL, VER_PPM, LIM_NONE>(k);
+  else if (s.hor == HOR_UPW1 && s.ver == VER_UPW1 && s.lim == LIM_FCT) phase_kernels_t<HOR_UPW1, VER_UPW1, LIM_FCT>(k);
+  else if (s.hor == HOR_UPW1 && s.ver == VER_UPW1 && s.lim == LIM_NONE) phase_kernels_t<HOR_UPW1, VER_UPW1, LIM_NONE>(k);
+  else return false;
+  return true;
+}
+
+// Edge volume fluxes of a member's velocity (the values k_edge computes), so
+// that every batch task loads them (vflux_mode 2) instead of recomputing them.
+__global__ void __launch_bounds__(256) k_batch_vflux(DMeshT<float> m, const float *vel, float *vflux) {
+  const size_t n = (size_t)m.E * m.S;
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
+    const int s = (int)(q / m.S), k = (int)(q - (size_t)s * m.S);
+    if (k >= m.edge_lev[s].y) continue;
+    vflux[q] = edge_vflux(m, edge_ctx(m, s), vel, k);
+  }
+}
+
 // test kernel: a barrier that waits for one block more than the grid has,
 // so it must give up after `limit` polls and report it
 __global__ void k_barrier_timeout(GridBarrier *bar, long long limit, int *status) {
@@ -179,6 +271,25 @@ struct BatchImpl {
   cudaGraphExec_t sep_exec = nullptr;
   std::vector<cudaEvent_t> sep_events;
 
+  // step path: 0 one cooperative launch per step, 1 one persistent launch
+  // per phase and wave
+  int mode = 1;
+  // work-array slots, host task table (wave-major) and blocks per phase
+  struct Slot {
+    void *adfh[kNT], *adfv[kNT], *lo[kNT], *rp[kNT], *rm[kNT], *gradn[kNT];
+  };
+  std::vector<std::vector<Slot>> slots;
+  std::vector<BatchTask> tasks;
+  std::vector<int> wave_first;
+  std::vector<std::vector<int>> nblk;
+  PhaseKernel phk[PH_COUNT];
+  int phgrid[PH_COUNT] = {0, 0, 0, 0, 0};
+  // phase launches of two steps captured as a graph; valid while the first
+  // tracer's current buffer is the one seen at capture
+  cudaGraph_t ph_graph = nullptr;
+  cudaGraphExec_t ph_exec = nullptr;
+  const void *ph_key = nullptr;
+
   ~BatchImpl() {
     release();
     release_sep();
@@ -198,12 +309,19 @@ struct BatchImpl {
     if (graph) cudaGraphDestroy(graph);
     graph_exec = nullptr;
     graph = nullptr;
+    if (ph_exec) cudaGraphExecDestroy(ph_exec);
+    if (ph_graph) cudaGraphDestroy(ph_graph);
+    ph_exec = nullptr;
+    ph_graph = nullptr;
+    ph_key = nullptr;
   }
   void release() {
     release_graph();
     for (void *w : work) cudaFree(w);
     work.clear();
     work_bytes = 0;
+    slots.clear();
+    tasks.clear();
     if (d_tasks) cudaFree(d_tasks);
     if (d_prefix) cudaFree(d_prefix);
     if (d_wave_first) cudaFree(d_wave_first);
@@ -220,6 +338,75 @@ struct BatchImpl {
     return p;
   }
 };
+
+namespace {
+
+// Every member's edge volume fluxes, computed once per velocity (the member
+// engine's own cache: a new velocity invalidates it).
+void refresh_vflux(BatchImpl &B) {
+  for (auto &mem : B.members) {
+    EngineImpl &P = *mem->impl();
+    if (P.vflux && P.vflux_valid) continue;
+    if (!P.vflux) P.vflux = P.dalloc_bytes((size_t)P.mesh.edge2D * P.S * P.r_bytes);
+    const size_t n = (size_t)P.dm32.E * P.dm32.S;
+    const int grid = (int)std::max<size_t>(1, std::min<size_t>((n + 255) / 256, (size_t)B.sms * 16));
+    mem->synchronize();
+    k_batch_vflux<<<grid, 256, 0, B.stream>>>(P.dm32, (const float *)P.vel, (float *)P.vflux);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(B.stream));
+    P.vflux_valid = true;
+  }
+}
+
+// The task table (wave-major) from the members' current tracer buffers and
+// the batch's work-array slots.
+void make_tasks(BatchImpl &B) {
+  const int M = (int)B.members.size(), W = B.tile.wave;
+  B.tasks.clear();
+  B.wave_first.clear();
+  B.nblk.assign(PH_COUNT, std::vector<int>());
+  for (int w = 0; w < B.nwaves; w++) {
+    B.wave_first.push_back((int)B.tasks.size());
+    for (int m = 0; m < M; m++) {
+      EngineImpl &P = *B.members[m]->impl();
+      for (int b = w * W; b < std::min((w + 1) * W, B.ntr[m] / kNT); b++) {
+        const BatchImpl::Slot &sl = B.slots[m][b % W];
+        BatchTask T{};
+        T.m = P.dm32;
+        FusedArgs<float, float> &a = T.a;
+        for (int t = 0; t < kNT; t++) {
+          auto &tr = P.tr[b * kNT + t];
+          a.T[t] = (const float *)tr.T;
+          a.TAB[t] = (const float *)(B.refresh_ab ? tr.T : tr.TAB);
+          a.T_out[t] = (float *)tr.Tout;
+          a.adf_h[t] = (float *)sl.adfh[t];
+          a.adf_v[t] = (float *)sl.adfv[t];
+          a.lo[t] = (float *)sl.lo[t];
+          a.rp[t] = (float *)sl.rp[t];
+          a.rm[t] = (float *)sl.rm[t];
+          a.gradn[t] = (float *)sl.gradn[t];
+        }
+        a.vflux = (float *)P.vflux;
+        a.vflux_mode = 2;
+        a.vel = (const float *)P.vel;
+        a.W = (const float *)P.W;
+        a.dt = (float)B.dt[m];
+        a.ph = (float)B.sch.ph;
+        a.pv = (float)B.sch.pv;
+        B.tasks.push_back(T);
+        B.nblk[PH_GRAD].push_back(B.sch.hor == HOR_UPW1 ? 0 : P.dm32.grad_sched.nblk);
+        B.nblk[PH_EDGE].push_back(P.dm32.edge_sched.nblk);
+        B.nblk[PH_COL1].push_back(P.dm32.node_sched.nblk);
+        B.nblk[PH_COL2].push_back(B.sch.lim == LIM_FCT ? P.dm32.node_sched.nblk : 0);
+        B.nblk[PH_COL3].push_back(P.dm32.node_sched.nblk);
+      }
+    }
+  }
+  B.wave_first.push_back((int)B.tasks.size());
+  B.ntasks = (int)B.tasks.size();
+}
+
+}  // namespace
 
 Batch::Batch() : p_(new BatchImpl) {
   CK(cudaStreamCreateWithFlags(&p_->stream, cudaStreamNonBlocking));
@@ -259,7 +446,7 @@ void Batch::configure(const TracerScheme &sch, const std::vector<double> &dt, bo
 
 BatchTile Batch::tile() const { return p_->tile; }
 long long Batch::work_bytes() const { return p_->work_bytes; }
-bool Batch::graph_captured() const { return p_->graph_exec != nullptr; }
+bool Batch::graph_captured() const { return p_->mode == 1 ? p_->ph_exec != nullptr : p_->graph_exec != nullptr; }
 
 long long Batch::wet_cells() const {
   long long c = 0;
@@ -277,6 +464,7 @@ void Batch::set_tile(const BatchTile &tile) {
   B.release();
   B.tile = tile;
   B.kernel = pick_kernel(B.sch, tile.threads, tile.blocks_per_sm);
+  phase_kernels(B.sch, B.phk);
   const size_t smem = batch_smem();
   CK(cudaFuncSetAttribute(B.kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int occ = 0;
@@ -297,7 +485,7 @@ void Batch::set_tile(const BatchTile &tile) {
     for (int m = 0; m < M; m++) {
       const EngineImpl &P = *B.members[m]->impl();
       const size_t ns = (size_t)P.mesh.nod2D * P.S * sizeof(float), es = (size_t)P.mesh.edge2D * P.S * sizeof(float);
-      need += (size_t)std::min(W, B.ntr[m] / kNT) * (es + kNT * (es + 6 * ns));
+      need += (size_t)std::min(W, B.ntr[m] / kNT) * kNT * (es + 6 * ns);
     }
     CK(cudaMemGetInfo(&free_b, &total_b));
     if (need > free_b / 10 * 9)
@@ -305,75 +493,49 @@ void Batch::set_tile(const BatchTile &tile) {
   }
   B.tile.wave = W;
   B.nwaves = (max_batches + W - 1) / W;
-  struct Slot { void *adfh[kNT], *adfv[kNT], *lo[kNT], *rp[kNT], *rm[kNT], *gradn[kNT], *vflux; };
-  std::vector<std::vector<Slot>> slots(M, std::vector<Slot>(W));
+  B.slots.assign(M, std::vector<BatchImpl::Slot>(W));
   for (int m = 0; m < M; m++) {
     EngineImpl &P = *B.members[m]->impl();
     const size_t ns = (size_t)P.mesh.nod2D * P.S * sizeof(float), es = (size_t)P.mesh.edge2D * P.S * sizeof(float);
     const int used = std::min(W, B.ntr[m] / kNT);
     for (int j = 0; j < used; j++) {
-      Slot &s = slots[m][j];
-      s.vflux = B.walloc(es);
+      BatchImpl::Slot &sl = B.slots[m][j];
       for (int t = 0; t < kNT; t++) {
-        s.adfh[t] = B.walloc(es);
-        s.adfv[t] = B.walloc(ns);
-        s.lo[t] = B.walloc(ns);
-        s.rp[t] = B.walloc(ns);
-        s.rm[t] = B.walloc(ns);
-        s.gradn[t] = B.walloc(2 * ns);
+        sl.adfh[t] = B.walloc(es);
+        sl.adfv[t] = B.walloc(ns);
+        sl.lo[t] = B.walloc(ns);
+        sl.rp[t] = B.walloc(ns);
+        sl.rm[t] = B.walloc(ns);
+        sl.gradn[t] = B.walloc(2 * ns);
       }
     }
   }
-  std::vector<BatchTask> tasks;
-  std::vector<int> wave_first;
-  std::vector<std::vector<int>> nblk(PH_COUNT);
-  for (int w = 0; w < B.nwaves; w++) {
-    wave_first.push_back((int)tasks.size());
-    for (int m = 0; m < M; m++) {
-      EngineImpl &P = *B.members[m]->impl();
-      for (int b = w * W; b < std::min((w + 1) * W, B.ntr[m] / kNT); b++) {
-        const Slot &s = slots[m][b % W];
-        BatchTask T{};
-        T.m = P.dm32;
-        FusedArgs<float, float> &a = T.a;
-        for (int t = 0; t < kNT; t++) {
-          auto &tr = P.tr[b * kNT + t];
-          a.T[t] = (const float *)tr.T;
-          a.TAB[t] = (const float *)(B.refresh_ab ? tr.T : tr.TAB);
-          a.T_out[t] = (float *)tr.Tout;
-          a.adf_h[t] = (float *)s.adfh[t];
-          a.adf_v[t] = (float *)s.adfv[t];
-          a.lo[t] = (float *)s.lo[t];
-          a.rp[t] = (float *)s.rp[t];
-          a.rm[t] = (float *)s.rm[t];
-          a.gradn[t] = (float *)s.gradn[t];
-        }
-        a.vflux = (float *)s.vflux;
-        a.vel = (const float *)P.vel;
-        a.W = (const float *)P.W;
-        a.dt = (float)B.dt[m];
-        a.ph = (float)B.sch.ph;
-        a.pv = (float)B.sch.pv;
-        tasks.push_back(T);
-        nblk[PH_GRAD].push_back(P.dm32.grad_sched.nblk);
-        nblk[PH_EDGE].push_back(P.dm32.edge_sched.nblk);
-        for (int ph : {PH_COL1, PH_COL2, PH_COL3}) nblk[ph].push_back(P.dm32.node_sched.nblk);
-      }
-    }
-  }
-  wave_first.push_back((int)tasks.size());
-  B.ntasks = (int)tasks.size();
+  refresh_vflux(B);
+  make_tasks(B);
   std::vector<int> prefix((size_t)PH_COUNT * (B.ntasks + 1), 0);
   for (int ph = 0; ph < PH_COUNT; ph++)
-    for (int i = 0; i < B.ntasks; i++) prefix[(size_t)ph * (B.ntasks + 1) + i + 1] = prefix[(size_t)ph * (B.ntasks + 1) + i] + nblk[ph][i];
+    for (int i = 0; i < B.ntasks; i++)
+      prefix[(size_t)ph * (B.ntasks + 1) + i + 1] = prefix[(size_t)ph * (B.ntasks + 1) + i] + B.nblk[ph][i];
   CK(cudaMalloc(&B.d_tasks, sizeof(BatchTask) * std::max(1, B.ntasks)));
   CK(cudaMalloc(&B.d_prefix, sizeof(int) * prefix.size()));
-  CK(cudaMalloc(&B.d_wave_first, sizeof(int) * wave_first.size()));
+  CK(cudaMalloc(&B.d_wave_first, sizeof(int) * B.wave_first.size()));
   CK(cudaMalloc(&B.d_bar, sizeof(GridBarrier)));
-  CK(cudaMemcpyAsync(B.d_tasks, tasks.data(), sizeof(BatchTask) * tasks.size(), cudaMemcpyHostToDevice, B.stream));
+  CK(cudaMemcpyAsync(B.d_tasks, B.tasks.data(), sizeof(BatchTask) * B.tasks.size(), cudaMemcpyHostToDevice, B.stream));
   CK(cudaMemcpyAsync(B.d_prefix, prefix.data(), sizeof(int) * prefix.size(), cudaMemcpyHostToDevice, B.stream));
-  CK(cudaMemcpyAsync(B.d_wave_first, wave_first.data(), sizeof(int) * wave_first.size(), cudaMemcpyHostToDevice, B.stream));
+  CK(cudaMemcpyAsync(B.d_wave_first, B.wave_first.data(), sizeof(int) * B.wave_first.size(), cudaMemcpyHostToDevice,
+                     B.stream));
   CK(cudaMemsetAsync(B.d_bar, 0, sizeof(GridBarrier), B.stream));
+  // persistent grid of every phase kernel
+  for (int ph = 0; ph < PH_COUNT; ph++) {
+    B.phgrid[ph] = 0;
+    if (!B.phk[ph].fn) continue;
+    const size_t sm = phase_smem(ph);
+    CK(cudaFuncSetAttribute(B.phk[ph].fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    int pocc = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pocc, B.phk[ph].fn, kThreads, sm));
+    if (pocc < 1) throw std::runtime_error("batched phase kernel cannot be resident");
+    B.phgrid[ph] = B.sms * pocc;
+  }
   CK(cudaStreamSynchronize(B.stream));
 }
 
@@ -424,40 +586,138 @@ void capture(BatchImpl &B) {
 
 }  // namespace
 
-void Batch::step(int nsteps, bool use_graph) {
-  BatchImpl &B = *p_;
-  if (!B.configured || !B.d_tasks) throw std::runtime_error("configure the batch first");
-  for (auto &m : B.members) m->synchronize();
+namespace {
+
+// the host task table after one step: new and old buffers swap
+void swap_tasks(BatchImpl &B) {
+  for (auto &T : B.tasks) {
+    FusedArgs<float, float> &a = T.a;
+    for (int q = 0; q < kNT; q++) {
+      float *old = const_cast<float *>(a.T[q]);
+      a.T[q] = a.T_out[q];
+      a.T_out[q] = old;
+      if (B.refresh_ab) a.TAB[q] = a.T[q];
+    }
+  }
+}
+
+// one step as persistent phase launches (one per phase and wave) from the
+// host task table, which then swaps
+void phase_step(BatchImpl &B) {
+  PhasePack p{};
+  for (int w = 0; w < B.nwaves; w++) {
+    const int t0 = B.wave_first[w], t1 = B.wave_first[w + 1];
+    for (int ph = 0; ph < PH_COUNT; ph++) {
+      if (!B.phk[ph].fn) continue;
+      for (int c0 = t0; c0 < t1; c0 += kPackTasks) {
+        p.ntasks = 0;
+        p.prefix[0] = 0;
+        for (int t = c0; t < std::min(t1, c0 + kPackTasks); t++) {
+          p.t[p.ntasks] = B.tasks[t];
+          p.prefix[p.ntasks + 1] = p.prefix[p.ntasks] + B.nblk[ph][t];
+          p.ntasks++;
+        }
+        const int total = p.prefix[p.ntasks];
+        if (total == 0) continue;
+        B.phk[ph].launch(p, std::min(total, B.phgrid[ph]), phase_smem(ph), B.stream);
+      }
+    }
+  }
+  swap_tasks(B);
+}
+
+void capture_phases(BatchImpl &B) {
+  const void *key = B.tasks.empty() ? nullptr : (const void *)B.tasks[0].a.T[0];
+  if (B.ph_exec && B.ph_key == key) return;
+  if (B.ph_exec) cudaGraphExecDestroy(B.ph_exec);
+  if (B.ph_graph) cudaGraphDestroy(B.ph_graph);
+  B.ph_exec = nullptr;
+  B.ph_graph = nullptr;
+  CK(cudaStreamBeginCapture(B.stream, cudaStreamCaptureModeThreadLocal));
+  phase_step(B);
+  phase_step(B);  // two steps: the task table is back where it started
+  cudaGraph_t g = nullptr;
+  CK(cudaStreamEndCapture(B.stream, &g));
+  B.ph_graph = g;
+  CK(cudaGraphInstantiate(&B.ph_exec, g, 0));
+  B.ph_key = key;
+}
+
+// nsteps of the selected path on the batch stream
+void run_steps(BatchImpl &B, int nsteps, bool use_graph, bool upload = true) {
+  if (B.mode == 1) {
+    if (use_graph && nsteps >= 2) {
+      capture_phases(B);
+      for (int s = 0; s + 1 < nsteps; s += 2) CK(cudaGraphLaunch(B.ph_exec, B.stream));
+      if (nsteps % 2) phase_step(B);
+    } else {
+      for (int s = 0; s < nsteps; s++) phase_step(B);
+    }
+    return;
+  }
+  // the cooperative kernel swaps its device-side table itself; the host copy follows
+  if (upload)
+    CK(cudaMemcpyAsync(B.d_tasks, B.tasks.data(), sizeof(BatchTask) * B.tasks.size(), cudaMemcpyHostToDevice, B.stream));
   if (use_graph) capture(B);
   for (int s = 0; s < nsteps; s++) {
     if (use_graph) CK(cudaGraphLaunch(B.graph_exec, B.stream));
     else launch_once(B);
   }
+  if (nsteps % 2) swap_tasks(B);
+}
+
+void begin_steps(BatchImpl &B) {
+  if (!B.configured || !B.d_tasks) throw std::runtime_error("configure the batch first");
+  for (auto &m : B.members) m->synchronize();
+  bool stale = false;
+  for (auto &m : B.members) stale = stale || !m->impl()->vflux_valid || !m->impl()->vflux;
+  if (stale) {
+    refresh_vflux(B);
+    make_tasks(B);
+    B.release_graph();
+  }
+}
+
+}  // namespace
+
+void Batch::set_path(int path) {
+  if (path != 0 && path != 1) throw std::invalid_argument("batch path: 0 (one cooperative launch per step) or 1 (one launch per phase)");
+  p_->mode = path;
+}
+int Batch::path() const { return p_->mode; }
+
+void Batch::step(int nsteps, bool use_graph) {
+  BatchImpl &B = *p_;
+  begin_steps(B);
+  run_steps(B, nsteps, use_graph);
   CK(cudaGetLastError());
-  check_barrier(B);
+  if (B.mode == 0) check_barrier(B);
+  else CK(cudaStreamSynchronize(B.stream));
   swap_host(B, nsteps);
 }
 
 double Batch::time_steps(int nsteps, bool use_graph) {
   BatchImpl &B = *p_;
-  if (!B.configured || !B.d_tasks) throw std::runtime_error("configure the batch first");
-  for (auto &m : B.members) m->synchronize();
-  if (use_graph) capture(B);
+  begin_steps(B);
+  // capture (and the device table upload) outside the timed region
+  if (use_graph && B.mode == 1 && nsteps >= 2) capture_phases(B);
+  if (B.mode == 0) {
+    CK(cudaMemcpyAsync(B.d_tasks, B.tasks.data(), sizeof(BatchTask) * B.tasks.size(), cudaMemcpyHostToDevice, B.stream));
+    if (use_graph) capture(B);
+  }
   cudaEvent_t a, b;
   CK(cudaEventCreate(&a));
   CK(cudaEventCreate(&b));
   CK(cudaEventRecord(a, B.stream));
-  for (int s = 0; s < nsteps; s++) {
-    if (use_graph) CK(cudaGraphLaunch(B.graph_exec, B.stream));
-    else launch_once(B);
-  }
+  run_steps(B, nsteps, use_graph, false);
   CK(cudaEventRecord(b, B.stream));
   CK(cudaEventSynchronize(b));
   float ms = 0.f;
   CK(cudaEventElapsedTime(&ms, a, b));
   cudaEventDestroy(a);
   cudaEventDestroy(b);
-  check_barrier(B);
+  CK(cudaGetLastError());
+  if (B.mode == 0) check_barrier(B);
   swap_host(B, nsteps);
   return ms;
 }
@@ -563,9 +823,35 @@ std::string Batch::autotune(int steps_per_candidate) {
   double best_ms = 1e30;
   int max_batches = 0;
   for (int m = 0; m < num_members(); m++) max_batches = std::max(max_batches, B.ntr[m] / kNT);
+  int best_mode = B.mode;
   for (int cells : {256, 384, 512}) {
     for (int wave : {1, 2, 4}) {
       if (wave > max_batches && wave != 1) continue;
+      // one launch per phase: the tile's threads and blocks per SM do not apply
+      {
+        BatchTile t;
+        t.cells_per_block = cells;
+        t.wave = wave;
+        bool ok = true;
+        try {
+          set_tile(t);
+        } catch (const std::exception &e) {
+          cudaGetLastError();
+          log << "path=phases cells=" << cells << " wave=" << wave << " skipped: " << e.what() << "\n";
+          ok = false;
+        }
+        if (ok) {
+          B.mode = 1;
+          time_steps(1, false);  // warm-up
+          const double ms = time_steps(steps_per_candidate, false) / steps_per_candidate;
+          log << "path=phases cells=" << cells << " wave=" << B.tile.wave << " ms_per_step=" << ms << "\n";
+          if (ms < best_ms) {
+            best_ms = ms;
+            best = B.tile;
+            best_mode = 1;
+          }
+        }
+      }
       for (int threads : {128, 256}) {
         for (int bps : {2, 3, 4, 5, 6, 8, 10}) {
           BatchTile t;
@@ -577,18 +863,20 @@ std::string Batch::autotune(int steps_per_candidate) {
             set_tile(t);
           } catch (const std::exception &e) {
             cudaGetLastError();
-            log << "cells=" << cells << " wave=" << wave << " threads=" << threads << " bps=" << bps
+            log << "path=cooperative cells=" << cells << " wave=" << wave << " threads=" << threads << " bps=" << bps
                 << " skipped: " << e.what() << "\n";
             continue;
           }
           if (B.tile.blocks_per_sm != bps) continue;  // occupancy cap: same as a smaller candidate
+          B.mode = 0;
           time_steps(1, false);  // warm-up
           const double ms = time_steps(steps_per_candidate, false) / steps_per_candidate;
-          log << "cells=" << cells << " wave=" << B.tile.wave << " threads=" << threads << " bps=" << bps
-              << " ms_per_step=" << ms << "\n";
+          log << "path=cooperative cells=" << cells << " wave=" << B.tile.wave << " threads=" << threads
+              << " bps=" << bps << " ms_per_step=" << ms << "\n";
           if (ms < best_ms) {
             best_ms = ms;
             best = B.tile;
+            best_mode = 0;
           }
         }
       }
@@ -607,8 +895,10 @@ std::string Batch::autotune(int steps_per_candidate) {
     }
   }
   set_tile(best);
-  log << "best: cells=" << best.cells_per_block << " wave=" << best.wave << " threads=" << best.threads
-      << " bps=" << best.blocks_per_sm << " ms_per_step=" << best_ms << "\n";
+  B.mode = best_mode;
+  log << "best: path=" << (best_mode == 1 ? "phases" : "cooperative") << " cells=" << best.cells_per_block
+      << " wave=" << best.wave << " threads=" << best.threads << " bps=" << best.blocks_per_sm
+      << " ms_per_step=" << best_ms << "\n";
   return log.str();
 }
 

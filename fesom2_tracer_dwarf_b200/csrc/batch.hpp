@@ -2,17 +2,22 @@
 // meshes of different sizes, advanced together).
 //
 // Every member is an FP32 Engine that owns its mesh, velocity and tracers.
-// One step of the whole batch is ONE persistent cooperative kernel launch:
-// the launch walks a work list of (member, 4-tracer batch, block of wet
-// cells) items phase by phase -- ring-mean gradients, edge fluxes, vertical
-// fluxes and low-order solution, FCT bounds and ratios, limiting and update --
-// with a grid-wide barrier between phases.  Tracer batches run in waves of a
-// bounded number per member so the work arrays stay small.  The kernel swaps
-// the new and old tracer buffers in its device-side task table at the end, so
-// the same launch, captured once in a CUDA graph, advances the batch step
-// after step.  An autotuner picks the tile (wet cells per block, i.e. nodes
-// per block x levels), the threads per block, the persistent grid size and
-// the number of tracer batches in flight.
+// Two step paths walk the same work list of (member, 4-tracer batch, block
+// of wet cells) items phase by phase -- ring-mean gradients, edge fluxes,
+// vertical fluxes and low-order solution, FCT bounds and ratios, limiting and
+// update.  Path 0: ONE persistent cooperative launch per step, a grid-wide
+// barrier between phases; the kernel swaps the new and old tracer buffers in
+// its device-side task table at the end, so the same launch, captured once in
+// a CUDA graph, advances the batch step after step.  Path 1: one persistent
+// launch per phase and wave over all members (kernel boundaries order the
+// phases), each phase kernel with its own register budget and the wave's task
+// descriptors passed by value in parameter space; two steps are captured as
+// one CUDA graph.  Tracer batches run in waves of a bounded number per member
+// so the work arrays stay small; every member's edge volume fluxes are
+// computed once per velocity.  An autotuner picks the path and the tile (wet
+// cells per block, i.e. nodes per block x levels), the threads per block and
+// persistent grid size of path 0, and the number of tracer batches in
+// flight.
 #pragma once
 #include <memory>
 #include <string>
@@ -49,7 +54,15 @@ class Batch {
   void set_tile(const BatchTile &tile);
   BatchTile tile() const;
 
-  // nsteps persistent launches (replayed from a CUDA graph when use_graph).
+  // Step path: 0 = one persistent cooperative launch per step (phases
+  // separated by a bounded-wait grid barrier); 1 (default) = one persistent
+  // launch per phase and wave over every member's blocks, each phase with the
+  // register budget of its standalone kernel and the task descriptors in
+  // kernel parameter space.
+  void set_path(int path);
+  int path() const;
+
+  // nsteps steps of the selected path (replayed from a CUDA graph when use_graph).
   void step(int nsteps, bool use_graph);
   // Device time of nsteps (CUDA events on the batch stream), milliseconds.
   double time_steps(int nsteps, bool use_graph);

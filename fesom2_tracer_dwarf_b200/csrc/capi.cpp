@@ -1025,6 +1025,17 @@ int tracer_batch_get_tile(int *tile4) {
   });
 }
 
+int tracer_batch_set_path(int path) {
+  return guarded([&] {
+    batch().set_path(path);
+    return 0;
+  });
+}
+
+int tracer_batch_get_path(void) {
+  return guarded([&] { return batch().path(); });
+}
+
 int tracer_batch_steps(int nsteps, int use_graph) {
   return guarded([&] {
     if (nsteps < 0) return fail("nsteps < 0");

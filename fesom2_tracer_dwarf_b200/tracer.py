@@ -32,6 +32,7 @@ class FESOMTracerAdvection:
 
     def __init__(self, lib_path=None):
         self.lib = _lib.load(lib_path)
+        self._pinned = {}  # host address -> array kept alive while page-locked
 
     # ---- methods of python/demo_tracer.py ---------------------------------
     def initialize_mpi(self, mpi_comm=0):
@@ -138,14 +139,27 @@ class FESOMTracerAdvection:
         _lib.check(self.lib, self.lib.tracer_set_precision(self.PRECISIONS[mode]), "tracer_set_precision")
 
     def pin(self, array):
-        """Page-lock a contiguous numpy array so its transfers take one DMA (tracer_host_register)."""
+        """Page-lock a contiguous numpy array so its transfers take one DMA
+        (tracer_host_register).  The array is kept alive until unpin() or
+        cleanup(): memory freed while still registered would leave the
+        registration behind for whatever the allocator puts there next."""
         if not (array.flags["F_CONTIGUOUS"] or array.flags["C_CONTIGUOUS"]):
             raise ValueError("pin needs a contiguous array")
+        addr = array.ctypes.data
+        if addr in self._pinned:
+            return array
         _lib.check(self.lib, self.lib.tracer_host_register(_lib.ptr(array), array.nbytes), "tracer_host_register")
+        self._pinned[addr] = array
         return array
 
     def unpin(self, array):
+        addr = array.ctypes.data
         _lib.check(self.lib, self.lib.tracer_host_unregister(_lib.ptr(array)), "tracer_host_unregister")
+        self._pinned.pop(addr, None)
+
+    def unpin_all(self):
+        for a in list(self._pinned.values()):
+            self.unpin(a)
 
     ROUNDING = {"nearest": 0, "stochastic": 1}
 
@@ -256,6 +270,7 @@ class FESOMTracerAdvection:
         _lib.check(self.lib, self.lib.tracer_scalar_output_close(), "tracer_scalar_output_close")
 
     def cleanup(self):
+        self.unpin_all()
         return self.lib.tracer_cleanup()
 
 

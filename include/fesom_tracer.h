@@ -199,7 +199,11 @@ int tracer_set_nan_check(int on);
  * and the storage is FP64 or FP32, the uploads, the per-tracer steps and the
  * downloads are pipelined on three streams (tracer t+1 uploads and tracer
  * t-1 downloads while tracer t steps); otherwise the same operations run one
- * after the other.  ntracers must equal the allocated tracers. */
+ * after the other.  ntracers must equal the allocated tracers.  FP64 results
+ * are those of tracer_set_values + tracer_advect_step + tracer_get_values bit
+ * for bit; in FP32 the pipelined form steps each tracer alone where
+ * tracer_advect_step batches up to four, and the FP32 kernels of different
+ * batch sizes may contract different multiply-adds (an ulp or so). */
 int tracer_advect_step_io(double dt, const double *const *values_in, double *const *values_out, int ntracers);
 int tracer_step_status(long long *nonfinite);
 /* Builds the fused kernel's patch plan for the loaded mesh on the host (no
@@ -299,13 +303,16 @@ int tracer_advect_device_noalloc(int tracer_id, const double *T_dev, const doubl
 long long tracer_noalloc_scratch_bytes(void);
 /* ---- multi-member batch: no counterpart in the reference -----------------
  * Many tracers of many ensemble members, each on its own analytic mesh (any
- * sizes, periodic or closed), advanced together in FP32.  One step of the
- * whole batch is one persistent cooperative kernel launch that walks every
- * member's work phase by phase with grid-wide barriers (bounded waits: a
- * timed-out barrier makes the step return -1); tracer_batch_steps with
- * use_graph = 1 replays that launch from a CUDA graph.  Members are numbered
- * from 0, tracers from 1.  Supported schemes: MUSCL+PPM or UPW1+UPW1, with or
- * without FCT, one scheme for all tracers. */
+ * sizes, periodic or closed), advanced together in FP32.  Two step paths
+ * (tracer_batch_set_path): path 1 (default) runs one persistent launch per
+ * phase (gradients, edge fluxes, vertical fluxes and LO solution, FCT ratios,
+ * limiting and update) and wave of tracer batches over every member's work;
+ * path 0 runs the whole step as one persistent cooperative launch with
+ * grid-wide barriers between the phases (bounded waits: a timed-out barrier
+ * makes the step return -1).  tracer_batch_steps with use_graph = 1 replays
+ * the launches from a CUDA graph.  Both paths give the same bits.  Members are
+ * numbered from 0, tracers from 1.  Supported schemes: MUSCL+PPM or
+ * UPW1+UPW1, with or without FCT, one scheme for all tracers. */
 int tracer_batch_create(void);
 int tracer_batch_destroy(void);
 /* Adds a member on the analytic mesh of tracer_init_analytic's arguments with
@@ -328,12 +335,16 @@ int tracer_batch_configure(const char *hor, const char *ver, const char *lim, do
  * per member. */
 int tracer_batch_set_tile(int cells_per_block, int threads, int blocks_per_sm, int wave);
 int tracer_batch_get_tile(int *tile4);
-/* Times every candidate tile on steps_per_candidate steps (the tracer state
- * is restored afterwards) and keeps the fastest; log receives one line per
- * candidate (truncated to log_capacity). */
+/* Times every candidate (path and tile) on steps_per_candidate steps (the
+ * tracer state is restored afterwards) and keeps the fastest; log receives
+ * one line per candidate (truncated to log_capacity). */
 int tracer_batch_autotune(int steps_per_candidate, char *log, int log_capacity);
+/* Step path: 0 one cooperative launch per step, 1 one persistent launch per
+ * phase and wave.  get returns the path or -1. */
+int tracer_batch_set_path(int path);
+int tracer_batch_get_path(void);
 int tracer_batch_steps(int nsteps, int use_graph);
-/* Device time (CUDA events) of nsteps persistent steps, milliseconds. */
+/* Device time (CUDA events) of nsteps steps of the selected path, milliseconds. */
 int tracer_batch_time_steps(int nsteps, int use_graph, double *ms);
 /* The same steps as per-member launches of the four-to-five step kernels per
  * 4-tracer batch (the path tracer_advect_step takes) on the members' own

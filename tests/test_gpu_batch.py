@@ -1,7 +1,9 @@
-"""Multi-member batch (tracer_batch_*): the persistent one-launch step, with
-and without its CUDA graph, at any tile, gives the bits of the per-member
-separate launches; the bounded grid barrier reports a timeout instead of
-hanging; the autotuner keeps the tracer state."""
+"""Multi-member batch (tracer_batch_*): both persistent step paths (one
+cooperative launch per step; one launch per phase and wave), with and
+without their CUDA graphs, at any tile, and mixed step by step, give the bits
+of the per-member separate launches, also after a member's velocity changes;
+the bounded grid barrier reports a timeout instead of hanging; the autotuner
+keeps the tracer state."""
 import numpy as np
 import pytest
 
@@ -39,9 +41,12 @@ def test_barrier_timeout_is_reported(lib):
     assert lib.tracer_selftest_barrier_timeout(1 << 14) == 1
 
 
-def test_persistent_step_matches_separate_launches(small_batch):
+@pytest.mark.parametrize("path", ["cooperative", "phases"])
+def test_persistent_step_matches_separate_launches(small_batch, path):
     b, specs, dts, init = small_batch
     b.set_tile(cells_per_block=256, threads=128, blocks_per_sm=2, wave=1)
+    b.set_path(path)
+    assert b.path() == path
     b.steps(3, graph=True)
     graph = _state(b)
     _reset(b, init)
@@ -63,13 +68,61 @@ def test_persistent_step_matches_separate_launches(small_batch):
 def test_tiles_do_not_change_results(small_batch):
     b, specs, dts, init = small_batch
     results = []
-    for tile in ({"cells_per_block": 128, "threads": 64, "blocks_per_sm": 1, "wave": 1},
-                 {"cells_per_block": 512, "threads": 256, "blocks_per_sm": 2, "wave": 2}):
+    for path in ("cooperative", "phases"):
+        for tile in ({"cells_per_block": 128, "threads": 64, "blocks_per_sm": 1, "wave": 1},
+                     {"cells_per_block": 512, "threads": 256, "blocks_per_sm": 2, "wave": 2}):
+            _reset(b, init)
+            b.set_tile(**tile)
+            b.set_path(path)
+            b.steps(2, graph=True)
+            results.append(_state(b))
+    assert all(_same(results[0], r) for r in results[1:])
+
+
+def test_paths_mixed_step_by_step(small_batch):
+    """Odd step counts on one path, then the other (the task tables of both
+    paths follow the buffer swaps), against separate launches."""
+    b, specs, dts, init = small_batch
+    b.set_tile(cells_per_block=256, threads=128, blocks_per_sm=2, wave=1)
+    b.set_path("cooperative")
+    b.steps(1, graph=True)
+    b.set_path("phases")
+    b.steps(3, graph=True)
+    b.set_path("cooperative")
+    b.steps(1, graph=False)
+    b.set_path("phases")
+    b.steps(2, graph=False)
+    mixed = _state(b)
+    _reset(b, init)
+    b.steps_separate(7)
+    assert _same(mixed, _state(b))
+
+
+def test_new_velocity_is_picked_up(small_batch, api):
+    """A member's velocity replaced between steps: the batch recomputes that
+    member's edge volume fluxes (both paths, as the separate launches do)."""
+    from fesom2_tracer_dwarf_b200.workloads import layered_flow_case
+    b, specs, dts, init = small_batch
+    s = specs[1]
+    c = layered_flow_case(api, s["nx"], s["nl"], periodic=s["periodic"], seed=s["seed"])
+    api.cleanup()
+    out = {}
+    for path in ("cooperative", "phases", "separate"):
         _reset(b, init)
-        b.set_tile(**tile)
-        b.steps(2, graph=True)
-        results.append(_state(b))
-    assert _same(results[0], results[1])
+        b.set_velocity(1, c.uv, c.w)
+        if path == "separate":
+            b.steps_separate(1)
+            b.set_velocity(1, 0.5 * c.uv, 0.5 * c.w)
+            b.steps_separate(2)
+        else:
+            b.set_path(path)
+            b.steps(1, graph=True)
+            b.set_velocity(1, 0.5 * c.uv, 0.5 * c.w)
+            b.steps(2, graph=True)
+        out[path] = _state(b)
+    assert _same(out["cooperative"], out["separate"])
+    assert _same(out["phases"], out["separate"])
+    assert not _same(out["phases"], init)
 
 
 def test_member_matches_single_mesh_fp32_engine(small_batch, api):
