@@ -155,13 +155,30 @@ struct PhasePack {
 };
 static_assert(sizeof(PhasePack) <= 32000, "phase pack must fit the kernel parameter space");
 
+// resident 256-thread blocks per SM each phase kernel's register budget is
+// cut for (build-time knobs; default: the standalone FP32 kernels' budgets)
+#ifndef FESOM_PHASE_MINB_GRAD
+#define FESOM_PHASE_MINB_GRAD FESOM_MINB32_GRAD
+#endif
+#ifndef FESOM_PHASE_MINB_EDGE
+#define FESOM_PHASE_MINB_EDGE FESOM_MINB32_EDGE
+#endif
+#ifndef FESOM_PHASE_MINB_COL1
+#define FESOM_PHASE_MINB_COL1 FESOM_MINB32_COL1
+#endif
+#ifndef FESOM_PHASE_MINB_COL2
+#define FESOM_PHASE_MINB_COL2 FESOM_MINB32_COL2
+#endif
+#ifndef FESOM_PHASE_MINB_COL3
+#define FESOM_PHASE_MINB_COL3 FESOM_MINB32_COL3
+#endif
 template <int PH>
 struct PhaseBudget {
-  static constexpr int v = PH == PH_GRAD   ? MinBlocks<float>::grad
-                           : PH == PH_EDGE ? MinBlocks<float>::edge
-                           : PH == PH_COL1 ? MinBlocks<float>::col1
-                           : PH == PH_COL2 ? MinBlocks<float>::col2
-                                           : MinBlocks<float>::col3;
+  static constexpr int v = PH == PH_GRAD   ? FESOM_PHASE_MINB_GRAD
+                           : PH == PH_EDGE ? FESOM_PHASE_MINB_EDGE
+                           : PH == PH_COL1 ? FESOM_PHASE_MINB_COL1
+                           : PH == PH_COL2 ? FESOM_PHASE_MINB_COL2
+                                           : FESOM_PHASE_MINB_COL3;
 };
 
 template <int PH, int HOR, int VER, int LIM>

@@ -46,11 +46,13 @@ def test_mlp_forward_matches_cpu(lib, S):
     y = np.zeros(S, dtype=np.float32)
     assert lib.tracer_mlp_forward(X.ctypes.data, S, p.ctypes.data, y.ctypes.data) == 0
     ref, _ = mo.forward(from_bf16_bits(X), p)
-    # error relative to the output's scale: the kernels' hardware tanh
-    # (tanh.approx.f32) is good to about 2^-11, and the BF16 rounding of the
-    # hidden activation can flip on the resulting differences
+    # error relative to the output's scale: the first hidden layer's GELU runs
+    # in FP16 pairs (FP16 rounding 2^-11, tanh.approx.f16x2) and the second's
+    # in FP32 (tanh.approx.f32, about 2^-11); the BF16 rounding of the first
+    # hidden activation can flip on the resulting differences.  Measured: 1.5e-2
+    # at the 99.9 % quantile (below 1e-2 with both layers in FP32), 1.8e-2 at most.
     err = np.abs(y - ref) / max(np.sqrt(np.mean(ref ** 2)), 1e-30)
-    assert np.quantile(err, 0.999) < 1e-2 and err.max() < 5e-2, (np.quantile(err, 0.999), err.max())
+    assert np.quantile(err, 0.999) < 2.5e-2 and err.max() < 5e-2, (np.quantile(err, 0.999), err.max())
 
 
 @pytest.mark.parametrize("S", [128, 777, 20000])
