@@ -269,7 +269,7 @@ __device__ __forceinline__ void grad_block(const DMeshT<R> &m, const FusedArgs<R
     const int j = s_item[lc], n = cm.i0 + j, k = m.grad_lev0[n] + lc - (s_off[j] - cm.c0);
     R gx[NTMAX], gy[NTMAX];
     ring_mean_n(m, a.TAB, a.off, NT, n, k, gx, gy);
-    const size_t o = (size_t)n * m.S + k;
+    const cix o = (cix)n * m.S + k;
     for (int t = 0; t < NT; t++) st_pair(a.gradn[t] + 2 * o, gx[t], gy[t]);
   }
 }
@@ -291,7 +291,7 @@ __device__ __forceinline__ void trxy_n(const DMeshT<R> &m, const TS *const *tab,
   const R *gs = m.grad_sca + 6 * elem;
   const R g0 = gs[0], g1 = gs[1], g2 = gs[2], g3 = gs[3], g4 = gs[4], g5 = gs[5];
   for (int t = 0; t < NT; t++) {
-    const R t1 = ldT(tab[t], (size_t)a * m.S + k, off[t]), t2 = ldT(tab[t], (size_t)b * m.S + k, off[t]), t3 = ldT(tab[t], (size_t)c * m.S + k, off[t]);
+    const R t1 = ldT(tab[t], (cix)a * m.S + k, off[t]), t2 = ldT(tab[t], (cix)b * m.S + k, off[t]), t3 = ldT(tab[t], (cix)c * m.S + k, off[t]);
     gx[t] = (g0 * t1 + g1 * t2) + g2 * t3;
     gy[t] = (g3 * t1 + g4 * t2) + g5 * t3;
   }
@@ -328,7 +328,7 @@ __device__ __forceinline__ void edge_block(const DMeshT<R> &m, const FusedArgs<R
   const R re = R(kREarthD), sixth = R(1.0 / 6.0);
   for (int lc = threadIdx.x; lc < cm.nc; lc += blockDim.x) {
     const int j = s_item[lc], e = cm.i0 + j, k = lc - (s_off[j] - cm.c0);
-    const size_t o = (size_t)e * m.S + k;
+    const cix o = (cix)e * m.S + k;
     const int2 nn = m.edge_nodes[e];
     R vflux;
     if (a.vflux_mode == 2) {
@@ -337,7 +337,7 @@ __device__ __forceinline__ void edge_block(const DMeshT<R> &m, const FusedArgs<R
       vflux = edge_vflux(m, edge_ctx(m, e), a.vel, k);
       if (LIM == LIM_FCT || a.vflux_mode == 1) a.vflux[o] = vflux;
     }
-    const size_t o1 = (size_t)nn.x * m.S + k, o2 = (size_t)nn.y * m.S + k;
+    const cix o1 = (cix)nn.x * m.S + k, o2 = (cix)nn.y * m.S + k;
     if (HOR == HOR_UPW1) {
       for (int t = 0; t < NT; t++) {
         const R flo = (LIM == LIM_FCT) ? upw1_flux(vflux, ldT(a.T[t], o1, a.off[t]), ldT(a.T[t], o2, a.off[t])) : R(0);
@@ -392,7 +392,7 @@ __device__ __forceinline__ void edge_block(const DMeshT<R> &m, const FusedArgs<R
           const R face = R(0.5) * (Tmean1 + Tmean2);
           const R sig = fabs(td - tu) + (fabs(xu) + fabs(xd)) * sixth + R(1e-6) * (fabs(tu) + fabs(td)) + R(1e-20);
           const R inv = R(1) / sig;
-          const size_t ou = fwd ? o1 : o2;
+          const cix ou = fwd ? o1 : o2;
           const R cour = fmin(fabs(vflux) * a.dt / (m.areasvol[ou] * m.hnode_new[ou]), R(4));
           const R gx = fwd ? gux[t] : gdx[t], gy = fwd ? guy[t] : gdy[t];
           const R trans = (-ey * re * gx + ex * aa * gy) * inv;
@@ -467,13 +467,13 @@ __device__ __forceinline__ void col1_block(const DMeshT<R> &m, const FusedArgs<R
     if (VER == VER_PPM) {
       const int nlev = m.nlev_node[n];
       if (nz >= 2 && nz <= nlev - 2) {
-        const R *HN = m.hnode_new + (size_t)n * S;
+        const R *HN = m.hnode_new + (cix)n * S;
         const R dzjm1 = HN[k - 1], dzj = HN[k], dzjp1 = HN[k + 1];
         const R c1 = dzj / (dzjm1 + dzj + dzjp1);
         const R c2 = (R(2) * dzjm1 + dzj) / (dzjp1 + dzj);
         const R c3 = (dzj + R(2) * dzjp1) / (dzjm1 + dzj);
         for (int t = 0; t < NT; t++) {
-          const TS *Tc = a.TAB[t] + (size_t)n * S;
+          const TS *Tc = a.TAB[t] + (cix)n * S;
           s_slope[t * kMaxCellsPerBlock + lc] = ppm_slope(ldT(Tc, k - 1, a.off[t]), ldT(Tc, k, a.off[t]), ldT(Tc, k + 1, a.off[t]), c1, c2, c3);
         }
       }
@@ -486,19 +486,19 @@ __device__ __forceinline__ void col1_block(const DMeshT<R> &m, const FusedArgs<R
     for (int lc = threadIdx.x; lc < cm.nc; lc += blockDim.x) {
       const int j = s_item[lc], n = cm.i0 + j, k = lc - (s_off[j] - cm.c0), i = k + 1;
       const int nlev = m.nlev_node[n];
-      const R *HN = m.hnode_new + (size_t)n * S;
-      const R *Wc = a.W + (size_t)n * S;
+      const R *HN = m.hnode_new + (cix)n * S;
+      const R *Wc = a.W + (cix)n * S;
       if (i == 1) {
-        for (int t = 0; t < NT; t++) s_tv[t * kMaxCellsPerBlock + lc] = ldT(a.TAB[t], (size_t)n * S, a.off[t]);
+        for (int t = 0; t < NT; t++) s_tv[t * kMaxCellsPerBlock + lc] = ldT(a.TAB[t], (cix)n * S, a.off[t]);
       } else if (i == nlev - 1) {
         const R s = sgn1(Wc[nlev - 2]);
         for (int t = 0; t < NT; t++) {
-          const TS *Tc = a.TAB[t] + (size_t)n * S;
+          const TS *Tc = a.TAB[t] + (cix)n * S;
           s_tv[t * kMaxCellsPerBlock + lc] = -ldT(Tc, nlev - 3, a.off[t]) * fmin2(s, R(0)) + ldT(Tc, nlev - 2, a.off[t]) * fmax2(s, R(0));
         }
       } else if (i == 2) {
         for (int t = 0; t < NT; t++) {
-          const TS *Tc = a.TAB[t] + (size_t)n * S;
+          const TS *Tc = a.TAB[t] + (cix)n * S;
           s_tv[t * kMaxCellsPerBlock + lc] = R(0.5) * (ldT(Tc, 0, a.off[t]) + ldT(Tc, 1, a.off[t]));
         }
       } else {
@@ -512,7 +512,7 @@ __device__ __forceinline__ void col1_block(const DMeshT<R> &m, const FusedArgs<R
         const R D = dzj * (dzjm1 + dzj) / (R(2) * dzj + dzjp1);
         const R E = dzjp1 * (dzjp1 + dzjp2) / (dzj + R(2) * dzjp1);
         for (int t = 0; t < NT; t++) {
-          const TS *Tc = a.TAB[t] + (size_t)n * S;
+          const TS *Tc = a.TAB[t] + (cix)n * S;
           const R T0 = ldT(Tc, nzz - 1, a.off[t]), T1 = ldT(Tc, nzz, a.off[t]);
           const R dj = s_slope[t * kMaxCellsPerBlock + lc - 1];   // layer nzz
           const R djp1 = s_slope[t * kMaxCellsPerBlock + lc];     // layer nzz + 1
@@ -526,7 +526,7 @@ __device__ __forceinline__ void col1_block(const DMeshT<R> &m, const FusedArgs<R
   // stage C: fluxes at interface i = nz (and the bottom one for the deepest layer)
   for (int lc = threadIdx.x; lc < cm.nc; lc += blockDim.x) {
     const int j = s_item[lc], n = cm.i0 + j, k = lc - (s_off[j] - cm.c0);
-    const size_t col = (size_t)n * S;
+    const cix col = (cix)n * S;
     const int nlev = m.nlev_node[n];
     const R *Wc = a.W + col, *Ac = m.area + col;
     const int i_last = (k + 2 == nlev) ? k + 2 : k + 1;
@@ -594,7 +594,7 @@ __device__ __forceinline__ void col1_block(const DMeshT<R> &m, const FusedArgs<R
   // (lib/oce_adv_tra_driver.F90:122-181, :202-211)
   for (int lc = threadIdx.x; lc < cm.nc; lc += blockDim.x) {
     const int j = s_item[lc], n = cm.i0 + j, k = lc - (s_off[j] - cm.c0), nz = k + 1;
-    const size_t o = (size_t)n * S + k;
+    const cix o = (cix)n * S + k;
     const int nlev = m.nlev_node[n];
     R acc[NTMAX], tself[NTMAX];
     for (int t = 0; t < NT; t++) {
@@ -607,8 +607,8 @@ __device__ __forceinline__ void col1_block(const DMeshT<R> &m, const FusedArgs<R
 #pragma unroll
       for (int u = 0; u < kGChunkCol1; u++) {
         qs[u] = inc.ne[min(p + u, pe - 1)];
-        vfs[u] = a.vflux[(size_t)(qs[u].x >> 1) * S + k];
-        const size_t oo = (size_t)qs[u].y * S + k;  // the edge's other node
+        vfs[u] = a.vflux[(cix)(qs[u].x >> 1) * S + k];
+        const cix oo = (cix)qs[u].w + k;  // the edge's other node (column base in .w)
         for (int t = 0; t < NT; t++) tos[u][t] = ldT(a.T[t], oo, a.off[t]);
       }
 #pragma unroll
@@ -661,7 +661,7 @@ __device__ __forceinline__ void col2_block(const DMeshT<R> &m, const FusedArgs<R
       // are the node itself and the far ends of its edges wet at this level
       // (each such edge has a wet triangle holding both ends); max and min
       // are exact, so the bounds equal the per-element ones below.
-      const size_t on = (size_t)n * S + k;
+      const cix on = (cix)n * S + k;
       for (int t = 0; t < NT; t++) {
         const R l = a.lo[t][on], tt = ldT(a.T[t], on, a.off[t]);
         tmx[t] = fmax2(l, tt);
@@ -671,7 +671,7 @@ __device__ __forceinline__ void col2_block(const DMeshT<R> &m, const FusedArgs<R
     for (int p = inc.nep[j] - inc.sub, pe = inc.nep[j + 1] - inc.sub; p < pe; p++) {
         const int4 q = inc.ne[p];
         if (nz > q.z) continue;
-        const size_t o = (size_t)q.y * S + k;
+        const cix o = (cix)q.w + k;
         for (int t = 0; t < NT; t++) {
           const R l = a.lo[t][o], tt = ldT(a.T[t], o, a.off[t]);
           tmx[t] = fmax2(tmx[t], fmax2(l, tt));
@@ -701,7 +701,7 @@ __device__ __forceinline__ void col2_block(const DMeshT<R> &m, const FusedArgs<R
       for (int t = 0; t < NT; t++) {
         R amx, amn;
         if (wet) {
-          const size_t o0 = (size_t)e0 * S + k, o1 = (size_t)e1 * S + k, o2 = (size_t)e2 * S + k;
+          const cix o0 = (cix)e0 * S + k, o1 = (cix)e1 * S + k, o2 = (cix)e2 * S + k;
           const R l0 = a.lo[t][o0], l1 = a.lo[t][o1], l2 = a.lo[t][o2];
           const R t0 = ldT(a.T[t], o0, a.off[t]), t1 = ldT(a.T[t], o1, a.off[t]), t2 = ldT(a.T[t], o2, a.off[t]);
           amx = fmax3(fmax2(l0, t0), fmax2(l1, t1), fmax2(l2, t2));
@@ -724,7 +724,7 @@ __device__ __forceinline__ void col2_block(const DMeshT<R> &m, const FusedArgs<R
   const R eps = R((double)1e-16f);  // real(MP) :: flux_eps = 1e-16 (default-real literal)
   for (int lc = threadIdx.x; lc < cm.nc; lc += blockDim.x) {
     const int j = s_item[lc], n = cm.i0 + j, k = lc - (s_off[j] - cm.c0), nz = k + 1;
-    const size_t col = (size_t)n * S, o = col + k;
+    const cix col = (cix)n * S, o = col + k;
     const int nl1 = m.nlev_node[n];
     const bool edge_lev = (nz == 1 || nz == nl1 - 1);
     R fp[NTMAX], fm[NTMAX];
@@ -738,7 +738,7 @@ __device__ __forceinline__ void col2_block(const DMeshT<R> &m, const FusedArgs<R
       const int4 q = inc.ne[p];
       if (nz > q.z) continue;
       for (int t = 0; t < NT; t++) {
-        const R f = a.adf_h[t][(size_t)(q.x >> 1) * S + k];
+        const R f = a.adf_h[t][(cix)(q.x >> 1) * S + k];
         if (q.x & 1) {
           fp[t] = fp[t] + fmax2(R(0), -f);
           fm[t] = fm[t] + fmin2(R(0), -f);
@@ -828,7 +828,7 @@ __device__ __forceinline__ void col3_block(const DMeshT<R> &m, const FusedArgs<R
   const int S = m.S;
   for (int lc = threadIdx.x; lc < cm.nc; lc += blockDim.x) {
     const int j = s_item[lc], n = cm.i0 + j, k = lc - (s_off[j] - cm.c0), nz = k + 1;
-    const size_t col = (size_t)n * S, o = col + k;
+    const cix col = (cix)n * S, o = col + k;
     const int nlev = m.nlev_node[n];
     const R asv = m.areasvol[o], hn = m.hnode_new[o];
     const R yasv = m.rcp[o], yhn = m.rcp[m.rcp_plane + o];
@@ -857,9 +857,9 @@ __device__ __forceinline__ void col3_block(const DMeshT<R> &m, const FusedArgs<R
       const int4 q = inc.ne[p];
       if (nz > q.z) continue;
       const bool second = q.x & 1;
-      const size_t oo = (size_t)q.y * S + k;  // the edge's other node
+      const cix oo = (cix)q.w + k;  // the edge's other node (column base in .w)
       for (int t = 0; t < NT; t++) {
-        R f = a.adf_h[t][(size_t)(q.x >> 1) * S + k];
+        R f = a.adf_h[t][(cix)(q.x >> 1) * S + k];
         if (LIM == LIM_FCT) {
           // r+/- at the edge's first (o1) and second (o2) node
           const R rpo = a.rp[t][oo], rmo = a.rm[t][oo];

@@ -41,14 +41,20 @@ template <typename R> __device__ __forceinline__ R fmin3(R a, R b, R c) { return
 __device__ __forceinline__ double sgn1(double w) { return copysign(1.0, w); }
 __device__ __forceinline__ float sgn1(float w) { return copysignf(1.0f, w); }
 
+// Cell index within a (S, N) or (S, E) array: 32-bit unsigned, so that
+// address arithmetic stays one multiply-add (the engine refuses meshes with
+// E x S or N x S of 2^32 cells or more).
+using cix = unsigned;
+
+// ---------------------------------------------------------------------------
 // ---------------------------------------------------------------------------
 // tracer storage.  FP64 and FP32 storage hold the tracer T itself; 16-bit
 // storage holds the anomaly T - off on wet cells, with off a per-tracer FP32
 // constant near the field's mean, so that the storage ulp follows the
 // anomaly's magnitude.  Arithmetic is always in R.
 // ---------------------------------------------------------------------------
-template <typename R, typename TS>
-__device__ __forceinline__ R ldT(const TS *p, size_t i, R off) {
+template <typename R, typename TS, typename I>
+__device__ __forceinline__ R ldT(const TS *p, I i, R off) {
   if constexpr (std::is_same<R, TS>::value) {
     (void)off;
     return p[i];

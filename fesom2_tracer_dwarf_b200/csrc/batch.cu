@@ -156,21 +156,26 @@ struct PhasePack {
 static_assert(sizeof(PhasePack) <= 32000, "phase pack must fit the kernel parameter space");
 
 // resident 256-thread blocks per SM each phase kernel's register budget is
-// cut for (build-time knobs; default: the standalone FP32 kernels' budgets)
+// cut for (build-time knobs).  One block fewer than the standalone FP32
+// kernels: the task lookup and the descriptor loads from parameter space
+// need registers of their own.  Measured on the 48-tracer x 8-member
+// ensemble: 424 ms per step against 456 with the standalone budgets.
+// (Copying the descriptor into shared memory instead was slower still:
+// 491-525 ms, the pointers then occupy registers.)
 #ifndef FESOM_PHASE_MINB_GRAD
 #define FESOM_PHASE_MINB_GRAD FESOM_MINB32_GRAD
 #endif
 #ifndef FESOM_PHASE_MINB_EDGE
-#define FESOM_PHASE_MINB_EDGE FESOM_MINB32_EDGE
+#define FESOM_PHASE_MINB_EDGE 5
 #endif
 #ifndef FESOM_PHASE_MINB_COL1
-#define FESOM_PHASE_MINB_COL1 FESOM_MINB32_COL1
+#define FESOM_PHASE_MINB_COL1 6
 #endif
 #ifndef FESOM_PHASE_MINB_COL2
-#define FESOM_PHASE_MINB_COL2 FESOM_MINB32_COL2
+#define FESOM_PHASE_MINB_COL2 6
 #endif
 #ifndef FESOM_PHASE_MINB_COL3
-#define FESOM_PHASE_MINB_COL3 FESOM_MINB32_COL3
+#define FESOM_PHASE_MINB_COL3 6
 #endif
 template <int PH>
 struct PhaseBudget {
@@ -297,6 +302,7 @@ struct BatchImpl {
   };
   std::vector<std::vector<Slot>> slots;
   std::vector<BatchTask> tasks;
+  std::vector<int> task_slot;  // work-array slot of each task
   std::vector<int> wave_first;
   std::vector<std::vector<int>> nblk;
   PhaseKernel phk[PH_COUNT];
@@ -306,11 +312,21 @@ struct BatchImpl {
   cudaGraph_t ph_graph = nullptr;
   cudaGraphExec_t ph_exec = nullptr;
   const void *ph_key = nullptr;
+  // the phase path runs the tasks of each work-array slot on its own stream
+  // (slots are independent), so that different phase kernels share the SMs
+  static constexpr int kPhaseStreams = 4;
+  cudaStream_t ph_streams[kPhaseStreams] = {};
+  cudaEvent_t ph_fork = nullptr, ph_join[kPhaseStreams] = {};
 
   ~BatchImpl() {
     release();
     release_sep();
     if (stream) cudaStreamDestroy(stream);
+    for (int i = 0; i < kPhaseStreams; i++) {
+      if (ph_streams[i]) cudaStreamDestroy(ph_streams[i]);
+      if (ph_join[i]) cudaEventDestroy(ph_join[i]);
+    }
+    if (ph_fork) cudaEventDestroy(ph_fork);
   }
   void release_sep() {
     if (sep_exec) cudaGraphExecDestroy(sep_exec);
@@ -380,6 +396,7 @@ void refresh_vflux(BatchImpl &B) {
 void make_tasks(BatchImpl &B) {
   const int M = (int)B.members.size(), W = B.tile.wave;
   B.tasks.clear();
+  B.task_slot.clear();
   B.wave_first.clear();
   B.nblk.assign(PH_COUNT, std::vector<int>());
   for (int w = 0; w < B.nwaves; w++) {
@@ -411,6 +428,7 @@ void make_tasks(BatchImpl &B) {
         a.ph = (float)B.sch.ph;
         a.pv = (float)B.sch.pv;
         B.tasks.push_back(T);
+        B.task_slot.push_back(b % W);
         B.nblk[PH_GRAD].push_back(B.sch.hor == HOR_UPW1 ? 0 : P.dm32.grad_sched.nblk);
         B.nblk[PH_EDGE].push_back(P.dm32.edge_sched.nblk);
         B.nblk[PH_COL1].push_back(P.dm32.node_sched.nblk);
@@ -427,6 +445,11 @@ void make_tasks(BatchImpl &B) {
 
 Batch::Batch() : p_(new BatchImpl) {
   CK(cudaStreamCreateWithFlags(&p_->stream, cudaStreamNonBlocking));
+  for (int i = 0; i < BatchImpl::kPhaseStreams; i++) {
+    CK(cudaStreamCreateWithFlags(&p_->ph_streams[i], cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&p_->ph_join[i], cudaEventDisableTiming));
+  }
+  CK(cudaEventCreateWithFlags(&p_->ph_fork, cudaEventDisableTiming));
   int dev = 0;
   CK(cudaGetDevice(&dev));
   CK(cudaDeviceGetAttribute(&p_->sms, cudaDevAttrMultiProcessorCount, dev));
@@ -618,26 +641,46 @@ void swap_tasks(BatchImpl &B) {
   }
 }
 
-// one step as persistent phase launches (one per phase and wave) from the
-// host task table, which then swaps
+// one step as persistent phase launches (one per phase, wave and slot
+// stream) from the host task table, which then swaps.  The tasks of one
+// work-array slot run in order on that slot's stream; slots are independent,
+// so up to kPhaseStreams phase kernels of different slots run side by side.
 void phase_step(BatchImpl &B) {
+  const int K = std::max(1, std::min(B.tile.wave, BatchImpl::kPhaseStreams));
+  if (K > 1) {
+    CK(cudaEventRecord(B.ph_fork, B.stream));
+    for (int k = 0; k < K; k++) CK(cudaStreamWaitEvent(B.ph_streams[k], B.ph_fork, 0));
+  }
   PhasePack p{};
+  std::vector<int> sel;
   for (int w = 0; w < B.nwaves; w++) {
     const int t0 = B.wave_first[w], t1 = B.wave_first[w + 1];
-    for (int ph = 0; ph < PH_COUNT; ph++) {
-      if (!B.phk[ph].fn) continue;
-      for (int c0 = t0; c0 < t1; c0 += kPackTasks) {
-        p.ntasks = 0;
-        p.prefix[0] = 0;
-        for (int t = c0; t < std::min(t1, c0 + kPackTasks); t++) {
-          p.t[p.ntasks] = B.tasks[t];
-          p.prefix[p.ntasks + 1] = p.prefix[p.ntasks] + B.nblk[ph][t];
-          p.ntasks++;
+    for (int k = 0; k < K; k++) {
+      sel.clear();
+      for (int t = t0; t < t1; t++)
+        if (B.task_slot[t] % K == k) sel.push_back(t);
+      cudaStream_t st = K > 1 ? B.ph_streams[k] : B.stream;
+      for (int ph = 0; ph < PH_COUNT; ph++) {
+        if (!B.phk[ph].fn) continue;
+        for (size_t c0 = 0; c0 < sel.size(); c0 += kPackTasks) {
+          p.ntasks = 0;
+          p.prefix[0] = 0;
+          for (size_t i = c0; i < std::min(sel.size(), c0 + kPackTasks); i++) {
+            p.t[p.ntasks] = B.tasks[sel[i]];
+            p.prefix[p.ntasks + 1] = p.prefix[p.ntasks] + B.nblk[ph][sel[i]];
+            p.ntasks++;
+          }
+          const int total = p.prefix[p.ntasks];
+          if (total == 0) continue;
+          B.phk[ph].launch(p, std::min(total, B.phgrid[ph]), phase_smem(ph), st);
         }
-        const int total = p.prefix[p.ntasks];
-        if (total == 0) continue;
-        B.phk[ph].launch(p, std::min(total, B.phgrid[ph]), phase_smem(ph), B.stream);
       }
+    }
+  }
+  if (K > 1) {
+    for (int k = 0; k < K; k++) {
+      CK(cudaEventRecord(B.ph_join[k], B.ph_streams[k]));
+      CK(cudaStreamWaitEvent(B.stream, B.ph_join[k], 0));
     }
   }
   swap_tasks(B);

@@ -11,8 +11,10 @@
 // a CUDA graph, advances the batch step after step.  Path 1: one persistent
 // launch per phase and wave over all members (kernel boundaries order the
 // phases), each phase kernel with its own register budget and the wave's task
-// descriptors passed by value in parameter space; two steps are captured as
-// one CUDA graph.  Tracer batches run in waves of a bounded number per member
+// descriptors passed by value in parameter space, the tasks of each
+// work-array slot on their own stream (so that different phase kernels of
+// independent slots share the SMs); two steps are captured as one CUDA
+// graph.  Tracer batches run in waves of a bounded number per member
 // so the work arrays stay small; every member's edge volume fluxes are
 // computed once per velocity.  An autotuner picks the path and the tile (wet
 // cells per block, i.e. nodes per block x levels), the threads per block and

@@ -52,7 +52,8 @@ struct DMeshT {
   const unsigned char *ring_full;  // (N) 1: the ring holds every element of the node
   const int *ne_ptr;        // (N+1)
   const int4 *ne4;          // per incidence, in ascending edge id:
-                            // (slot << 1 | node is the edge's 2nd node, other node, edge levels, 0)
+                            // (slot << 1 | node is the edge's 2nd node, other node, edge levels,
+                            //  other node x S: its column base)
   const R *zbar;            // (nl)
   const R *Z;               // (nl-1)
   // 3D geometry, stride S

@@ -167,7 +167,7 @@ void build_dmesh(EngineImpl &P, DMeshT<R> &d, const std::vector<int> &slot_edge,
       for (int p = M.node_edge_ptr[n]; p < M.node_edge_ptr[n + 1]; p++) {
         const int code = M.node_edge[p], e = code >> 1, second = code & 1;
         const int other = M.edge_nodes[2 * e + (second ? 0 : 1)];
-        ne4[p] = make_int4((edge_slot[e] << 1) | second, other, M.edge_levels(e), 0);
+        ne4[p] = make_int4((edge_slot[e] << 1) | second, other, M.edge_levels(e), other * P.S);
       }
     d.ne4 = P.upload(ne4);
   }
@@ -247,6 +247,10 @@ Engine::Engine(const MeshHost &mesh, Precision prec) : p_(new EngineImpl) {
   // level stride: 32-byte aligned columns for FP64, 16-byte aligned ones (or
   // better) for the 4- and 2-byte types
   P.S = prec == Precision::FP64 ? (M.nl + 3) / 4 * 4 : (M.nl + 7) / 8 * 8;
+  // the kernels index cells with 32-bit offsets (node column bases as int)
+  if ((long long)M.nod2D * P.S >= (1ll << 31) || (long long)M.edge2D * P.S >= (1ll << 32))
+    throw std::invalid_argument("mesh too large: nodes x level stride must stay below 2^31 and edges x level stride "
+                                "below 2^32");
   CK(cudaGetDevice(&P.device));
   CK(cudaStreamCreateWithFlags(&P.stream, cudaStreamNonBlocking));
   const std::vector<int> edge_slot = edge_slot_order(M);
