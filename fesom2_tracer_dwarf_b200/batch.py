@@ -81,11 +81,12 @@ class TracerBatch:
         _lib.check(self.lib, self.lib.tracer_batch_autotune(steps_per_candidate, buf, len(buf)), "tracer_batch_autotune")
         return buf.value.decode()
 
-    PATHS = {"cooperative": 0, "phases": 1}
+    PATHS = {"cooperative": 0, "phases": 1, "separate": 2}
 
     def set_path(self, path):
         """'phases' (default): one persistent launch per phase and wave;
-        'cooperative': the whole step as one cooperative launch."""
+        'cooperative': the whole step as one cooperative launch; 'separate':
+        the members' own per-batch kernel launches on their streams."""
         _lib.check(self.lib, self.lib.tracer_batch_set_path(self.PATHS[path]), "tracer_batch_set_path")
 
     def path(self):

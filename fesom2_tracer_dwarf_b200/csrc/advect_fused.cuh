@@ -155,7 +155,7 @@ struct FusedArgs {
   R *adf_h[NTMAX];        // (S, edge)
   R *adf_v[NTMAX];        // (S, node) interfaces
   R *lo[NTMAX];           // (S, node)
-  R *rp[NTMAX], *rm[NTMAX];
+  R *rpm[NTMAX];          // (2, S, node): limiter ratios R+ and R- of each cell side by side
   R *vflux;               // (S, edge), shared by the tracers
   R *gradn[NTMAX];        // (2, S, node): ring-mean gradient (gx, gy) of valuesAB
   const R *vel;           // (2, S, elem)
@@ -762,18 +762,19 @@ __device__ __forceinline__ void col2_block(const DMeshT<R> &m, const FusedArgs<R
         bmin = fmin3(s_mn[b - 1], s_mn[b], s_mn[b + 1]) - LO;
       }
       if constexpr (sizeof(R) == 8) {
+        // two scalar stores into the pair: R+ leaves the registers before R- is formed
         R flux = div_rcp(fp[t] * a.dt, asv, yasv) + eps;
-        a.rp[t][o] = fmin2(R(1), bmax / flux);
+        a.rpm[t][2 * o] = fmin2(R(1), bmax / flux);
         flux = div_rcp(fm[t] * a.dt, asv, yasv) - eps;
-        a.rm[t][o] = fmin2(R(1), bmin / flux);
+        a.rpm[t][2 * o + 1] = fmin2(R(1), bmin / flux);
       } else {
         // FP32 arithmetic: the ratio denominators, where cancellation with
         // flux_eps matters, are formed and divided in FP64
         const double e64 = (double)1e-16f, dt64 = (double)a.dt, asv64 = (double)asv;
         double flux = (double)fp[t] * dt64 / asv64 + e64;
-        a.rp[t][o] = (R)fmin2(1.0, (double)bmax / flux);
+        a.rpm[t][2 * o] = (R)fmin2(1.0, (double)bmax / flux);
         flux = (double)fm[t] * dt64 / asv64 - e64;
-        a.rm[t][o] = (R)fmin2(1.0, (double)bmin / flux);
+        a.rpm[t][2 * o + 1] = (R)fmin2(1.0, (double)bmin / flux);
       }
     }
   }
@@ -785,20 +786,21 @@ __global__ void __launch_bounds__(kThreads, MinBlocks<R>::col2) k_col2(DMeshT<R>
   col2_block<R, TS, NT>(m, a, blockIdx.x, smem);
 }
 
-// limited vertical flux at interface i (lib/oce_adv_tra_fct.F90:396-427)
+// limited vertical flux at interface i (lib/oce_adv_tra_fct.F90:396-427);
+// rpm: the column's (R+, R-) pairs
 template <typename R>
-__device__ __forceinline__ R limit_v(const R *av, const R *rp, const R *rm, int i, int nlev) {
+__device__ __forceinline__ R limit_v(const R *av, const R *rpm, int i, int nlev) {
   const R f = av[i - 1];
   if (i == nlev) return f;
   R ae = R(1);
   if (i == 1) {
-    ae = (f >= R(0)) ? fmin2(ae, rp[0]) : fmin2(ae, rm[0]);
+    ae = (f >= R(0)) ? fmin2(ae, rpm[0]) : fmin2(ae, rpm[1]);
   } else if (f >= R(0)) {
-    ae = fmin2(ae, rm[i - 2]);
-    ae = fmin2(ae, rp[i - 1]);
+    ae = fmin2(ae, rpm[2 * (i - 2) + 1]);
+    ae = fmin2(ae, rpm[2 * (i - 1)]);
   } else {
-    ae = fmin2(ae, rp[i - 2]);
-    ae = fmin2(ae, rm[i - 1]);
+    ae = fmin2(ae, rpm[2 * (i - 2)]);
+    ae = fmin2(ae, rpm[2 * (i - 1) + 1]);
   }
   return ae * f;
 }
@@ -838,8 +840,8 @@ __device__ __forceinline__ void col3_block(const DMeshT<R> &m, const FusedArgs<R
       dv[t] = R(0);
       if (LIM == LIM_FCT) {
         dv[t] = dv[t] - ldT(a.T[t], o, a.off[t]) * m.hnode[o] + a.lo[t][o] * hn;
-        const R fk = limit_v(av, a.rp[t] + col, a.rm[t] + col, nz, nlev);
-        const R fk1 = limit_v(av, a.rp[t] + col, a.rm[t] + col, nz + 1, nlev);
+        const R fk = limit_v(av, a.rpm[t] + 2 * col, nz, nlev);
+        const R fk1 = limit_v(av, a.rpm[t] + 2 * col, nz + 1, nlev);
         dv[t] = dv[t] + div_rcp((fk - fk1) * a.dt, asv, yasv);
       } else {
         dv[t] = dv[t] + div_rcp((av[k] - av[k + 1]) * a.dt, asv, yasv);
@@ -849,8 +851,7 @@ __device__ __forceinline__ void col3_block(const DMeshT<R> &m, const FusedArgs<R
     R rps[NTMAX], rms[NTMAX];
     if (LIM == LIM_FCT)
       for (int t = 0; t < NT; t++) {
-        rps[t] = a.rp[t][o];
-        rms[t] = a.rm[t][o];
+        ld_pair(a.rpm[t] + 2 * o, rps[t], rms[t]);
       }
 #pragma unroll 4
     for (int p = inc.nep[j] - inc.sub, pe = inc.nep[j + 1] - inc.sub; p < pe; p++) {
@@ -862,7 +863,8 @@ __device__ __forceinline__ void col3_block(const DMeshT<R> &m, const FusedArgs<R
         R f = a.adf_h[t][(cix)(q.x >> 1) * S + k];
         if (LIM == LIM_FCT) {
           // r+/- at the edge's first (o1) and second (o2) node
-          const R rpo = a.rp[t][oo], rmo = a.rm[t][oo];
+          R rpo, rmo;
+          ld_pair(a.rpm[t] + 2 * oo, rpo, rmo);
           const R rp1 = second ? rpo : rps[t], rm1 = second ? rmo : rms[t];
           const R rp2 = second ? rps[t] : rpo, rm2 = second ? rms[t] : rmo;
           R ae = R(1);

@@ -298,7 +298,7 @@ struct BatchImpl {
   int mode = 1;
   // work-array slots, host task table (wave-major) and blocks per phase
   struct Slot {
-    void *adfh[kNT], *adfv[kNT], *lo[kNT], *rp[kNT], *rm[kNT], *gradn[kNT];
+    void *adfh[kNT], *adfv[kNT], *lo[kNT], *rpm[kNT], *gradn[kNT];
   };
   std::vector<std::vector<Slot>> slots;
   std::vector<BatchTask> tasks;
@@ -416,8 +416,7 @@ void make_tasks(BatchImpl &B) {
           a.adf_h[t] = (float *)sl.adfh[t];
           a.adf_v[t] = (float *)sl.adfv[t];
           a.lo[t] = (float *)sl.lo[t];
-          a.rp[t] = (float *)sl.rp[t];
-          a.rm[t] = (float *)sl.rm[t];
+          a.rpm[t] = (float *)sl.rpm[t];
           a.gradn[t] = (float *)sl.gradn[t];
         }
         a.vflux = (float *)P.vflux;
@@ -486,7 +485,10 @@ void Batch::configure(const TracerScheme &sch, const std::vector<double> &dt, bo
 
 BatchTile Batch::tile() const { return p_->tile; }
 long long Batch::work_bytes() const { return p_->work_bytes; }
-bool Batch::graph_captured() const { return p_->mode == 1 ? p_->ph_exec != nullptr : p_->graph_exec != nullptr; }
+bool Batch::graph_captured() const {
+  if (p_->mode == 2) return p_->sep_exec != nullptr;
+  return p_->mode == 1 ? p_->ph_exec != nullptr : p_->graph_exec != nullptr;
+}
 
 long long Batch::wet_cells() const {
   long long c = 0;
@@ -544,8 +546,7 @@ void Batch::set_tile(const BatchTile &tile) {
         sl.adfh[t] = B.walloc(es);
         sl.adfv[t] = B.walloc(ns);
         sl.lo[t] = B.walloc(ns);
-        sl.rp[t] = B.walloc(ns);
-        sl.rm[t] = B.walloc(ns);
+        sl.rpm[t] = B.walloc(2 * ns);
         sl.gradn[t] = B.walloc(2 * ns);
       }
     }
@@ -741,13 +742,19 @@ void begin_steps(BatchImpl &B) {
 }  // namespace
 
 void Batch::set_path(int path) {
-  if (path != 0 && path != 1) throw std::invalid_argument("batch path: 0 (one cooperative launch per step) or 1 (one launch per phase)");
+  if (path < 0 || path > 2)
+    throw std::invalid_argument("batch path: 0 (one cooperative launch per step), 1 (one launch per phase) or 2 "
+                                "(per-member launches)");
   p_->mode = path;
 }
 int Batch::path() const { return p_->mode; }
 
 void Batch::step(int nsteps, bool use_graph) {
   BatchImpl &B = *p_;
+  if (B.mode == 2) {
+    step_separate(nsteps, use_graph);
+    return;
+  }
   begin_steps(B);
   run_steps(B, nsteps, use_graph);
   CK(cudaGetLastError());
@@ -758,6 +765,7 @@ void Batch::step(int nsteps, bool use_graph) {
 
 double Batch::time_steps(int nsteps, bool use_graph) {
   BatchImpl &B = *p_;
+  if (B.mode == 2) return time_separate(nsteps, use_graph);
   begin_steps(B);
   // capture (and the device table upload) outside the timed region
   if (use_graph && B.mode == 1 && nsteps >= 2) capture_phases(B);
@@ -885,6 +893,21 @@ std::string Batch::autotune(int steps_per_candidate) {
   for (int m = 0; m < num_members(); m++) max_batches = std::max(max_batches, B.ntr[m] / kNT);
   int best_mode = B.mode;
   for (int cells : {256, 384, 512}) {
+    {
+      // per-member launches: only the cells per block of the members apply
+      BatchTile t;
+      t.cells_per_block = cells;
+      t.wave = 1;
+      set_tile(t);
+      B.mode = 2;
+      const double ms = time_steps(steps_per_candidate, false) / steps_per_candidate;
+      log << "path=separate cells=" << cells << " ms_per_step=" << ms << "\n";
+      if (ms < best_ms) {
+        best_ms = ms;
+        best = B.tile;
+        best_mode = 2;
+      }
+    }
     for (int wave : {1, 2, 4}) {
       if (wave > max_batches && wave != 1) continue;
       // one launch per phase: the tile's threads and blocks per SM do not apply
@@ -956,7 +979,8 @@ std::string Batch::autotune(int steps_per_candidate) {
   }
   set_tile(best);
   B.mode = best_mode;
-  log << "best: path=" << (best_mode == 1 ? "phases" : "cooperative") << " cells=" << best.cells_per_block
+  log << "best: path=" << (best_mode == 2 ? "separate" : best_mode == 1 ? "phases" : "cooperative")
+      << " cells=" << best.cells_per_block
       << " wave=" << best.wave << " threads=" << best.threads << " bps=" << best.blocks_per_sm
       << " ms_per_step=" << best_ms << "\n";
   return log.str();

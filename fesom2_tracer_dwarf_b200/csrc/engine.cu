@@ -370,7 +370,7 @@ void Engine::release_work() {
   EngineImpl &P = *p_;
   CK(cudaStreamSynchronize(P.stream));
   for (int t = 0; t < P.slots; t++) {
-    for (void **q : {&P.adfh[t], &P.adfv[t], &P.lo[t], &P.rp[t], &P.rm[t], &P.gradn[t]}) {
+    for (void **q : {&P.adfh[t], &P.adfv[t], &P.lo[t], &P.rpm[t], &P.gradn[t]}) {
       P.dfree(*q);
       *q = nullptr;
     }
@@ -470,8 +470,7 @@ static void ensure_slots(EngineImpl &P, int n) {
     P.adfh[t] = P.dalloc_bytes(es);
     P.adfv[t] = P.dalloc_bytes(ns);
     P.lo[t] = P.dalloc_bytes(ns);
-    P.rp[t] = P.dalloc_bytes(ns);
-    P.rm[t] = P.dalloc_bytes(ns);
+    P.rpm[t] = P.dalloc_bytes(2 * ns);
     P.gradn[t] = P.dalloc_bytes(2 * ns);
   }
   P.slots = n;
@@ -507,8 +506,7 @@ static void run_batch(EngineImpl &P, int first, int nt, double dt, bool refresh_
     b.adf_h[t] = P.adfh[t];
     b.adf_v[t] = P.adfv[t];
     b.lo[t] = P.lo[t];
-    b.rp[t] = P.rp[t];
-    b.rm[t] = P.rm[t];
+    b.rpm[t] = P.rpm[t];
     b.gradn[t] = P.gradn[t];
     if (learned_active(P) && tr.sch.hor == 1) learned_slot_buffers(P, t, &b.feat[t], &b.fscale[t]);
     b.off[t] = tr.off;
@@ -654,8 +652,7 @@ void Engine::step_with_scratch(int id, const double *T, const double *TAB, doubl
   b.adf_h[0] = scratch + es;
   b.adf_v[0] = scratch + 2 * es;
   b.lo[0] = scratch + 2 * es + ns;
-  b.rp[0] = scratch + 2 * es + 2 * ns;
-  b.rm[0] = scratch + 2 * es + 3 * ns;
+  b.rpm[0] = scratch + 2 * es + 2 * ns;  // 2 ns
   b.gradn[0] = scratch + 2 * es + 4 * ns;
   dispatch(P, P.tr[id].sch, 1, b, dt);
   CK(cudaStreamSynchronize(P.stream));

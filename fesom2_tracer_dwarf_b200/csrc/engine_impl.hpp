@@ -31,8 +31,7 @@ struct BatchPtrs {
   void *adf_h[kBatchMax] = {};
   void *adf_v[kBatchMax] = {};
   void *lo[kBatchMax] = {};
-  void *rp[kBatchMax] = {};
-  void *rm[kBatchMax] = {};
+  void *rpm[kBatchMax] = {};  // (2, S, node): R+ and R- side by side
   void *vflux = nullptr;
   int vflux_mode = 0;             // edge volume fluxes (FusedArgs::vflux_mode)
   void *gradn[kBatchMax] = {};
@@ -93,7 +92,7 @@ struct EngineImpl {
   TilePlanHost tplan;
   DTiles tiles{};
   int step_path = 1;
-  void *adfh[kBatchMax] = {}, *adfv[kBatchMax] = {}, *lo[kBatchMax] = {}, *rp[kBatchMax] = {}, *rm[kBatchMax] = {};
+  void *adfh[kBatchMax] = {}, *adfv[kBatchMax] = {}, *lo[kBatchMax] = {}, *rpm[kBatchMax] = {};
   void *gradn[kBatchMax] = {};
 
   // launch profiling: when prof is set, every launch is bracketed by events

@@ -172,8 +172,7 @@ void launch_batch_t(EngineImpl &P, const TracerScheme &sc, int nt, const BatchPt
     a.adf_h[t] = (R *)b.adf_h[t];
     a.adf_v[t] = (R *)b.adf_v[t];
     a.lo[t] = (R *)b.lo[t];
-    a.rp[t] = (R *)b.rp[t];
-    a.rm[t] = (R *)b.rm[t];
+    a.rpm[t] = (R *)b.rpm[t];
     a.gradn[t] = (R *)b.gradn[t];
     a.feat[t] = (__nv_bfloat16 *)b.feat[t];
     a.fscale[t] = (float *)b.fscale[t];

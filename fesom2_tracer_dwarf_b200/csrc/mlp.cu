@@ -562,7 +562,8 @@ __global__ void __launch_bounds__(kThreads) k_learn_apply(DMeshT<float> m, float
 
 // dL/dy for L = sum_n V_n (T_n - target_n)^2 / sum V after an unlimited step:
 // an edge flux f enters T_n1 with +dt/V and T_n2 with -dt/V, f = base + scale y
-// With the FCT limiter (adf, rp, rm set), the flux entering the update is
+// With the FCT limiter (adf, rp, rm set; rp and rm point into one array of
+// (R+, R-) pairs, stride 2), the flux entering the update is
 // ae * f with the limiter's factor ae held at its forward value.
 __global__ void __launch_bounds__(kThreads) k_learn_dy(DMeshT<float> m, const float *T, const float *target,
                                                       const float *scale, float c, const float *adf, const float *rp,
@@ -577,7 +578,7 @@ __global__ void __launch_bounds__(kThreads) k_learn_dy(DMeshT<float> m, const fl
     float ae = 1.0f;
     if (rp) {
       const float f = adf[(size_t)e * m.S + k];
-      ae = f >= 0.0f ? fminf(1.0f, fminf(rp[o1], rm[o2])) : fminf(1.0f, fminf(rm[o1], rp[o2]));
+      ae = f >= 0.0f ? fminf(1.0f, fminf(rp[2 * (o1)], rm[2 * (o2)])) : fminf(1.0f, fminf(rm[2 * (o1)], rp[2 * (o2)]));
     }
     dy[cell] = ae * scale[cell] * c * ((T[o1] - target[o1]) - (T[o2] - target[o2]));
   }
@@ -607,7 +608,7 @@ __global__ void __launch_bounds__(kThreads) k_learn_fct_g(DMeshT<float> m, const
     const size_t col = (size_t)n * S, o = col + k;
     const int nlev = m.nlev_node[n];
     const float *av = adfv + col;
-    const float rpn = rp[o], rmn = rm[o];
+    const float rpn = rp[2 * (o)], rmn = rm[2 * (o)];
     const float rho = learn_rho(T, target, o, c);
     float gp = 0.f, gm = 0.f;
     float fp = 0.f + (fmax2(0.f, av[k]) + fmax2(0.f, -av[k + 1]));
@@ -620,7 +621,7 @@ __global__ void __launch_bounds__(kThreads) k_learn_fct_g(DMeshT<float> m, const
       if (second) { fp = fp + fmax2(0.f, -f); fm = fm + fmin2(0.f, -f); }
       else { fp = fp + fmax2(0.f, f); fm = fm + fmin2(0.f, f); }
       const size_t oo = (size_t)q.y * S + k;
-      const float rpo = rp[oo], rmo = rm[oo], rho_o = learn_rho(T, target, oo, c);
+      const float rpo = rp[2 * (oo)], rmo = rm[2 * (oo)], rho_o = learn_rho(T, target, oo, c);
       const float rp1 = second ? rpo : rpn, rm1 = second ? rmo : rmn, rp2 = second ? rpn : rpo, rm2 = second ? rmn : rmo;
       const float dLdF = second ? (rho_o - rho) : (rho - rho_o);  // first node gains the flux
       if (f >= 0.f) {
@@ -643,10 +644,10 @@ __global__ void __launch_bounds__(kThreads) k_learn_fct_g(DMeshT<float> m, const
           if (f >= 0.f) { if (rpn < 1.f) gp += dLdF * f; }
           else if (rmn < 1.f) gm += dLdF * f;
         } else if (f >= 0.f) {
-          const float r_up = rm[col + i - 2], a1 = r_up < 1.f ? r_up : 1.f;
+          const float r_up = rm[2 * (col + i - 2)], a1 = r_up < 1.f ? r_up : 1.f;
           if (rpn < a1) gp += dLdF * f;
         } else {
-          const float r_up = rp[col + i - 2], a1 = r_up < 1.f ? r_up : 1.f;
+          const float r_up = rp[2 * (col + i - 2)], a1 = r_up < 1.f ? r_up : 1.f;
           if (rmn < a1) gm += dLdF * f;
         }
       }
@@ -659,10 +660,10 @@ __global__ void __launch_bounds__(kThreads) k_learn_fct_g(DMeshT<float> m, const
         const float dLdF = learn_rho(T, target, col + i - 1, c) - rho;
         if (f >= 0.f) {
           const float a1 = rmn < 1.f ? rmn : 1.f;
-          if (!(rp[col + i - 1] < a1) && rmn < 1.f) gm += dLdF * f;
+          if (!(rp[2 * (col + i - 1)] < a1) && rmn < 1.f) gm += dLdF * f;
         } else {
           const float a1 = rpn < 1.f ? rpn : 1.f;
-          if (!(rm[col + i - 1] < a1) && rpn < 1.f) gp += dLdF * f;
+          if (!(rm[2 * (col + i - 1)] < a1) && rpn < 1.f) gp += dLdF * f;
         }
       }
     }
@@ -687,7 +688,7 @@ __global__ void __launch_bounds__(kThreads) k_learn_dy_fct(DMeshT<float> m, cons
     const int2 nn = m.edge_nodes[e];
     const size_t o1 = (size_t)nn.x * m.S + k, o2 = (size_t)nn.y * m.S + k;
     const float f = adfh[(size_t)e * m.S + k];
-    const float ae = f >= 0.f ? fmin2(fmin2(1.f, rp[o1]), rm[o2]) : fmin2(fmin2(1.f, rm[o1]), rp[o2]);
+    const float ae = f >= 0.f ? fmin2(fmin2(1.f, rp[2 * (o1)]), rm[2 * (o2)]) : fmin2(fmin2(1.f, rm[2 * (o1)]), rp[2 * (o2)]);
     float g = ae * (learn_rho(T, target, o1, c) - learn_rho(T, target, o2, c));
     if (f > 0.f) g += hp[o1] - hm[o2];
     else if (f < 0.f) g += hm[o1] - hp[o2];
@@ -867,16 +868,16 @@ double Engine::learn_step(const double *T_in, const double *T_target, double dt,
         L.hm = dmalloc<float>((size_t)P.mesh.nod2D * P.S);
       }
       k_learn_fct_g<<<m.node_sched.nblk, kThreads, smem_edge(), P.stream>>>(
-          m, T, L.target, c, (const float *)P.adfh[0], (const float *)P.adfv[0], (const float *)P.rp[0],
-          (const float *)P.rm[0], (float)dt, L.hp, L.hm);
+          m, T, L.target, c, (const float *)P.adfh[0], (const float *)P.adfv[0], (const float *)P.rpm[0],
+          (const float *)P.rpm[0] + 1, (float)dt, L.hp, L.hm);
       CK(cudaGetLastError());
       k_learn_dy_fct<<<m.edge_sched.nblk, kThreads, smem_edge(), P.stream>>>(
-          m, T, L.target, c, L.fscale[0], (const float *)P.adfh[0], (const float *)P.rp[0], (const float *)P.rm[0],
+          m, T, L.target, c, L.fscale[0], (const float *)P.adfh[0], (const float *)P.rpm[0], (const float *)P.rpm[0] + 1,
           L.hp, L.hm, L.dy);
     } else {
       k_learn_dy<<<m.edge_sched.nblk, kThreads, smem_edge(), P.stream>>>(
-          m, T, L.target, L.fscale[0], c, (const float *)P.adfh[0], fct ? (const float *)P.rp[0] : nullptr,
-          fct ? (const float *)P.rm[0] : nullptr, L.dy);
+          m, T, L.target, L.fscale[0], c, (const float *)P.adfh[0], fct ? (const float *)P.rpm[0] : nullptr,
+          fct ? (const float *)P.rpm[0] + 1 : nullptr, L.dy);
     }
     CK(cudaGetLastError());
     CK(cudaMemsetAsync(L.mlp.grad, 0, kParams * sizeof(float), P.stream));

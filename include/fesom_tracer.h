@@ -340,7 +340,8 @@ int tracer_batch_get_tile(int *tile4);
  * one line per candidate (truncated to log_capacity). */
 int tracer_batch_autotune(int steps_per_candidate, char *log, int log_capacity);
 /* Step path: 0 one cooperative launch per step, 1 one persistent launch per
- * phase and wave.  get returns the path or -1. */
+ * phase and wave, 2 the members' own per-batch launches on their streams
+ * (tracer_batch_steps_separate).  get returns the path or -1. */
 int tracer_batch_set_path(int path);
 int tracer_batch_get_path(void);
 int tracer_batch_steps(int nsteps, int use_graph);
