@@ -67,6 +67,8 @@ def parse():
     p.add_argument("--precision", default="fp64", choices=["fp64", "fp64fma", "fp32", "bf16", "fp16"])
     p.add_argument("--step-path", default="five", choices=["fused", "five"],
                    help="the five-kernel path (default) or the fused patch kernel")
+    p.add_argument("--cells-per-block", type=int, default=0,
+                   help="target wet cells per block of the five-kernel schedules (0: the default, 512)")
     p.add_argument("--learned", action="store_true",
                    help="FP32 with the learned antidiffusive flux (shipped parameters) ahead of FCT")
     p.add_argument("--config", default="c2", choices=["c2", "c3", "c4", "dd"],
@@ -256,6 +258,8 @@ def run_ours(args):
     K, uv, w, T, S, dt, cells = make_inputs(api, args.nx, args.nl)
     api.set_precision(args.precision)
     api.set_step_path(args.step_path)
+    if args.cells_per_block:
+        api.set_cells_per_block(args.cells_per_block)
     api.allocate_tracers(2)
     api.set_values(1, T)
     api.set_values(2, S)
@@ -366,7 +370,8 @@ def run_ours(args):
             "metric": "tracer cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": DTYPE[args.precision], "data": "synthetic",
-            "config": workload_config(args.nx, args.nl, cells, dt, world),
+            "config": dict(workload_config(args.nx, args.nl, cells, dt, world),
+                           **({"cells_per_block": args.cells_per_block} if args.cells_per_block else {})),
             "device_bytes": dev_bytes,
             "precision": args.precision + (", learned antidiffusive flux (MLP on tcgen05) ahead of FCT"
                                            if args.learned else ""),

@@ -62,6 +62,7 @@ SIGNATURES = {
     "tracer_set_step_path": (ctypes.c_int, [ctypes.c_int]),
     "tracer_step_info": (ctypes.c_int, [_vp]),
     "tracer_set_patch_size": (ctypes.c_int, [ctypes.c_int]),
+    "tracer_set_cells_per_block": (ctypes.c_int, [ctypes.c_int]),
     "tracer_set_nan_check": (ctypes.c_int, [ctypes.c_int]),
     "tracer_advect_step_io": (ctypes.c_int, [ctypes.c_double, _vp, _vp, ctypes.c_int]),
     "tracer_step_status": (ctypes.c_int, [_vp]),

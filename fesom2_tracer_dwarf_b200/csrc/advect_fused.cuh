@@ -152,9 +152,9 @@ struct FusedArgs {
   const TS *T[NTMAX];     // values
   const TS *TAB[NTMAX];   // valuesAB (high-order fluxes)
   TS *T_out[NTMAX];
-  R *adf_h[NTMAX];        // (S, edge)
+  R *adf_h[NTMAX];        // (NT, S, edge) tracer-interleaved: adf_h[t] = adf_h[0] + t, stride NT
   R *adf_v[NTMAX];        // (S, node) interfaces
-  R *lo[NTMAX];           // (S, node)
+  R *lo[NTMAX];           // (NT, S, node) tracer-interleaved like adf_h
   R *rpm[NTMAX];          // (2, S, node): limiter ratios R+ and R- of each cell side by side
   R *vflux;               // (S, edge), shared by the tracers
   R *gradn[NTMAX];        // (2, S, node): ring-mean gradient (gx, gy) of valuesAB
@@ -261,6 +261,42 @@ __device__ __forceinline__ void st_pair(float *p, float x, float y) {
   *reinterpret_cast<float2 *>(p) = make_float2(x, y);
 }
 
+// Tracer-interleaved work arrays (adf_h, lo): tracer t's value of cell o is
+// at X[t][o * NT] with X[t] = X[0] + t, so one vector load brings a cell's
+// values of every tracer of the batch (NT = 1, 2 or 4).
+template <int NT, typename R>
+__device__ __forceinline__ R &il(R *const *x, int t, cix o) {
+  return x[t][(size_t)o * NT];
+}
+template <int NT>
+__device__ __forceinline__ void il_load(const double *x0, cix o, double *v) {
+  const double *p = x0 + (size_t)o * NT;
+  if constexpr (NT == 1) {
+    v[0] = p[0];
+  } else if constexpr (NT == 2) {
+    const double2 a = *reinterpret_cast<const double2 *>(p);
+    v[0] = a.x; v[1] = a.y;
+  } else {
+    static_assert(NT == 4, "batches hold 1, 2 or 4 tracers");
+    const double2 a = reinterpret_cast<const double2 *>(p)[0], b = reinterpret_cast<const double2 *>(p)[1];
+    v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+  }
+}
+template <int NT>
+__device__ __forceinline__ void il_load(const float *x0, cix o, float *v) {
+  const float *p = x0 + (size_t)o * NT;
+  if constexpr (NT == 1) {
+    v[0] = p[0];
+  } else if constexpr (NT == 2) {
+    const float2 a = *reinterpret_cast<const float2 *>(p);
+    v[0] = a.x; v[1] = a.y;
+  } else {
+    static_assert(NT == 4, "batches hold 1, 2 or 4 tracers");
+    const float4 a = *reinterpret_cast<const float4 *>(p);
+    v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+  }
+}
+
 template <typename R, typename TS, int NT>
 __device__ __forceinline__ void grad_block(const DMeshT<R> &m, const FusedArgs<R, TS> &a, int blk, int *smem) {
   int *s_off = smem, *s_item = smem + kMaxItemsPerBlock + 1;
@@ -341,7 +377,7 @@ __device__ __forceinline__ void edge_block(const DMeshT<R> &m, const FusedArgs<R
     if (HOR == HOR_UPW1) {
       for (int t = 0; t < NT; t++) {
         const R flo = (LIM == LIM_FCT) ? upw1_flux(vflux, ldT(a.T[t], o1, a.off[t]), ldT(a.T[t], o2, a.off[t])) : R(0);
-        a.adf_h[t][o] = upw1_flux(vflux, ldT(a.TAB[t], o1, a.off[t]), ldT(a.TAB[t], o2, a.off[t])) - flo;
+        il<NT>(a.adf_h, t, o) = upw1_flux(vflux, ldT(a.TAB[t], o1, a.off[t]), ldT(a.TAB[t], o2, a.off[t])) - flo;
       }
       continue;
     }
@@ -382,7 +418,7 @@ __device__ __forceinline__ void edge_block(const DMeshT<R> &m, const FusedArgs<R
       const R cHO = (vflux + fabs(vflux)) * Tmean1 + (vflux - fabs(vflux)) * Tmean2;
       const R ho = -(R(0.5) * (R(1) - a.ph) * cHO) - vflux * a.ph * R(0.5) * (Tmean1 + Tmean2);
       const R flo = (LIM == LIM_FCT) ? upw1_flux(vflux, ldT(a.T[t], o1, a.off[t]), ldT(a.T[t], o2, a.off[t])) : R(0);
-      a.adf_h[t][o] = ho - flo;
+      il<NT>(a.adf_h, t, o) = ho - flo;
       if constexpr (sizeof(R) == 4 && HOR == HOR_MUSCL) {
         if (a.feat[t]) {
           // features in the flow's frame, in units of the local variation sig
@@ -623,12 +659,12 @@ __device__ __forceinline__ void col1_block(const DMeshT<R> &m, const FusedArgs<R
       }
     }
     const R asv = m.areasvol[o], hn = m.hnode_new[o], h = m.hnode[o];
-    const R yasv = R(1) / asv, yhn = R(1) / hn;
+    const R yasv = m.rcp[o], yhn = m.rcp[m.rcp_plane + o];  // reciprocal planes (k_rcp_planes)
     for (int t = 0; t < NT; t++) {
       const R fk = s_fv[t * kMaxCellsPerBlock + lc];
       const R fk1 = (k + 2 == nlev) ? R(0) : s_fv[t * kMaxCellsPerBlock + lc + 1];
       const R num = tself[t] * h + div_rcp((acc[t] + (fk - fk1)) * a.dt, asv, yasv);
-      a.lo[t][o] = div_rcp(num, hn, yhn);
+      il<NT>(a.lo, t, o) = div_rcp(num, hn, yhn);
     }
   }
 }
@@ -662,8 +698,10 @@ __device__ __forceinline__ void col2_block(const DMeshT<R> &m, const FusedArgs<R
       // (each such edge has a wet triangle holding both ends); max and min
       // are exact, so the bounds equal the per-element ones below.
       const cix on = (cix)n * S + k;
+      R lv[NTMAX];
+      il_load<NT>(a.lo[0], on, lv);
       for (int t = 0; t < NT; t++) {
-        const R l = a.lo[t][on], tt = ldT(a.T[t], on, a.off[t]);
+        const R l = lv[t], tt = ldT(a.T[t], on, a.off[t]);
         tmx[t] = fmax2(l, tt);
         tmn[t] = fmin2(l, tt);
       }
@@ -672,8 +710,9 @@ __device__ __forceinline__ void col2_block(const DMeshT<R> &m, const FusedArgs<R
         const int4 q = inc.ne[p];
         if (nz > q.z) continue;
         const cix o = (cix)q.w + k;
+        il_load<NT>(a.lo[0], o, lv);
         for (int t = 0; t < NT; t++) {
-          const R l = a.lo[t][o], tt = ldT(a.T[t], o, a.off[t]);
+          const R l = lv[t], tt = ldT(a.T[t], o, a.off[t]);
           tmx[t] = fmax2(tmx[t], fmax2(l, tt));
           tmn[t] = fmin2(tmn[t], fmin2(l, tt));
         }
@@ -702,7 +741,7 @@ __device__ __forceinline__ void col2_block(const DMeshT<R> &m, const FusedArgs<R
         R amx, amn;
         if (wet) {
           const cix o0 = (cix)e0 * S + k, o1 = (cix)e1 * S + k, o2 = (cix)e2 * S + k;
-          const R l0 = a.lo[t][o0], l1 = a.lo[t][o1], l2 = a.lo[t][o2];
+          const R l0 = il<NT>(a.lo, t, o0), l1 = il<NT>(a.lo, t, o1), l2 = il<NT>(a.lo, t, o2);
           const R t0 = ldT(a.T[t], o0, a.off[t]), t1 = ldT(a.T[t], o1, a.off[t]), t2 = ldT(a.T[t], o2, a.off[t]);
           amx = fmax3(fmax2(l0, t0), fmax2(l1, t1), fmax2(l2, t2));
           amn = fmin3(fmin2(l0, t0), fmin2(l1, t1), fmin2(l2, t2));
@@ -737,8 +776,10 @@ __device__ __forceinline__ void col2_block(const DMeshT<R> &m, const FusedArgs<R
     for (int p = inc.nep[j] - inc.sub, pe = inc.nep[j + 1] - inc.sub; p < pe; p++) {
       const int4 q = inc.ne[p];
       if (nz > q.z) continue;
+      R fv[NTMAX];
+      il_load<NT>(a.adf_h[0], (cix)(q.x >> 1) * S + k, fv);
       for (int t = 0; t < NT; t++) {
-        const R f = a.adf_h[t][(cix)(q.x >> 1) * S + k];
+        const R f = fv[t];
         if (q.x & 1) {
           fp[t] = fp[t] + fmax2(R(0), -f);
           fm[t] = fm[t] + fmin2(R(0), -f);
@@ -749,10 +790,10 @@ __device__ __forceinline__ void col2_block(const DMeshT<R> &m, const FusedArgs<R
       }
     }
     const R asv = m.areasvol[o];
-    const R yasv = R(1) / asv;
+    const R yasv = m.rcp[o];  // 1/areasvol plane (k_rcp_planes)
     for (int t = 0; t < NT; t++) {
       const int b = t * kMaxCellsPerBlock + lc;
-      const R LO = a.lo[t][o];
+      const R LO = il<NT>(a.lo, t, o);
       R bmax, bmin;
       if (edge_lev) {
         bmax = s_mx[b] - LO;
@@ -808,9 +849,11 @@ __device__ __forceinline__ R limit_v(const R *av, const R *rpm, int i, int nlev)
 // ---------------------------------------------------------------------------
 // k_col3: limiting + flux2dtracer + update
 // ---------------------------------------------------------------------------
-// Reciprocals of the static cell geometry for k_col3 (computed per step
-// they cost two divisions per cell; measured: loading them is 2-3 % faster
-// there, while the same for k_col1's PPM weights was slower).
+// Reciprocals of the static cell geometry, 1/areasvol and 1/hnode_new, for
+// the Markstein divisions of k_col1's LO solution, k_col2's ratio
+// denominators and k_col3's update (computed per step they cost an IEEE
+// division each; measured in k_col3: loading them is 2-3 % faster, while
+// the same for k_col1's ten PPM weights was slower).
 template <typename R>
 __global__ void k_rcp_planes(DMeshT<R> m, R *rcp) {
   const size_t plane = (size_t)m.S * m.N;
@@ -839,7 +882,7 @@ __device__ __forceinline__ void col3_block(const DMeshT<R> &m, const FusedArgs<R
       const R *av = a.adf_v[t] + col;
       dv[t] = R(0);
       if (LIM == LIM_FCT) {
-        dv[t] = dv[t] - ldT(a.T[t], o, a.off[t]) * m.hnode[o] + a.lo[t][o] * hn;
+        dv[t] = dv[t] - ldT(a.T[t], o, a.off[t]) * m.hnode[o] + il<NT>(a.lo, t, o) * hn;
         const R fk = limit_v(av, a.rpm[t] + 2 * col, nz, nlev);
         const R fk1 = limit_v(av, a.rpm[t] + 2 * col, nz + 1, nlev);
         dv[t] = dv[t] + div_rcp((fk - fk1) * a.dt, asv, yasv);
@@ -859,8 +902,10 @@ __device__ __forceinline__ void col3_block(const DMeshT<R> &m, const FusedArgs<R
       if (nz > q.z) continue;
       const bool second = q.x & 1;
       const cix oo = (cix)q.w + k;  // the edge's other node (column base in .w)
+      R fv[NTMAX];
+      il_load<NT>(a.adf_h[0], (cix)(q.x >> 1) * S + k, fv);
       for (int t = 0; t < NT; t++) {
-        R f = a.adf_h[t][(cix)(q.x >> 1) * S + k];
+        R f = fv[t];
         if (LIM == LIM_FCT) {
           // r+/- at the edge's first (o1) and second (o2) node
           R rpo, rmo;

@@ -44,6 +44,7 @@ struct State {
   bool fma64 = false;  // precision mode 4: FP64 with FMA-contracted kernels
   bool nan_check = false;  // tracer_set_nan_check
   int patch_size = 0;  // tracer_set_patch_size (0: the default)
+  int cells_per_block = 0;  // tracer_set_cells_per_block (0: the default)
   std::vector<int> ids;  // tracer IDs read from a restart
 };
 State g;
@@ -77,6 +78,7 @@ void ensure_engine() {
   g.eng->set_step_path(g.step_path);
   g.eng->set_fma64(g.fma64);
   if (g.patch_size > 0) g.eng->set_patch_size(g.patch_size);
+  if (g.cells_per_block > 0) g.eng->set_cells_per_block(g.cells_per_block);
   if (g.ntr > 0) {
     g.eng->allocate_tracers(g.ntr);
     for (int i = 0; i < g.ntr; i++) {
@@ -577,6 +579,15 @@ int tracer_set_patch_size(int owned) {
     if (owned < 0) return fail("patch size must be >= 0 (0: the default)");
     g.patch_size = owned;
     if (g.eng) g.eng->set_patch_size(owned > 0 ? owned : kTileOwned);
+    return 0;
+  });
+}
+
+int tracer_set_cells_per_block(int cells) {
+  return guarded([&] {
+    if (cells != 0 && (cells < 32 || cells > 576)) return fail("cells per block must be 0 (the default) or in [32, 576]");
+    g.cells_per_block = cells;
+    if (g.eng) g.eng->set_cells_per_block(cells > 0 ? cells : Engine::kDefaultCellsPerBlock);
     return 0;
   });
 }

@@ -222,6 +222,8 @@ void build_tiles(EngineImpl &P, const std::vector<int> &edge_slot, int owned) {
 
 }  // namespace
 
+static_assert(Engine::kDefaultCellsPerBlock == kCellsPerBlock, "one default schedule tile");
+
 std::vector<int> edge_slot_order(const MeshHost &M) {
   // slot order: edges sorted by their smaller node id (stable in edge id)
   const int E = M.edge2D;
@@ -369,8 +371,11 @@ void Engine::allocate_tracers(int ntr, bool with_ab) {
 void Engine::release_work() {
   EngineImpl &P = *p_;
   CK(cudaStreamSynchronize(P.stream));
+  P.dfree(P.adfh[0]);  // the interleaved arrays: one allocation each
+  P.dfree(P.lo[0]);
   for (int t = 0; t < P.slots; t++) {
-    for (void **q : {&P.adfh[t], &P.adfv[t], &P.lo[t], &P.rpm[t], &P.gradn[t]}) {
+    P.adfh[t] = P.lo[t] = nullptr;
+    for (void **q : {&P.adfv[t], &P.rpm[t], &P.gradn[t]}) {
       P.dfree(*q);
       *q = nullptr;
     }
@@ -466,10 +471,18 @@ static void ensure_slots(EngineImpl &P, int n) {
   if (n <= P.slots) return;
   const size_t ns = (size_t)P.mesh.nod2D * P.S * P.r_bytes, es = (size_t)P.mesh.edge2D * P.S * P.r_bytes;
   if (!P.vflux) P.vflux = P.dalloc_bytes(es);
+  // adf_h and lo are interleaved by tracer (a batch of NT tracers uses stride
+  // NT): one array each, reallocated for the larger batch
+  CK(cudaStreamSynchronize(P.stream));
+  P.dfree(P.adfh[0]);
+  P.dfree(P.lo[0]);
+  char *ah = (char *)P.dalloc_bytes(n * es), *lo = (char *)P.dalloc_bytes(n * ns);
+  for (int t = 0; t < n; t++) {
+    P.adfh[t] = ah + t * P.r_bytes;
+    P.lo[t] = lo + t * P.r_bytes;
+  }
   for (int t = P.slots; t < n; t++) {
-    P.adfh[t] = P.dalloc_bytes(es);
     P.adfv[t] = P.dalloc_bytes(ns);
-    P.lo[t] = P.dalloc_bytes(ns);
     P.rpm[t] = P.dalloc_bytes(2 * ns);
     P.gradn[t] = P.dalloc_bytes(2 * ns);
   }

@@ -58,6 +58,8 @@ class Engine {
   const MeshHost &mesh() const;
   int level_stride() const;
   // Schedule tile: target wet cells per block (32..576, default 512).
+  // target wet cells per block of the step kernels' schedules (32..576)
+  static constexpr int kDefaultCellsPerBlock = 512;
   void set_cells_per_block(int cells);
   int cells_per_block() const;
   // Internal state, for the multi-member batch runner (batch.cu).

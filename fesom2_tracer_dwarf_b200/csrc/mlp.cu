@@ -550,13 +550,16 @@ struct LearnedState {
 
 namespace {
 
-__global__ void __launch_bounds__(kThreads) k_learn_apply(DMeshT<float> m, float *adf, const float *scale, const float *y) {
+// adf: tracer t's slot of the batch's tracer-interleaved antidiffusive fluxes
+// (stride nt)
+__global__ void __launch_bounds__(kThreads) k_learn_apply(DMeshT<float> m, float *adf, int nt, const float *scale,
+                                                         const float *y) {
   extern __shared__ int smem[];
   int *s_off = smem, *s_item = smem + kMaxItemsPerBlock + 1;
   const CellMap cm = map_cells(m.edge_sched, blockIdx.x, s_off, s_item);
   for (int lc = threadIdx.x; lc < cm.nc; lc += blockDim.x) {
     const int j = s_item[lc], e = cm.i0 + j, k = lc - (s_off[j] - cm.c0), cell = cm.c0 + lc;
-    adf[(size_t)e * m.S + k] += scale[cell] * y[cell];
+    adf[((size_t)e * m.S + k) * nt] += scale[cell] * y[cell];
   }
 }
 
@@ -762,7 +765,7 @@ void learned_correct_f32(EngineImpl &P, int nt, const FusedArgs<float, float> &a
     if (mlp_forward_dev(L.mlp, a.feat[t], L.ncells, L.y[t], P.stream) != 0)
       throw std::runtime_error("learned flux: MLP forward launch failed");
     if (P.dm32.edge_sched.nblk > 0)
-      k_learn_apply<<<P.dm32.edge_sched.nblk, kThreads, smem_edge(), P.stream>>>(P.dm32, a.adf_h[t], a.fscale[t],
+      k_learn_apply<<<P.dm32.edge_sched.nblk, kThreads, smem_edge(), P.stream>>>(P.dm32, a.adf_h[t], nt, a.fscale[t],
                                                                                   L.y[t]);
     CK(cudaGetLastError());
   }

@@ -195,6 +195,10 @@ class FESOMTracerAdvection:
         """'five' (default: five kernels) or 'fused' (one patch kernel per tracer where the scheme allows it)."""
         _lib.check(self.lib, self.lib.tracer_set_step_path({"fused": 0, "five": 1}[path]), "tracer_set_step_path")
 
+    def set_cells_per_block(self, cells):
+        """Target wet cells per block of the five-kernel schedules (0: the default, 512)."""
+        _lib.check(self.lib, self.lib.tracer_set_cells_per_block(int(cells)), "tracer_set_cells_per_block")
+
     def set_patch_size(self, owned):
         """Owned nodes per patch of the fused kernel (0: the default)."""
         _lib.check(self.lib, self.lib.tracer_set_patch_size(int(owned)), "tracer_set_patch_size")

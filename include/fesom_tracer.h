@@ -186,6 +186,9 @@ int tracer_step_info(double *out4);
 /* Owned nodes per patch of the fused kernel's plan (0 = the default, 225);
  * every size gives the same results, small ones recompute more halo. */
 int tracer_set_patch_size(int owned);
+/* Target wet cells per thread block of the five-kernel path's schedules (0 =
+ * the default, 512; 32..576); every size gives the same results. */
+int tracer_set_cells_per_block(int cells);
 /* Failure detection (no counterpart in the reference): the update kernels
  * count, on the device, every new tracer value that is not finite.
  * tracer_step_status returns that count since its last call (and resets
