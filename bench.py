@@ -68,7 +68,7 @@ def parse():
     p.add_argument("--step-path", default="five", choices=["fused", "five"],
                    help="the five-kernel path (default) or the fused patch kernel")
     p.add_argument("--cells-per-block", type=int, default=0,
-                   help="target wet cells per block of the five-kernel schedules (0: the default, 512)")
+                   help="most wet cells per block of the five-kernel schedules (0: the default, 512)")
     p.add_argument("--learned", action="store_true",
                    help="FP32 with the learned antidiffusive flux (shipped parameters) ahead of FCT")
     p.add_argument("--config", default="c2", choices=["c2", "c3", "c4", "dd"],

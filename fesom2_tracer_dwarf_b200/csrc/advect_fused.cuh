@@ -108,7 +108,7 @@ struct StageIncidence<float> {
 #define FESOM_GCHUNK_COL1 2
 #endif
 constexpr int kGChunkCol1 = FESOM_GCHUNK_COL1;
-constexpr int kCellsPerBlock = 512;      // schedule target: wet cells per block
+constexpr int kCellsPerBlock = 512;      // schedule cap: wet cells per block (two per thread)
 constexpr int kMaxCellsPerBlock = 576;   // upper bound (target + deepest column)
 constexpr int kMaxItemsPerBlock = 512;
 
@@ -153,7 +153,7 @@ struct FusedArgs {
   const TS *TAB[NTMAX];   // valuesAB (high-order fluxes)
   TS *T_out[NTMAX];
   R *adf_h[NTMAX];        // (NT, S, edge) tracer-interleaved: adf_h[t] = adf_h[0] + t, stride NT
-  R *adf_v[NTMAX];        // (S, node) interfaces
+  R *adf_v[NTMAX];        // (NT, S, node) interfaces, tracer-interleaved like adf_h
   R *lo[NTMAX];           // (NT, S, node) tracer-interleaved like adf_h
   R *rpm[NTMAX];          // (2, S, node): limiter ratios R+ and R- of each cell side by side
   R *vflux;               // (S, edge), shared by the tracers
@@ -618,7 +618,7 @@ __device__ __forceinline__ void col1_block(const DMeshT<R> &m, const FusedArgs<R
         }
       }
       for (int t = 0; t < NT; t++) {
-        a.adf_v[t][col + i - 1] = hov[t];
+        il<NT>(a.adf_v, t, col + i - 1) = hov[t];
         if (LIM == LIM_FCT && i == k + 1) s_fv[t * kMaxCellsPerBlock + lc] = lov[t];
       }
     }
@@ -767,10 +767,14 @@ __device__ __forceinline__ void col2_block(const DMeshT<R> &m, const FusedArgs<R
     const int nl1 = m.nlev_node[n];
     const bool edge_lev = (nz == 1 || nz == nl1 - 1);
     R fp[NTMAX], fm[NTMAX];
-    for (int t = 0; t < NT; t++) {
-      const R *av = a.adf_v[t] + col;
-      fp[t] = R(0) + (fmax2(R(0), av[k]) + fmax2(R(0), -av[k + 1]));
-      fm[t] = R(0) + (fmin2(R(0), av[k]) + fmin2(R(0), -av[k + 1]));
+    {
+      R v0[NTMAX], v1[NTMAX];  // interfaces k and k + 1 of every tracer
+      il_load<NT>(a.adf_v[0], o, v0);
+      il_load<NT>(a.adf_v[0], o + 1, v1);
+      for (int t = 0; t < NT; t++) {
+        fp[t] = R(0) + (fmax2(R(0), v0[t]) + fmax2(R(0), -v1[t]));
+        fm[t] = R(0) + (fmin2(R(0), v0[t]) + fmin2(R(0), -v1[t]));
+      }
     }
 #pragma unroll 4
     for (int p = inc.nep[j] - inc.sub, pe = inc.nep[j + 1] - inc.sub; p < pe; p++) {
@@ -828,10 +832,11 @@ __global__ void __launch_bounds__(kThreads, MinBlocks<R>::col2) k_col2(DMeshT<R>
 }
 
 // limited vertical flux at interface i (lib/oce_adv_tra_fct.F90:396-427);
-// rpm: the column's (R+, R-) pairs
-template <typename R>
+// av: the tracer's slot of the column's interleaved interface fluxes (stride
+// NT); rpm: the column's (R+, R-) pairs
+template <int NT, typename R>
 __device__ __forceinline__ R limit_v(const R *av, const R *rpm, int i, int nlev) {
-  const R f = av[i - 1];
+  const R f = av[(i - 1) * NT];
   if (i == nlev) return f;
   R ae = R(1);
   if (i == 1) {
@@ -879,15 +884,15 @@ __device__ __forceinline__ void col3_block(const DMeshT<R> &m, const FusedArgs<R
     const R yasv = m.rcp[o], yhn = m.rcp[m.rcp_plane + o];
     R dv[NTMAX], dh[NTMAX];
     for (int t = 0; t < NT; t++) {
-      const R *av = a.adf_v[t] + col;
+      const R *av = a.adf_v[t] + (size_t)col * NT;
       dv[t] = R(0);
       if (LIM == LIM_FCT) {
         dv[t] = dv[t] - ldT(a.T[t], o, a.off[t]) * m.hnode[o] + il<NT>(a.lo, t, o) * hn;
-        const R fk = limit_v(av, a.rpm[t] + 2 * col, nz, nlev);
-        const R fk1 = limit_v(av, a.rpm[t] + 2 * col, nz + 1, nlev);
+        const R fk = limit_v<NT>(av, a.rpm[t] + 2 * col, nz, nlev);
+        const R fk1 = limit_v<NT>(av, a.rpm[t] + 2 * col, nz + 1, nlev);
         dv[t] = dv[t] + div_rcp((fk - fk1) * a.dt, asv, yasv);
       } else {
-        dv[t] = dv[t] + div_rcp((av[k] - av[k + 1]) * a.dt, asv, yasv);
+        dv[t] = dv[t] + div_rcp((av[k * NT] - av[(k + 1) * NT]) * a.dt, asv, yasv);
       }
       dh[t] = R(0);
     }

@@ -542,11 +542,11 @@ void Batch::set_tile(const BatchTile &tile) {
     const int used = std::min(W, B.ntr[m] / kNT);
     for (int j = 0; j < used; j++) {
       BatchImpl::Slot &sl = B.slots[m][j];
-      // adf_h and lo interleaved by tracer (stride kNT)
-      char *ah = (char *)B.walloc(kNT * es), *lo = (char *)B.walloc(kNT * ns);
+      // adf_h, lo and adf_v interleaved by tracer (stride kNT)
+      char *ah = (char *)B.walloc(kNT * es), *lo = (char *)B.walloc(kNT * ns), *av = (char *)B.walloc(kNT * ns);
       for (int t = 0; t < kNT; t++) {
         sl.adfh[t] = ah + t * sizeof(float);
-        sl.adfv[t] = B.walloc(ns);
+        sl.adfv[t] = av + t * sizeof(float);
         sl.lo[t] = lo + t * sizeof(float);
         sl.rpm[t] = B.walloc(2 * ns);
         sl.gradn[t] = B.walloc(2 * ns);

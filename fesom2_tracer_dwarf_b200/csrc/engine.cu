@@ -30,22 +30,24 @@ void build_sched(const std::vector<int> &counts, std::vector<int> &off, std::vec
   blk.clear();
   blk.push_back(0);
   max_items = 1;
+  // cells_per_block is a cap: a block takes whole items while its wet cells
+  // stay within it, so that the 256 threads of a block walk its cells in at
+  // most cap / 256 rounds (with a target instead, blocks overshooting 512
+  // cells by a column gave a third round to a few threads, and the block's
+  // time followed them: measured at 1000x1000x64, a 448 target was 6 %
+  // faster than a 512 one).  A single item larger than the cap gets a block
+  // of its own.
+  const int cap = std::min(cells_per_block, kMaxCellsPerBlock);
   int start = 0, cells = 0;
   for (int i = 0; i < n; i++) {
     // close the block before an item that would overflow its capacity
-    if (i > start && (cells + counts[i] > kMaxCellsPerBlock || i - start >= kMaxItemsPerBlock)) {
+    if (i > start && (cells + counts[i] > cap || i - start >= kMaxItemsPerBlock)) {
       blk.push_back(i);
       max_items = std::max(max_items, i - start);
       start = i;
       cells = 0;
     }
     cells += counts[i];
-    if (cells >= cells_per_block) {
-      blk.push_back(i + 1);
-      max_items = std::max(max_items, i + 1 - start);
-      start = i + 1;
-      cells = 0;
-    }
   }
   if (start < n || n == 0) {
     blk.push_back(n);
@@ -71,7 +73,7 @@ R *upload_conv(EngineImpl &P, const std::vector<double> &h) {
   return P.upload(st);
 }
 
-// Work schedules (node, edge and gradient cells) for a target number of wet
+// Work schedules (node, edge and gradient cells) for a cap on the wet
 // cells per block; the arrays of a previous tiling are released.
 template <typename R>
 void build_schedules(EngineImpl &P, DMeshT<R> &d, int cells_per_block) {
@@ -373,9 +375,10 @@ void Engine::release_work() {
   CK(cudaStreamSynchronize(P.stream));
   P.dfree(P.adfh[0]);  // the interleaved arrays: one allocation each
   P.dfree(P.lo[0]);
+  P.dfree(P.adfv[0]);
   for (int t = 0; t < P.slots; t++) {
-    P.adfh[t] = P.lo[t] = nullptr;
-    for (void **q : {&P.adfv[t], &P.rpm[t], &P.gradn[t]}) {
+    P.adfh[t] = P.lo[t] = P.adfv[t] = nullptr;
+    for (void **q : {&P.rpm[t], &P.gradn[t]}) {
       P.dfree(*q);
       *q = nullptr;
     }
@@ -471,18 +474,19 @@ static void ensure_slots(EngineImpl &P, int n) {
   if (n <= P.slots) return;
   const size_t ns = (size_t)P.mesh.nod2D * P.S * P.r_bytes, es = (size_t)P.mesh.edge2D * P.S * P.r_bytes;
   if (!P.vflux) P.vflux = P.dalloc_bytes(es);
-  // adf_h and lo are interleaved by tracer (a batch of NT tracers uses stride
+  // adf_h, lo and adf_v are interleaved by tracer (a batch of NT tracers uses stride
   // NT): one array each, reallocated for the larger batch
   CK(cudaStreamSynchronize(P.stream));
   P.dfree(P.adfh[0]);
   P.dfree(P.lo[0]);
-  char *ah = (char *)P.dalloc_bytes(n * es), *lo = (char *)P.dalloc_bytes(n * ns);
+  P.dfree(P.adfv[0]);
+  char *ah = (char *)P.dalloc_bytes(n * es), *lo = (char *)P.dalloc_bytes(n * ns), *av = (char *)P.dalloc_bytes(n * ns);
   for (int t = 0; t < n; t++) {
     P.adfh[t] = ah + t * P.r_bytes;
     P.lo[t] = lo + t * P.r_bytes;
+    P.adfv[t] = av + t * P.r_bytes;
   }
   for (int t = P.slots; t < n; t++) {
-    P.adfv[t] = P.dalloc_bytes(ns);
     P.rpm[t] = P.dalloc_bytes(2 * ns);
     P.gradn[t] = P.dalloc_bytes(2 * ns);
   }

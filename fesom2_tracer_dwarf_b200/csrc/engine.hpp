@@ -57,8 +57,8 @@ class Engine {
 
   const MeshHost &mesh() const;
   int level_stride() const;
-  // Schedule tile: target wet cells per block (32..576, default 512).
-  // target wet cells per block of the step kernels' schedules (32..576)
+  // Schedule tile: the most wet cells a block of the step kernels takes
+  // (32..576, default 512: two per thread of a 256-thread block).
   static constexpr int kDefaultCellsPerBlock = 512;
   void set_cells_per_block(int cells);
   int cells_per_block() const;

@@ -196,7 +196,7 @@ class FESOMTracerAdvection:
         _lib.check(self.lib, self.lib.tracer_set_step_path({"fused": 0, "five": 1}[path]), "tracer_set_step_path")
 
     def set_cells_per_block(self, cells):
-        """Target wet cells per block of the five-kernel schedules (0: the default, 512)."""
+        """Most wet cells per block of the five-kernel schedules (0: the default, 512)."""
         _lib.check(self.lib, self.lib.tracer_set_cells_per_block(int(cells)), "tracer_set_cells_per_block")
 
     def set_patch_size(self, owned):

@@ -186,7 +186,7 @@ int tracer_step_info(double *out4);
 /* Owned nodes per patch of the fused kernel's plan (0 = the default, 225);
  * every size gives the same results, small ones recompute more halo. */
 int tracer_set_patch_size(int owned);
-/* Target wet cells per thread block of the five-kernel path's schedules (0 =
+/* Most wet cells per thread block of the five-kernel path's schedules (0 =
  * the default, 512; 32..576); every size gives the same results. */
 int tracer_set_cells_per_block(int cells);
 /* Failure detection (no counterpart in the reference): the update kernels
@@ -333,7 +333,7 @@ int tracer_batch_get_values(int member, int tracer_id, double *values);
  * tile. */
 int tracer_batch_configure(const char *hor, const char *ver, const char *lim, double ph, double pv, const double *dt,
                            int refresh_ab);
-/* Tile: target wet cells per block (32..576), threads per block (64..256),
+/* Tile: most wet cells per block (32..576), threads per block (64..256),
  * persistent blocks per SM (capped by occupancy), 4-tracer batches in flight
  * per member. */
 int tracer_batch_set_tile(int cells_per_block, int threads, int blocks_per_sm, int wave);
