@@ -66,7 +66,8 @@ class Batch {
 
   // nsteps steps of the selected path (replayed from a CUDA graph when use_graph).
   void step(int nsteps, bool use_graph);
-  // Device time of nsteps (CUDA events on the batch stream), milliseconds.
+  // Device time of nsteps (CUDA events on the batch stream), milliseconds;
+  // path 2 returns time_separate's host time (one more, untimed step first).
   double time_steps(int nsteps, bool use_graph);
   // The same steps as separate per-member, per-batch kernel launches on the
   // members' streams; with use_graph those launches are replayed from a CUDA

@@ -348,7 +348,9 @@ int tracer_batch_autotune(int steps_per_candidate, char *log, int log_capacity);
 int tracer_batch_set_path(int path);
 int tracer_batch_get_path(void);
 int tracer_batch_steps(int nsteps, int use_graph);
-/* Device time (CUDA events) of nsteps steps of the selected path, milliseconds. */
+/* Device time (CUDA events) of nsteps steps of the selected path,
+ * milliseconds; path 2 behaves as tracer_batch_time_separate (one more,
+ * untimed step first, host time between device synchronisations). */
 int tracer_batch_time_steps(int nsteps, int use_graph, double *ms);
 /* The same steps as per-member launches of the four-to-five step kernels per
  * 4-tracer batch (the path tracer_advect_step takes) on the members' own
