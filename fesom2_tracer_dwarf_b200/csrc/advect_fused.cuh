@@ -101,11 +101,13 @@ struct StageIncidence<float> {
 // address of a cell's level lies inside its padded column, so the loads of
 // dry edge levels, and of the clamped records past the node's last edge, are
 // in bounds; their values are discarded.  The fluxes are still accumulated
-// one edge at a time in ascending incidence order.  (Measured per kernel: 2
-// is faster than 1 or 4 for k_col1; the same form is slower in k_col2 and
+// one edge at a time in ascending incidence order.  (Measured per kernel on
+// the 512-cell capped schedules at 1000x1000x64: k_col1 FP64 with 1 / 2 / 3
+// / 4 / 6 edges 3.24 / 2.89 / 2.76 / 3.14 / 2.98 ms, FP32 with 2 / 3 / 4 / 6
+// 1.71 / 1.59 / 1.71 / 1.76 ms; the same form is slower in k_col2 and
 // k_col3, whose loops stay one edge at a time.)
 #ifndef FESOM_GCHUNK_COL1
-#define FESOM_GCHUNK_COL1 2
+#define FESOM_GCHUNK_COL1 3
 #endif
 constexpr int kGChunkCol1 = FESOM_GCHUNK_COL1;
 constexpr int kCellsPerBlock = 512;      // schedule cap: wet cells per block (two per thread)
