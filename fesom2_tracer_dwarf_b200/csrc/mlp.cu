@@ -99,6 +99,13 @@ __device__ __forceinline__ float gelu(float z) {
   const float t = tanh_fast(kGeluC * (z + kGeluA * z * z * z));
   return 0.5f * z * (1.0f + t);
 }
+// acc + GELU(z) w3 with hw3 = w3 / 2, i.e. acc + hw3 z (1 + tanh u):
+// u = z (c + c a z^2), then one add and one FMA
+__device__ __forceinline__ float gelu_out(float z, float hw3, float acc) {
+  const float t = tanh_fast(z * fmaf(kGeluC * kGeluA, z * z, kGeluC));
+  const float hz = z * hw3;
+  return fmaf(hz, t, acc + hz);
+}
 __device__ __forceinline__ float gelu_grad(float z) {
   const float t = tanh_fast(kGeluC * (z + kGeluA * z * z * z));
   return 0.5f * (1.0f + t) + 0.5f * z * (1.0f - t * t) * kGeluC * (1.0f + 3.0f * kGeluA * z * z);
@@ -124,9 +131,12 @@ __device__ __forceinline__ __half2 gelu2(__half2 z) {
   return __hfma2(hz, tanh_fast2(u), hz);             // z/2 (1 + tanh u)
 }
 // 16 FP32 pre-activations (bias added) -> GELU -> 16 BF16 in two 16-byte stores
+// (bias: 16-byte aligned shared memory, read as four 16-byte vectors)
 __device__ __forceinline__ void gelu_store16(unsigned char *base, uint32_t off_lo, uint32_t off_hi, const float *v,
-                                             const float *bias) {
+                                             const float *bias_s) {
   __align__(16) __nv_bfloat162 o[8];
+  float bias[16];
+  for (int i = 0; i < 4; i++) reinterpret_cast<float4 *>(bias)[i] = reinterpret_cast<const float4 *>(bias_s)[i];
   for (int i = 0; i < 8; i++) {
     const __half2 g = gelu2(__floats2half2_rn(v[2 * i] + bias[2 * i], v[2 * i + 1] + bias[2 * i + 1]));
     o[i] = __float22bfloat162_rn(__half22float2(g));
@@ -207,22 +217,30 @@ __device__ __forceinline__ void smem_to_tc() {
   umma::tc_fence_after();
 }
 
+// TMEM columns of one forward CTA (the 64 FP32 accumulator columns of a
+// 128 x 64 layer output).  With 64 columns, eight CTAs fit an SM's 512 TMEM
+// columns, so shared memory (about 32 KB per CTA) sets how many run side by
+// side; their tiles' load, MMA and epilogue phases overlap one another.
+constexpr uint32_t kFwdTmemCols = 64;
+
 __global__ void __launch_bounds__(128, 1)
     k_mlp_fwd(const __nv_bfloat16 *X, long long S, MlpDev w, float *y, int *status) {
   extern __shared__ __align__(1024) unsigned char sm[];
   __shared__ __align__(8) uint64_t mbar;
   __shared__ uint32_t tbase;
-  __shared__ float sb1[kH], sb2[kH], sw3[kH];
+  __shared__ __align__(16) float sb1[kH];
+  __shared__ __align__(16) float sb2[kH];
+  __shared__ __align__(16) float shw3[kH];
   const int tid = threadIdx.x, warp = tid >> 5;
   load_weights(sm, w, FwdSmem::W1, FwdSmem::W2, 0xffffffffu);
   if (tid < kH) {
     sb1[tid] = w.p[kOffB1 + tid];
     sb2[tid] = w.p[kOffB2 + tid];
-    sw3[tid] = w.p[kOffW3 + tid];
+    shw3[tid] = 0.5f * w.p[kOffW3 + tid];  // the GELU's 1/2 folded into the output weights
   }
   const float b3 = w.p[kOffB3];
   if (warp == 0) {
-    umma::tmem_alloc(&tbase, 128);
+    umma::tmem_alloc(&tbase, kFwdTmemCols);
     umma::tmem_relinquish();
   }
   if (tid == 0) {
@@ -231,7 +249,11 @@ __global__ void __launch_bounds__(128, 1)
   }
   smem_to_tc();
   const uint32_t tmem = tbase, lane = (uint32_t)(warp * 32) << 16;
-  const uint32_t D1 = tmem, D2 = tmem + 64;
+  // both layers accumulate into the same 64 columns: every thread has read
+  // the first layer's result (tcgen05.ld + wait::ld) before the barrier that
+  // precedes the second MMA, and has read the second's before the barrier
+  // that ends the tile
+  const uint32_t D1 = tmem, D2 = tmem;
   const uint32_t aX = umma::smem_u32(sm + FwdSmem::X), aH1 = umma::smem_u32(sm + FwdSmem::H1);
   const uint32_t aW1 = umma::smem_u32(sm + FwdSmem::W1), aW2 = umma::smem_u32(sm + FwdSmem::W2);
   uint32_t phase = 0;
@@ -264,7 +286,12 @@ __global__ void __launch_bounds__(128, 1)
     for (int c = 0; c < kH; c += 16) {
       float v[16];
       umma::tmem_ld16(D2 + lane + c, v);
-      for (int i = 0; i < 16; i++) acc += gelu(v[i] + sb2[c + i]) * sw3[c + i];
+      float b[16], hw[16];
+      for (int i = 0; i < 4; i++) {
+        reinterpret_cast<float4 *>(b)[i] = reinterpret_cast<const float4 *>(sb2 + c)[i];
+        reinterpret_cast<float4 *>(hw)[i] = reinterpret_cast<const float4 *>(shw3 + c)[i];
+      }
+      for (int i = 0; i < 16; i++) acc = gelu_out(v[i] + b[i], hw[i], acc);
     }
     if (sample < S) y[sample] = acc + b3;
     umma::tc_fence_before();
@@ -279,7 +306,7 @@ __global__ void __launch_bounds__(128, 1)
   __syncthreads();
   if (warp == 0) {
     umma::tc_fence_after();
-    umma::tmem_dealloc(tmem, 128);
+    umma::tmem_dealloc(tmem, kFwdTmemCols);
   }
 }
 
@@ -495,14 +522,37 @@ static size_t train_smem() { return TrainSmem::END; }
 // y[S] = MLP(X[S][16]) on the device (X BF16, 16-byte aligned rows)
 int mlp_forward_dev(const MlpState &s, const __nv_bfloat16 *X, long long S, float *y, cudaStream_t st) {
   static bool attr = false;
+  static int per_sm = 1;
   if (!attr) {
     if (cudaFuncSetAttribute(k_mlp_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fwd_smem()) != cudaSuccess)
       return -1;
+    // A CTA's tile loop is grid-strided, so the grid is exactly the CTAs that
+    // are resident together (a CTA started after another one's exit would run
+    // its whole share late): the CTAs an SM's shared memory, registers and
+    // threads hold, at most 512 / kFwdTmemCols for TMEM.  (Counted here from
+    // the kernel's attributes: the runtime's occupancy query answered one CTA
+    // per SM for this kernel, which the shared memory does not require.)
+    if (cudaFuncSetAttribute(k_mlp_fwd, cudaFuncAttributePreferredSharedMemoryCarveout,
+                             (int)cudaSharedmemCarveoutMaxShared) != cudaSuccess)
+      return -1;
+    cudaFuncAttributes fa{};
+    int dev = 0, smem_sm = 0, resv = 0, regs_sm = 0, thr_sm = 0;
+    if (cudaFuncGetAttributes(&fa, k_mlp_fwd) != cudaSuccess || cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&resv, cudaDevAttrReservedSharedMemoryPerBlock, dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&thr_sm, cudaDevAttrMaxThreadsPerMultiProcessor, dev) != cudaSuccess)
+      return -1;
+    const int per_cta_smem = (int)(fwd_smem() + fa.sharedSizeBytes) + resv;
+    const int regs_cta = ((fa.numRegs + 7) / 8) * 8 * 128;
+    per_sm = std::min({smem_sm / per_cta_smem, regs_sm / std::max(regs_cta, 1), thr_sm / 128,
+                       512 / (int)kFwdTmemCols});
+    if (per_sm < 1) return -1;
     attr = true;
   }
   if (S <= 0) return 0;
   const long long tiles = (S + 127) / 128;
-  const int grid = (int)std::min<long long>(tiles, (long long)s.sms * 4);
+  const int grid = (int)std::min<long long>(tiles, (long long)s.sms * per_sm);
   k_mlp_fwd<<<grid, 128, fwd_smem(), st>>>(X, S, mlp_view(s), y, s.status);
   return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
