@@ -108,6 +108,7 @@ SIGNATURES = {
     "tracer_batch_get_tile": (ctypes.c_int, [_vp]),
     "tracer_batch_autotune": (ctypes.c_int, [ctypes.c_int, ctypes.c_char_p, ctypes.c_int]),
     "tracer_batch_set_path": (ctypes.c_int, [ctypes.c_int]),
+    "tracer_batch_learn_set": (ctypes.c_int, [_vp, ctypes.c_int]),
     "tracer_batch_get_path": (ctypes.c_int, []),
     "tracer_batch_steps": (ctypes.c_int, [ctypes.c_int, ctypes.c_int]),
     "tracer_batch_time_steps": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),

@@ -94,6 +94,15 @@ class TracerBatch:
         _lib.check(self.lib, min(rc, 0), "tracer_batch_get_path")
         return {v: k for k, v in self.PATHS.items()}[rc]
 
+    def learn_set(self, params=None, on=True):
+        """The learned antidiffusive flux on every member's MUSCL tracers
+        (params: the MLP's packed FP32 parameters; None keeps each member's).
+        While on, the batch steps on the 'separate' path."""
+        p = None if params is None else np.ascontiguousarray(params, dtype=np.float32)
+        if p is not None and p.shape != (self.lib.tracer_mlp_num_params(),):
+            raise ValueError("params must hold tracer_mlp_num_params() floats")
+        _lib.check(self.lib, self.lib.tracer_batch_learn_set(_lib.ptr(p), int(bool(on))), "tracer_batch_learn_set")
+
     def steps(self, n, graph=True):
         _lib.check(self.lib, self.lib.tracer_batch_steps(n, int(bool(graph))), "tracer_batch_steps")
 

@@ -294,8 +294,12 @@ struct BatchImpl {
   std::vector<cudaEvent_t> sep_events;
 
   // step path: 0 one cooperative launch per step, 1 one persistent launch
-  // per phase and wave
+  // per phase and wave, 2 the members' own launches
   int mode = 1;
+  // learned antidiffusive flux on every member (path 2 only: the member
+  // engines run the MLP between their edge and column kernels; the
+  // persistent paths' phase kernels have no MLP phase)
+  bool learned = false;
   // work-array slots, host task table (wave-major) and blocks per phase
   struct Slot {
     void *adfh[kNT], *adfv[kNT], *lo[kNT], *rpm[kNT], *gradn[kNT];
@@ -747,12 +751,24 @@ void Batch::set_path(int path) {
   if (path < 0 || path > 2)
     throw std::invalid_argument("batch path: 0 (one cooperative launch per step), 1 (one launch per phase) or 2 "
                                 "(per-member launches)");
+  if (p_->learned && path != 2)
+    throw std::invalid_argument("batch path: with the learned flux only path 2 (per-member launches) runs");
   p_->mode = path;
 }
 int Batch::path() const { return p_->mode; }
 
+void Batch::set_learned(const float *params, bool on) {
+  BatchImpl &B = *p_;
+  CK(cudaStreamSynchronize(B.stream));
+  for (auto &m : B.members) m->set_learned(params, on);
+  B.learned = on;
+  if (on) B.mode = 2;
+}
+bool Batch::learned() const { return p_->learned; }
+
 void Batch::step(int nsteps, bool use_graph) {
   BatchImpl &B = *p_;
+  if (B.learned && B.mode != 2) throw std::logic_error("batch: the learned flux runs on path 2 only");
   if (B.mode == 2) {
     step_separate(nsteps, use_graph);
     return;
@@ -767,6 +783,7 @@ void Batch::step(int nsteps, bool use_graph) {
 
 double Batch::time_steps(int nsteps, bool use_graph) {
   BatchImpl &B = *p_;
+  if (B.learned && B.mode != 2) throw std::logic_error("batch: the learned flux runs on path 2 only");
   if (B.mode == 2) return time_separate(nsteps, use_graph);
   begin_steps(B);
   // capture (and the device table upload) outside the timed region
@@ -911,6 +928,7 @@ std::string Batch::autotune(int steps_per_candidate) {
       }
     }
     for (int wave : {1, 2, 4}) {
+      if (B.learned) break;  // the persistent paths have no MLP phase
       if (wave > max_batches && wave != 1) continue;
       // one launch per phase: the tile's threads and blocks per SM do not apply
       {

@@ -64,6 +64,13 @@ class Batch {
   void set_path(int path);
   int path() const;
 
+  // Learned antidiffusive flux (MUSCL tracers) on every member with these
+  // parameters (nullptr: keep each member's); while on, the batch runs path
+  // 2, whose member engines evaluate the MLP between their edge and column
+  // kernels, and set_path refuses the persistent paths.
+  void set_learned(const float *params, bool on);
+  bool learned() const;
+
   // nsteps steps of the selected path (replayed from a CUDA graph when use_graph).
   void step(int nsteps, bool use_graph);
   // Device time of nsteps (CUDA events on the batch stream), milliseconds;

@@ -1047,6 +1047,14 @@ int tracer_batch_get_path(void) {
   return guarded([&] { return batch().path(); });
 }
 
+int tracer_batch_learn_set(const float *params, int on) {
+  return guarded([&] {
+    if (batch().num_members() == 0) return fail("the batch has no members");
+    batch().set_learned(params, on != 0);
+    return 0;
+  });
+}
+
 int tracer_batch_steps(int nsteps, int use_graph) {
   return guarded([&] {
     if (nsteps < 0) return fail("nsteps < 0");

@@ -347,6 +347,13 @@ int tracer_batch_autotune(int steps_per_candidate, char *log, int log_capacity);
  * (tracer_batch_steps_separate).  get returns the path or -1. */
 int tracer_batch_set_path(int path);
 int tracer_batch_get_path(void);
+/* Learned antidiffusive flux (no counterpart in the reference) on every
+ * member's MUSCL tracers: params as for tracer_learn_set (NULL keeps each
+ * member's), on = 0/1.  While on, the batch steps on path 2 (the members'
+ * own launches, which evaluate the MLP between their edge and column
+ * kernels), tracer_batch_set_path(0 or 1) returns -1, and the autotuner
+ * times path 2's tiles only. */
+int tracer_batch_learn_set(const float *params, int on);
 int tracer_batch_steps(int nsteps, int use_graph);
 /* Device time (CUDA events) of nsteps steps of the selected path,
  * milliseconds; path 2 behaves as tracer_batch_time_separate (one more,
