@@ -461,6 +461,8 @@ Batch::~Batch() { delete p_; }
 
 int Batch::add_member(const MeshHost &mesh, int ntracers) {
   if (ntracers < kNT || ntracers % kNT) throw std::invalid_argument("batch members need a multiple of 4 tracers");
+  if (p_->learned)
+    throw std::logic_error("batch: switch the learned flux off (tracer_batch_learn_set) before adding members");
   p_->members.emplace_back(new Engine(mesh, Precision::FP32));
   p_->members.back()->allocate_tracers(ntracers, false);  // valuesAB := values
   p_->ntr.push_back(ntracers);

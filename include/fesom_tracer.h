@@ -306,14 +306,15 @@ int tracer_advect_device_noalloc(int tracer_id, const double *T_dev, const doubl
 long long tracer_noalloc_scratch_bytes(void);
 /* ---- multi-member batch: no counterpart in the reference -----------------
  * Many tracers of many ensemble members, each on its own analytic mesh (any
- * sizes, periodic or closed), advanced together in FP32.  Two step paths
+ * sizes, periodic or closed), advanced together in FP32.  Three step paths
  * (tracer_batch_set_path): path 1 (default) runs one persistent launch per
  * phase (gradients, edge fluxes, vertical fluxes and LO solution, FCT ratios,
  * limiting and update) and wave of tracer batches over every member's work;
  * path 0 runs the whole step as one persistent cooperative launch with
  * grid-wide barriers between the phases (bounded waits: a timed-out barrier
- * makes the step return -1).  tracer_batch_steps with use_graph = 1 replays
- * the launches from a CUDA graph.  Both paths give the same bits.  Members are
+ * makes the step return -1); path 2 runs the members' own launches.
+ * tracer_batch_steps with use_graph = 1 replays the launches from a CUDA
+ * graph.  The three paths give the same bits.  Members are
  * numbered from 0, tracers from 1.  Supported schemes: MUSCL+PPM or
  * UPW1+UPW1, with or without FCT, one scheme for all tracers. */
 int tracer_batch_create(void);
@@ -351,8 +352,8 @@ int tracer_batch_get_path(void);
  * member's MUSCL tracers: params as for tracer_learn_set (NULL keeps each
  * member's), on = 0/1.  While on, the batch steps on path 2 (the members'
  * own launches, which evaluate the MLP between their edge and column
- * kernels), tracer_batch_set_path(0 or 1) returns -1, and the autotuner
- * times path 2's tiles only. */
+ * kernels), tracer_batch_set_path(0 or 1) and tracer_batch_add_member
+ * return -1, and the autotuner times path 2's tiles only. */
 int tracer_batch_learn_set(const float *params, int on);
 int tracer_batch_steps(int nsteps, int use_graph);
 /* Device time (CUDA events) of nsteps steps of the selected path,

@@ -178,6 +178,8 @@ def test_learned_flux_runs_on_the_member_path(small_batch, api):
     assert b.path() == "separate"
     with pytest.raises(RuntimeError):
         b.set_path("phases")
+    with pytest.raises(RuntimeError):
+        b.add_member(12, 12, 6, 4)
     b.steps(2, graph=False)
     learned = _state(b)
     _reset(b, init)
