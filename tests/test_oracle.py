@@ -68,21 +68,23 @@ def _volume_sum(m, T):
     return float(np.sum(np.where(wet, T * asv * h, 0.0)))
 
 
-@pytest.mark.parametrize("hor,ver", [("MUSCL", "PPM"), ("MFCT", "QR4C"), ("UPW1", "CDIFF"), ("MUSCL", "UPW1")])
-def test_fct_conserves_and_bounds(oracle, hor, ver):
+@pytest.mark.parametrize("hor,ver,periodic", [("MUSCL", "PPM", True), ("MFCT", "QR4C", True), ("UPW1", "CDIFF", True),
+                                              ("MUSCL", "UPW1", True), ("MUSCL", "PPM", False), ("MFCT", "CDIFF", False)])
+def test_fct_conserves_and_bounds(oracle, hor, ver, periodic):
     """Sum(T*vol) conserved to round-off and the FCT solution stays inside
-    the local min/max of the old and low-order fields (lib/oce_adv_tra_fct.F90)."""
+    the local min/max of the old and low-order fields (lib/oce_adv_tra_fct.F90),
+    on a periodic mesh and on one closed by walls, both with bathymetry."""
     import ctypes
     lib = pytest.importorskip("fesom2_tracer_dwarf_b200._lib").load()
     nx, ny, nl = 18, 14, 9
-    N = lib.tracer_analytic_nodes(nx, ny, 1)
+    N = lib.tracer_analytic_nodes(nx, ny, int(periodic))
     K = np.zeros(N, dtype=np.int32)
     lib.tracer_synth_bathymetry(N, nl, 3, K.ctypes.data_as(ctypes.c_void_p))
-    m = pyoracle.OracleMesh(oracle, nx, ny, nl, periodic=True, full_rings=True, node_K=K)
+    m = pyoracle.OracleMesh(oracle, nx, ny, nl, periodic=periodic, full_rings=True, node_K=K)
     from fesom2_tracer_dwarf_b200 import FESOMTracerAdvection
     api = FESOMTracerAdvection()
     api.cleanup()
-    api.init_analytic(nx, ny, nl, periodic=True, full_rings=True, node_K=K)
+    api.init_analytic(nx, ny, nl, periodic=periodic, full_rings=True, node_K=K)
     uv, w = api.synth_velocity(seed=1, umax=1.0, mode2=0.4)
     T = np.asfortranarray(api.synth_tracer(seed=2, kind=0))
     api.cleanup()
