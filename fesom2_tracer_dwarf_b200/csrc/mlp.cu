@@ -500,6 +500,11 @@ static bool mlp_alloc(MlpState &s) {
       cudaMalloc(&s.W1b, kH * kF * 2) != cudaSuccess || cudaMalloc(&s.W2b, kH * kH * 2) != cudaSuccess ||
       cudaMalloc(&s.status, 4) != cudaSuccess)
     return false;
+  // until parameters are given the network is zero (y = 0: the plain scheme)
+  cudaMemset(s.p, 0, kParams * 4);
+  cudaMemset(s.grad, 0, kParams * 4);
+  cudaMemset(s.W1b, 0, kH * kF * 2);
+  cudaMemset(s.W2b, 0, kH * kH * 2);
   cudaMemset(s.m1, 0, kParams * 4);
   cudaMemset(s.m2, 0, kParams * 4);
   cudaMemset(s.status, 0, 4);

@@ -392,7 +392,8 @@ int tracer_mlp_forward(const uint16_t *X, long long S, const float *params, floa
 /* grads = d/dparams sum_s dy[s] * y(X[s]) (host arrays). */
 int tracer_mlp_grads(const uint16_t *X, const float *dy, long long S, const float *params, float *grads);
 /* The learned flux inside the engine (precision mode 1, FP32; MUSCL
- * tracers): set the parameters (NULL keeps them) and switch it on or off.  On,
+ * tracers): set the parameters (NULL keeps them; an engine never given any
+ * has the zero network, whose correction is 0) and switch it on or off.  On,
  * every MUSCL edge flux becomes HO - LO + scale * MLP(features) before the
  * vertical fluxes and the unchanged FCT limiter.  A precision change drops it. */
 int tracer_learn_set(const float *params, int on);
