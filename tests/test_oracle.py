@@ -241,3 +241,24 @@ def test_mlp_oracle_gradients_match_finite_differences():
         e[i] = 1e-6
         fd = (dy @ mo.forward(X, p + e, False)[0] - dy @ mo.forward(X, p - e, False)[0]) / 2e-6
         assert abs(fd - g[i]) <= 1e-6 * max(1.0, abs(g[i])), (i, fd, g[i])
+
+
+@pytest.mark.parametrize("periodic", [True, False])
+def test_openmp_oracle_equals_serial(oracle, periodic):
+    """The OpenMP build of the oracle (the checker of the full-size GPU parity
+    test and the CPU baseline) gives the serial build's bits: every node sums
+    its edges in ascending edge id on both, whatever the thread count."""
+    omp = pyoracle.Oracle(openmp=True)
+    omp.set_threads(4)
+    results = []
+    for o in (oracle, omp):
+        m, K, uv, w, T, S, dt, wet = pyoracle.layered_flow_case(o, 90, 24, seed=3, periodic=periodic)
+        for hor, ver in (("MUSCL", "PPM"), ("MFCT", "QR4C")):
+            X = np.asfortranarray(T.copy())
+            for _ in range(3):
+                m.step(X, X.copy(order="F"), uv, w, dt, hor, ver, "FCT")
+            results.append(X)
+    half = len(results) // 2
+    for a, b in zip(results[:half], results[half:]):
+        assert np.array_equal(a.view(np.uint64), b.view(np.uint64))
+    assert not np.array_equal(results[0], T)
