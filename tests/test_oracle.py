@@ -262,3 +262,18 @@ def test_openmp_oracle_equals_serial(oracle, periodic):
     for a, b in zip(results[:half], results[half:]):
         assert np.array_equal(a.view(np.uint64), b.view(np.uint64))
     assert not np.array_equal(results[0], T)
+
+
+@pytest.mark.parametrize("hor,ver", [("MUSCL", "PPM"), ("MFCT", "QR4C"), ("UPW1", "CDIFF"), ("MUSCL", "UPW1")])
+def test_unlimited_schemes_conserve(oracle, hor, ver):
+    """Without the limiter every scheme still conserves Sum(T*vol): the edge
+    fluxes leave one node and enter the other, and the vertical fluxes vanish
+    at the surface (w = 0 there) and the bottom."""
+    m, K, uv, w, T, S, dt, wet = pyoracle.layered_flow_case(oracle, 40, 12, seed=5, periodic=True)
+    X = np.asfortranarray(T.copy())
+    s0 = _volume_sum(m, X)
+    for _ in range(4):
+        m.step(X, X.copy(order="F"), uv, w, dt, hor, ver, "NONE")
+    assert np.all(np.isfinite(X))
+    assert not np.array_equal(X, T)
+    assert abs(_volume_sum(m, X) - s0) <= 1e-12 * abs(s0)
